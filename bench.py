@@ -1,0 +1,326 @@
+"""Benchmark of the RK4 + RBF-FD hot path on B200.
+
+Default workload: the plain GPU drop-in on the N=40962 (level-6) icosahedral
+grid in FP64, CFDL layout, RCM order, dt = 225 s -- the configuration the
+reference's "plain GPU drop-in vs reference OpenMP" comparison is quoted on.
+A step is one full RK4 step (4 fused stage kernels) of one state.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  `value` = node-stage updates/s (4 * N * steps / s)
+with the state resident in HBM, timed with CUDA events around each step on the
+library's stream, L2 flushed (a 256 MB write) between timed steps; `e2e` = the
+same metric through the C ABI with host buffers (pinned H2D of the state,
+one RK4 step, D2H of the state every step); `roofline` = the fused stage
+kernel's algorithmic bytes (1396 B per FP64 node-stage, 760 B FP32) over its
+CUDA-event duration against the measured HBM copy bandwidth.  Multi-GPU runs
+are independent replicas (the path does not shard across GPUs here): every
+rank steps its own state, time is the max over ranks, value is the sum.
+
+--impl reference times the reference's own CPU code (oracle/_ref, built from
+the reference's sources; the oracle port if that is absent) on the host cores
+with OpenMP, on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rbf-fd-swe_b200"))
+
+WORKLOADS = {
+    # name: (level, precision, description)
+    "plain_fp64_n40962": (6, "fp64", "plain FP64, N=40962 (level 6), CFDL, RCM, dt=225 s"),
+    "plain_fp64_n655362": (8, "fp64", "plain FP64, N=655362 (level 8), CFDL, RCM, dt=60 s"),
+    "plain_fp32_n655362": (8, "fp32", "plain FP32, N=655362 (level 8), CFDL, RCM, dt=60 s"),
+}
+ALG_BYTES = {"fp64": 1396, "fp32": 760}      # per node-stage (FP64: 4*31*8+31*4+17*8+4*8+14*8)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def build_workload(level: int, prec: str, device: str):
+    from swe_b200 import gen, layout, swe_input
+
+    t0 = time.time()
+    d = gen.generate(level, seed=1, device=device)
+    m = swe_input.to_model(d)
+    pm, mapping = layout.prepare(m, use_rcm=True, simd_length=32)
+    log(f"[bench] generated level {level} (N={d.N}) in {time.time() - t0:.1f}s")
+    return d, m, pm
+
+
+def cpu_baseline_sample(d, prec: str, target_s: float = 15.0):
+    """The reference's own CPU code (oracle/_ref) on a bounded number of steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from swe_b200 import swe_input
+
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_SCHEDULE", "static")
+    tmp = tempfile.mkdtemp(prefix="swe_bench_")
+    path = os.path.join(tmp, f"icos{d.N}.bin")
+    swe_input.write_input(path, d)
+    if oracle.reference_available(prec, "cfdl"):
+        ref = oracle.Ref(path, prec, "cfdl", use_rcm=1)
+        H = ref.H_init()
+        H, t1, _ = ref.run(H, 1)                    # warm-up step, also sizes the sample
+        steps = max(1, min(200, int(target_s / max(t1, 1e-4))))
+        H, t, t_rhs = ref.run(H, steps)
+        kind = "reference"
+        sample = f"{steps} RK4 steps of the reference's RK_substep (OpenMP, {cores} threads, CFDL, RCM) on N={d.N}"
+    else:
+        m = swe_input.to_model(d)
+        port = oracle.Port(m, prec)
+        t0 = time.time()
+        port.run(m.H_init, 1)
+        t1 = time.time() - t0
+        steps = max(1, min(200, int(target_s / max(t1, 1e-4))))
+        t0 = time.time()
+        port.run(m.H_init, steps)
+        t = time.time() - t0
+        kind = "port"
+        sample = f"{steps} RK4 steps of the C port (OpenMP, {cores} threads) on N={d.N}"
+    os.remove(path)
+    return {"value": 4.0 * d.N * steps / t, "unit": "node-stage updates/s", "cores": cores,
+            "kind": kind, "sample": sample, "seconds": round(t, 3)}
+
+
+def run_reference(args, level, prec, wl):
+    """--impl reference: the reference's own CPU implementation, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from swe_b200 import gen
+
+    d = gen.generate(level, seed=1, device="cpu")
+    base = cpu_baseline_sample(d, prec, target_s=max(5.0, 2.0 * args.steps))
+    line = {
+        "metric": "node-stage updates/s (RK4 + RBF-FD stage, plain form)",
+        "value": base["value"], "unit": "node-stage updates/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * 4.0 * d.N / base["value"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32", "data": "synthetic",
+        "config": {"workload": wl, "nodes": d.N, "nnbr": 31, "dt": d.dt, "layout": "CFDL", "rcm": True},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": "node-stage updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain_fp64_n40962", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    level, prec, desc = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, level, prec, args.workload)
+
+    import torch
+    import torch.distributed as dist
+
+    from swe_b200 import capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    d, m, pm = build_workload(level, prec, device=f"cuda:{local}")
+    N = d.N
+    dt_np = np.float64 if prec == "fp64" else np.float32
+    plain = capi.Plain()
+    capi.check("swe_cuda_select_device", plain.lib.swe_cuda_select_device(local))
+    plain.init_model(pm, prec)
+    stream = torch.cuda.ExternalStream(plain.stream())
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    plain.set_state(pm.H_init)
+    for _ in range(args.warmup):
+        plain.step(1)
+    plain.sync()
+
+    # ---- device-resident timed region -------------------------------------------------
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = capi.kernel_launches()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            for s in range(args.steps):
+                flush.zero_()                       # L2 flush between timed steps (not timed)
+                starts[s].record(stream)
+                plain.step(1)
+                stops[s].record(stream)
+        torch.cuda.synchronize()
+        launches = capi.kernel_launches() - launches0
+        t_steps = [a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops)]
+        t_total = float(sum(t_steps))
+        # ---- per-stage kernel durations for the roofline (same stream, events) -------
+        plain.set_timing(True)
+        with torch.cuda.stream(stream):
+            for s in range(max(3, args.steps // 4)):
+                flush.zero_()
+                for st in range(4):
+                    plain.rk_substep(st)
+        k_time, k_launches, _ = plain.timings()
+        plain.set_timing(False)
+    if world > 1:
+        t = torch.tensor([t_total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+    value = 4.0 * N * args.steps * world / t_total
+
+    # ---- end to end through the C ABI with pinned host buffers --------------------------
+    H_host = torch.from_numpy(np.ascontiguousarray(pm.H_init, dtype=dt_np).reshape(-1)).pin_memory()
+    H_out = torch.empty_like(H_host).pin_memory()
+    nbytes = H_host.numel() * H_host.element_size()
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(2):
+        plain.set_state_ptr(H_host.data_ptr())
+        plain.step(1)
+        plain.get_state_ptr(H_out.data_ptr())
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        plain.set_state_ptr(H_host.data_ptr())
+        plain.step(1)
+        plain.get_state_ptr(H_out.data_ptr())     # synchronises
+    t_e2e = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([t_e2e], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = 4.0 * N * e2e_steps * world / t_e2e
+    finite = bool(np.isfinite(H_out.numpy()).all())
+
+    # ---- roofline of the fused stage kernel ------------------------------------------
+    peak, peak_kind = measured_peak_hbm()
+    t_kernel = k_time / max(k_launches, 1)
+    achieved = ALG_BYTES[prec] * N / t_kernel / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                "kernel": "swe::stage_kernel", "kernel_us": round(t_kernel * 1e6, 2),
+                "alg_bytes_per_node_stage": ALG_BYTES[prec]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_sample(d, prec)
+        except Exception as e:            # reported, not fatal
+            cpu = {"value": None, "unit": "node-stage updates/s", "error": str(e)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": "node-stage updates/s (RK4 + RBF-FD stage, plain form)",
+            "value": value, "unit": "node-stage updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32",
+            "data": "synthetic (seeded icosahedral grid, PHS RBF-FD weights, TC5 Gaussian-mountain ICs)",
+            "config": {"workload": args.workload, "description": desc, "nodes": N, "nnbr": 31, "dt": d.dt,
+                       "layout": "CFDL", "rcm": True, "parallelism": f"replicas x{world}",
+                       "l2": "flushed (256 MB write) between timed steps"},
+            "e2e": {"value": e2e, "unit": "node-stage updates/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "state_finite": finite,
+        }
+        print(json.dumps(line), flush=True)
+    plain.finalize()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

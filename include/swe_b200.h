@@ -1,0 +1,151 @@
+/*
+ * swe_b200.h -- C ABI of the B200 (sm_100a) implementation of the RBF-FD
+ * shallow-water RK4 hot path of cenamiller/RBF-FD-SWE.
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *   RK_substep(H, K, F, D, id)     swe_code/main/include/rk4_rbffd_swe.h:8,
+ *                                  swe_code/main/rk4_rbffd_swe.c:30-72
+ *   eval_RHS_swe(K, F)             swe_code/main/rk4_rbffd_swe.c:189-362
+ *                                  (external linkage, not in a header)
+ *   RK_substep_ocl(..., substep)   swe_code/ocl/RK_ocl.c:9-51 (device precedent:
+ *                                  buffers set once, state device-resident)
+ *   static data of PSMD_struct     swe_code/main/include/swe_config.h:187-233
+ *   layout macros DM_LIN_ID, VECT_LIN_ID, SVM_LIN_ID
+ *                                  swe_code/main/include/swe_config.h:31-54
+ *
+ * Conventions.  Every entry point returns an int status (SWE_OK = 0) and never
+ * exits the process; swe_cuda_last_error() describes the last failure.  Host
+ * arrays are owned by the caller and use the caller's compile-time layout
+ * (SWE_LAYOUT_* flags and the SIMD tile width), exactly as the reference's
+ * LPSMD holds them.  The library owns all device memory and one CUDA stream;
+ * calls come from one host thread.  fsize = sizeof(fType): 8 (FP64) or 4 (FP32),
+ * which selects the arithmetic precision of the plain form.
+ */
+#ifndef SWE_B200_H
+#define SWE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SWE_OK 0
+#define SWE_ERR_ARG 1       /* invalid argument or size                        */
+#define SWE_ERR_STATE 2     /* call out of order (e.g. step before init)       */
+#define SWE_ERR_CUDA 3      /* CUDA runtime failure                            */
+#define SWE_ERR_NOMEM 4     /* device allocation failed or budget exceeded     */
+#define SWE_ERR_INDEX 5     /* stencil index outside the patch                 */
+#define SWE_ERR_TIMEOUT 6   /* a bounded device wait ran out                   */
+#define SWE_ERR_NONFINITE 7 /* NaN/Inf detected by a watchdog reduction        */
+#define SWE_ERR_CANCELLED 8 /* request cancelled                               */
+
+/* layout flags: the reference's USE_CFDL / USE_SFDL compile options */
+#define SWE_LAYOUT_CFDL 1
+#define SWE_LAYOUT_SFDL 2
+
+const char* swe_cuda_last_error(void);
+
+/* Selects the CUDA device for the calling thread's subsequent calls (one
+ * process per GPU: call with the local rank before swe_cuda_init). */
+int swe_cuda_select_device(int device);
+
+/* ---------------------------------------------------------------------------
+ * Plain drop-in form (one state, FP64 or FP32)
+ * ------------------------------------------------------------------------- */
+
+/* Uploads the static model data of one patch and canonicalises it for the
+ * device.  Replaces the reference's implicit global LPSMD (rk4_rbffd_swe.c:19)
+ * and the OpenCL buffer setup (ocl/buffers.c:26-49, main.c:318-322).
+ * Arrays are laid out as swe_config.h:31-54 prescribes for `layout` with tile
+ * width `simd_length`: x, y, z, f, ghm [compute_size]; p_u, p_v, p_w, gradghm
+ * by VECT_LIN_ID; idx, Dx, Dy, Dz, L by DM_LIN_ID with row length padded_nnbr.
+ * idx is 0-based and patch-local.  Weight columns j >= nnbr are never read
+ * (the reference pads them by replicating the last column,
+ * layout/matrix_transformations.c:20-21).  Requires nnbr <= 32.  Re-init
+ * replaces the previous patch. */
+int swe_cuda_init(int fsize, int layout, int simd_length,
+                  int compute_size, int patch_size, int compute_pid_s,
+                  int nnbr, int padded_nnbr, double gh0, double dt,
+                  const void* x, const void* y, const void* z, const void* f, const void* ghm,
+                  const void* p_u, const void* p_v, const void* p_w, const void* gradghm,
+                  const int* idx, const void* Dx, const void* Dy, const void* Dz, const void* L);
+
+/* State transfer, H of patch_size*4 values in the init layout (SVM_LIN_ID).
+ * set_state also resets the RK registers (K <- H), as the reference's time
+ * loop does at the start of each attempt (main.c:297, :308-314). */
+int swe_cuda_set_state(const void* H);
+int swe_cuda_get_state(void* H);
+
+/* Parity entry point with eval_RHS_swe semantics: F = RHS(K).  K holds
+ * patch_size*4 and F compute_size*4 values, both host pointers in the init
+ * layout.  Synchronous. */
+int swe_cuda_eval_rhs(const void* K, void* F);
+
+/* One RK4 stage on the device-resident state; same stage semantics as
+ * RK_substep (rk4_rbffd_swe.c:30-72).  The RHS, the stage combine and the
+ * D/K (or H) update are one fused kernel per stage.  Asynchronous. */
+int swe_cuda_rk_substep(int substep_id);
+
+/* nsteps full RK4 steps (4 stages each) from a captured CUDA graph.
+ * Asynchronous; requires compute_pid_s == 0 and patch_size == compute_size
+ * (one GPU, no halo exchange). */
+int swe_cuda_step(int nsteps);
+
+/* Waits for all work of the library's stream. */
+int swe_cuda_sync(void);
+
+/* Timing of the fused stage kernels, measured with CUDA events on the
+ * library's stream while enabled.  out[0] = seconds of stage kernels since
+ * the last reset, out[1] = stage launches, out[2] = seconds of the last
+ * swe_cuda_step call.  Reading synchronises. */
+int swe_cuda_set_timing(int enabled);
+int swe_cuda_last_timings(double* out);
+
+/* The library's CUDA stream (a cudaStream_t) for callers that want to order
+ * their own work or events against it. */
+void* swe_cuda_stream(void);
+
+/* FP64 (mass, energy) of the device state with equal node areas 4*pi/n:
+ * mass = sum A (h + gh0 - ghm), energy = sum A (0.5 (h+gh0-ghm)|u|^2 + 0.5 (h+gh0)^2). */
+int swe_cuda_invariants(double* mass_energy);
+
+/* Frees all device memory and the stream. */
+int swe_cuda_finalize(void);
+
+/* ---------------------------------------------------------------------------
+ * Host utilities (no device work)
+ * ------------------------------------------------------------------------- */
+
+/* Reverse Cuthill-McKee node order of the stencil graph, the same permutation
+ * as the reference's rcm_mapping (swe_code/rcm/rcm.c:9-62): mapping[new] = old.
+ * idx is [n][nnbr], 0-based, self first. */
+int swe_host_rcm_mapping(int n, int nnbr, const int* idx, int* mapping);
+
+/* Number of kernels this library has launched since load (all forms). */
+long long swe_b200_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+/* Convenience for reference host code that already includes swe_config.h:
+ * forwards one PSMD_struct with the build's own layout options. */
+#if defined(SWE_CONFIG_H) && !defined(__cplusplus)
+static inline int swe_cuda_init_psmd(const PSMD_struct* p) {
+    int layout = 0;
+#ifdef USE_CFDL
+    layout |= SWE_LAYOUT_CFDL;
+#endif
+#ifdef USE_SFDL
+    layout |= SWE_LAYOUT_SFDL;
+#endif
+    return swe_cuda_init((int)sizeof(fType), layout, SIMD_LENGTH, p->compute_size, p->patch_size,
+                         p->compute_pid_s, p->Nnbr, p->padded_Nnbr, (double)p->gh0, (double)p->dt,
+                         p->x, p->y, p->z, p->f, p->ghm, p->p_u, p->p_v, p->p_w, p->gradghm,
+                         p->idx, p->Dx, p->Dy, p->Dz, p->L);
+}
+#endif
+
+#endif /* SWE_B200_H */

@@ -1,0 +1,537 @@
+// Plain drop-in form: the swe_cuda_* entry points of include/swe_b200.h.
+//
+// Host side of the fused stage kernel: canonicalisation of the caller's
+// (reference-layout) static data into the device layout, device-resident RK
+// registers H, K (ping-pong), D, the four stage launches of RK_substep
+// (swe_code/main/rk4_rbffd_swe.c:30-72) and a captured CUDA graph for whole
+// steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "stage_kernel.cuh"
+
+namespace swe {
+
+static thread_local std::string g_err;
+static std::atomic<long long> g_launches{0};
+
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+void count_launch(long long n) { g_launches += n; }
+
+// ---------------------------------------------------------------------------
+// Packing of the static data (host) -----------------------------------------
+
+// Weights of node i, slot j = 8m + k, packed in 16-byte units at
+// unit ((i*4 + m)*U + q)*8 + k; unit q of FP64 holds (Dx, Dy) or (Dz, L),
+// the single FP32 unit holds (Dx, Dy, Dz, L).  Slots j >= nnbr are zero.
+template <typename T>
+static void pack_weights(const CallerLayout& cl, int n, int nnbr, const T* Dx, const T* Dy, const T* Dz,
+                         const T* L, std::vector<T>& out) {
+    constexpr int U = Quad<T>::kUnits;
+    constexpr int per_unit = 16 / sizeof(T);
+    out.assign((size_t)n * kSlotChunks * U * 8 * per_unit, T(0));
+    const T* ops[4] = {Dx, Dy, Dz, L};
+    for (long i = 0; i < n; ++i)
+        for (int j = 0; j < nnbr; ++j) {
+            const int m = j / 8, k = j % 8;
+            const long dm = cl.dm(i, j);
+            for (int op = 0; op < 4; ++op) {
+                const int q = op / per_unit, e = op % per_unit;
+                const size_t unit = (((size_t)i * kSlotChunks + m) * U + q) * 8 + k;
+                out[unit * per_unit + e] = ops[op][dm];
+            }
+        }
+}
+
+// idx of node i for lane k: int4 (slots k, k+8, k+16, k+24); padded slots
+// point at the node's own row (their weights are zero).
+static int pack_idx(const CallerLayout& cl, int n, int rows, int pid0, int nnbr, const int* idx,
+                    std::vector<int>& out) {
+    out.assign((size_t)n * kSlots, 0);
+    for (long i = 0; i < n; ++i)
+        for (int j = 0; j < kSlots; ++j) {
+            int p = (int)i + pid0;
+            if (j < nnbr) {
+                p = idx[cl.dm(i, j)];
+                if (p < 0 || p >= rows) {
+                    set_error("idx[node %ld][nbr %d] = %d outside the patch [0, %d)", i, j, p, rows);
+                    return SWE_ERR_INDEX;
+                }
+            }
+            out[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)] = p;
+        }
+    return SWE_OK;
+}
+
+template <typename T>
+static void pack_points(const CallerLayout& cl, int n, const T* x, const T* y, const T* z, const T* f,
+                        const T* ghm, const T* pu, const T* pv, const T* pw, const T* gg, std::vector<T>& out) {
+    out.assign((size_t)n * kPointStride, T(0));
+    for (long i = 0; i < n; ++i) {
+        T* r = &out[(size_t)i * kPointStride];
+        r[PT_X] = x[i]; r[PT_Y] = y[i]; r[PT_Z] = z[i]; r[PT_F] = f[i]; r[PT_GHM] = ghm[i];
+        for (int c = 0; c < 3; ++c) {
+            const long v = cl.vect(i, c);
+            r[PT_PU + c] = pu[v]; r[PT_PV + c] = pv[v]; r[PT_PW + c] = pw[v]; r[PT_GG + c] = gg[v];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Device helpers ---------------------------------------------------------------
+
+// caller layout (SVM_LIN_ID) <-> node-major rows; dir 0: caller -> canonical
+template <typename T>
+__global__ void permute_state_kernel(const T* __restrict__ src, T* __restrict__ dst, long rows,
+                                     CallerLayout cl, int dir) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= rows * 4) return;
+    const long p = t >> 2, sv = t & 3;
+    const long c = cl.svm(p, sv);
+    if (dir == 0) dst[t] = src[c];
+    else dst[c] = src[t];
+}
+
+// FP64 mass/energy sums over n nodes (equal areas 4*pi/n).
+template <typename T>
+__global__ void invariants_kernel(const T* __restrict__ H, const T* __restrict__ PT, int n, double gh0,
+                                  double* __restrict__ out) {
+    double mass = 0.0, energy = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double u = H[4 * i], v = H[4 * i + 1], w = H[4 * i + 2], h = H[4 * i + 3];
+        const double phi = h + gh0;
+        const double thick = phi - (double)PT[i * kPointStride + PT_GHM];
+        mass += thick;
+        energy += 0.5 * thick * (u * u + v * v + w * w) + 0.5 * phi * phi;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mass += __shfl_xor_sync(0xffffffffu, mass, o);
+        energy += __shfl_xor_sync(0xffffffffu, energy, o);
+    }
+    __shared__ double sm[2][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { sm[0][warp] = mass; sm[1][warp] = energy; }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        mass = lane < nw ? sm[0][lane] : 0.0;
+        energy = lane < nw ? sm[1][lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            mass += __shfl_xor_sync(0xffffffffu, mass, o);
+            energy += __shfl_xor_sync(0xffffffffu, energy, o);
+        }
+        if (lane == 0) { atomicAdd(out, mass); atomicAdd(out + 1, energy); }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Plain solver ---------------------------------------------------------------
+
+struct Plain {
+    bool ready = false;
+    int fsize = 8, n = 0, rows = 0, pid0 = 0, nnbr = 0;
+    CallerLayout cl;
+    double gh0 = 0, dt = 0;
+    void *W = nullptr, *PT = nullptr, *H = nullptr, *Ka = nullptr, *Kb = nullptr, *D = nullptr, *F = nullptr,
+         *Kx = nullptr, *raw = nullptr;
+    int* idx = nullptr;
+    double* inv = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int grid = 0;
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;   // pairs (start, stop) of timed launches
+    size_t ev_used = 0;
+    double t_step_last = 0.0;
+    cudaEvent_t step_ev[2] = {nullptr, nullptr};
+    bool step_timed = false;
+
+    size_t fbytes(long count) const { return (size_t)count * fsize; }
+
+    void release() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        for (void* p : {W, PT, H, Ka, Kb, D, F, Kx, raw}) if (p) cudaFree(p);
+        if (idx) cudaFree(idx);
+        if (inv) cudaFree(inv);
+        W = PT = H = Ka = Kb = D = F = Kx = raw = nullptr;
+        idx = nullptr;
+        inv = nullptr;
+        for (auto e : ev) cudaEventDestroy(e);
+        ev.clear();
+        ev_used = 0;
+        for (auto& e : step_ev) { if (e) cudaEventDestroy(e); e = nullptr; }
+        if (stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+        ready = false;
+    }
+
+    int timed_begin(cudaEvent_t* pair) {
+        if (!timing) return SWE_OK;
+        if (ev_used + 2 > ev.size()) {
+            for (int t = 0; t < 64; ++t) {
+                cudaEvent_t e;
+                SWE_CUDA_TRY(cudaEventCreate(&e));
+                ev.push_back(e);
+            }
+        }
+        pair[0] = ev[ev_used];
+        pair[1] = ev[ev_used + 1];
+        ev_used += 2;
+        SWE_CUDA_TRY(cudaEventRecord(pair[0], stream));
+        return SWE_OK;
+    }
+
+    template <typename T>
+    StageArgs<T> args(int mode) const {
+        StageArgs<T> a{};
+        a.n = n;
+        a.pid0 = pid0;
+        a.idx = reinterpret_cast<const int4*>(idx);
+        a.W = reinterpret_cast<const uint4*>(W);
+        a.PT = reinterpret_cast<const T*>(PT);
+        a.H = reinterpret_cast<T*>(H);
+        a.D = reinterpret_cast<T*>(D);
+        a.F = reinterpret_cast<T*>(F);
+        a.gh0 = (T)gh0;
+        const T dtT = (T)dt;
+        a.dt6 = (double)dtT / 6.0;
+        switch (mode) {
+            case 0: a.Kin = reinterpret_cast<const T*>(H); a.Kout = reinterpret_cast<T*>(Ka); a.c = (T)(dtT / 2.0); break;
+            case 1: a.Kin = reinterpret_cast<const T*>(Ka); a.Kout = reinterpret_cast<T*>(Kb); a.c = (T)(dtT / 2.0); break;
+            case 2: a.Kin = reinterpret_cast<const T*>(Kb); a.Kout = reinterpret_cast<T*>(Ka); a.c = dtT; break;
+            case 3: a.Kin = reinterpret_cast<const T*>(Ka); a.Kout = nullptr; a.c = dtT; break;
+            default: a.Kin = reinterpret_cast<const T*>(Kx); a.Kout = nullptr; a.c = T(0); break;
+        }
+        return a;
+    }
+
+    template <typename T>
+    void launch_t(int mode) {
+        const StageArgs<T> a = args<T>(mode);
+        switch (mode) {
+            case 0: stage_kernel<T, kStage0><<<grid, kStageThreads, 0, stream>>>(a); break;
+            case 1: stage_kernel<T, kStage1><<<grid, kStageThreads, 0, stream>>>(a); break;
+            case 2: stage_kernel<T, kStage2><<<grid, kStageThreads, 0, stream>>>(a); break;
+            case 3: stage_kernel<T, kStage3><<<grid, kStageThreads, 0, stream>>>(a); break;
+            default: stage_kernel<T, kEvalOnly><<<grid, kStageThreads, 0, stream>>>(a); break;
+        }
+    }
+
+    int launch(int mode) {
+        cudaEvent_t pair[2] = {nullptr, nullptr};
+        SWE_TRY(timed_begin(pair));
+        if (fsize == 8) launch_t<double>(mode);
+        else launch_t<float>(mode);
+        count_launch();
+        SWE_CUDA_TRY(cudaGetLastError());
+        if (pair[1]) SWE_CUDA_TRY(cudaEventRecord(pair[1], stream));
+        return SWE_OK;
+    }
+
+    int build_graph() {
+        cudaGraph_t g;
+        SWE_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        const bool was = timing;
+        timing = false;
+        for (int s = 0; s < 4; ++s) {
+            if (fsize == 8) launch_t<double>(s);
+            else launch_t<float>(s);
+        }
+        timing = was;
+        SWE_CUDA_TRY(cudaStreamEndCapture(stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            set_error("cudaGraphInstantiate: %s", cudaGetErrorString(e));
+            graph = nullptr;
+            return SWE_ERR_CUDA;
+        }
+        return SWE_OK;
+    }
+};
+
+static Plain g_plain;
+
+template <typename T>
+static int upload_static(Plain& P, const void* x, const void* y, const void* z, const void* f, const void* ghm,
+                         const void* pu, const void* pv, const void* pw, const void* gg, const int* idx,
+                         const void* Dx, const void* Dy, const void* Dz, const void* L) {
+    std::vector<T> wbuf, pbuf;
+    std::vector<int> ibuf;
+    pack_weights<T>(P.cl, P.n, P.nnbr, (const T*)Dx, (const T*)Dy, (const T*)Dz, (const T*)L, wbuf);
+    SWE_TRY(pack_idx(P.cl, P.n, P.rows, P.pid0, P.nnbr, idx, ibuf));
+    pack_points<T>(P.cl, P.n, (const T*)x, (const T*)y, (const T*)z, (const T*)f, (const T*)ghm, (const T*)pu,
+                   (const T*)pv, (const T*)pw, (const T*)gg, pbuf);
+    SWE_CUDA_TRY(cudaMalloc(&P.W, wbuf.size() * sizeof(T)));
+    SWE_CUDA_TRY(cudaMalloc(&P.idx, ibuf.size() * sizeof(int)));
+    SWE_CUDA_TRY(cudaMalloc(&P.PT, pbuf.size() * sizeof(T)));
+    SWE_CUDA_TRY(cudaMemcpy(P.W, wbuf.data(), wbuf.size() * sizeof(T), cudaMemcpyHostToDevice));
+    SWE_CUDA_TRY(cudaMemcpy(P.idx, ibuf.data(), ibuf.size() * sizeof(int), cudaMemcpyHostToDevice));
+    SWE_CUDA_TRY(cudaMemcpy(P.PT, pbuf.data(), pbuf.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return SWE_OK;
+}
+
+static int require_ready() {
+    if (!g_plain.ready) {
+        set_error("swe_cuda_init has not been called");
+        return SWE_ERR_STATE;
+    }
+    return SWE_OK;
+}
+
+static int permute_state(const void* src, void* dst, int dir) {
+    Plain& P = g_plain;
+    const long total = (long)P.rows * 4;
+    const int threads = 256;
+    const int blocks = ceil_div(total, threads);
+    if (P.fsize == 8)
+        permute_state_kernel<double><<<blocks, threads, 0, P.stream>>>((const double*)src, (double*)dst, P.rows, P.cl, dir);
+    else
+        permute_state_kernel<float><<<blocks, threads, 0, P.stream>>>((const float*)src, (float*)dst, P.rows, P.cl, dir);
+    count_launch();
+    SWE_CUDA_TRY(cudaGetLastError());
+    return SWE_OK;
+}
+
+}  // namespace swe
+
+using namespace swe;
+
+extern "C" {
+
+const char* swe_cuda_last_error(void) { return g_err.c_str(); }
+
+long long swe_b200_kernel_launches(void) { return g_launches.load(); }
+
+int swe_cuda_select_device(int device) {
+    SWE_CUDA_TRY(cudaSetDevice(device));
+    return SWE_OK;
+}
+
+int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int patch_size, int compute_pid_s,
+                  int nnbr, int padded_nnbr, double gh0, double dt, const void* x, const void* y, const void* z,
+                  const void* f, const void* ghm, const void* p_u, const void* p_v, const void* p_w,
+                  const void* gradghm, const int* idx, const void* Dx, const void* Dy, const void* Dz,
+                  const void* L) {
+    if (fsize != 8 && fsize != 4) { set_error("fsize must be 8 or 4, got %d", fsize); return SWE_ERR_ARG; }
+    if (layout & ~(SWE_LAYOUT_CFDL | SWE_LAYOUT_SFDL)) { set_error("unknown layout flags %d", layout); return SWE_ERR_ARG; }
+    if (compute_size <= 0 || patch_size < compute_size || compute_pid_s < 0 ||
+        compute_pid_s + compute_size > patch_size) {
+        set_error("bad patch: compute_size %d patch_size %d compute_pid_s %d", compute_size, patch_size, compute_pid_s);
+        return SWE_ERR_ARG;
+    }
+    if (nnbr <= 0 || nnbr > kSlots || padded_nnbr < nnbr) {
+        set_error("nnbr %d / padded_nnbr %d unsupported (need 1 <= nnbr <= %d <= padded)", nnbr, padded_nnbr, kSlots);
+        return SWE_ERR_ARG;
+    }
+    if (simd_length <= 0 || ((layout & SWE_LAYOUT_SFDL) && compute_size % simd_length) ||
+        (!(layout & SWE_LAYOUT_CFDL) && patch_size % simd_length)) {
+        set_error("tile width %d does not divide the padded sizes", simd_length);
+        return SWE_ERR_ARG;
+    }
+    if (!x || !y || !z || !f || !ghm || !p_u || !p_v || !p_w || !gradghm || !idx || !Dx || !Dy || !Dz || !L) {
+        set_error("null static array");
+        return SWE_ERR_ARG;
+    }
+    Plain& P = g_plain;
+    P.release();
+    P.fsize = fsize;
+    P.n = compute_size;
+    P.rows = patch_size;
+    P.pid0 = compute_pid_s;
+    P.nnbr = nnbr;
+    P.cl.layout = layout;
+    P.cl.S = simd_length;
+    P.cl.pnbr = padded_nnbr;
+    P.gh0 = gh0;
+    P.dt = dt;
+    SWE_CUDA_TRY(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
+    int st = fsize == 8 ? upload_static<double>(P, x, y, z, f, ghm, p_u, p_v, p_w, gradghm, idx, Dx, Dy, Dz, L)
+                        : upload_static<float>(P, x, y, z, f, ghm, p_u, p_v, p_w, gradghm, idx, Dx, Dy, Dz, L);
+    if (st != SWE_OK) { P.release(); return st; }
+    const size_t srow = P.fbytes(4L * P.rows), scomp = P.fbytes(4L * P.n);
+    SWE_CUDA_TRY(cudaMalloc(&P.H, srow));
+    SWE_CUDA_TRY(cudaMalloc(&P.Ka, srow));
+    SWE_CUDA_TRY(cudaMalloc(&P.Kb, srow));
+    SWE_CUDA_TRY(cudaMalloc(&P.Kx, srow));
+    SWE_CUDA_TRY(cudaMalloc(&P.raw, srow));
+    SWE_CUDA_TRY(cudaMalloc(&P.D, scomp));
+    SWE_CUDA_TRY(cudaMalloc(&P.F, scomp));
+    SWE_CUDA_TRY(cudaMalloc(&P.inv, 2 * sizeof(double)));
+    SWE_CUDA_TRY(cudaMemset(P.H, 0, srow));
+    SWE_CUDA_TRY(cudaMemset(P.Ka, 0, srow));
+    SWE_CUDA_TRY(cudaMemset(P.Kb, 0, srow));
+    SWE_CUDA_TRY(cudaMemset(P.D, 0, scomp));
+    int dev = 0, sms = 0, per_sm = 0;
+    SWE_CUDA_TRY(cudaGetDevice(&dev));
+    SWE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (fsize == 8)
+        SWE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel<double, kStage1>, kStageThreads, 0));
+    else
+        SWE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel<float, kStage1>, kStageThreads, 0));
+    const int want = ceil_div(P.n, 4 * kStageWarps);
+    P.grid = std::max(1, std::min(want, sms * std::max(per_sm, 1)));
+    P.ready = true;
+    if ((st = P.build_graph()) != SWE_OK) return st;
+    return SWE_OK;
+}
+
+int swe_cuda_set_state(const void* Hh) {
+    SWE_TRY(require_ready());
+    if (!Hh) { set_error("null H"); return SWE_ERR_ARG; }
+    Plain& P = g_plain;
+    const size_t bytes = P.fbytes(4L * P.rows);
+    SWE_CUDA_TRY(cudaMemcpyAsync(P.raw, Hh, bytes, cudaMemcpyHostToDevice, P.stream));
+    SWE_TRY(permute_state(P.raw, P.H, 0));
+    SWE_CUDA_TRY(cudaMemcpyAsync(P.Ka, P.H, bytes, cudaMemcpyDeviceToDevice, P.stream));
+    SWE_CUDA_TRY(cudaMemcpyAsync(P.Kb, P.H, bytes, cudaMemcpyDeviceToDevice, P.stream));
+    return SWE_OK;
+}
+
+int swe_cuda_get_state(void* Hh) {
+    SWE_TRY(require_ready());
+    if (!Hh) { set_error("null H"); return SWE_ERR_ARG; }
+    Plain& P = g_plain;
+    const size_t bytes = P.fbytes(4L * P.rows);
+    SWE_TRY(permute_state(P.H, P.raw, 1));
+    SWE_CUDA_TRY(cudaMemcpyAsync(Hh, P.raw, bytes, cudaMemcpyDeviceToHost, P.stream));
+    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    return SWE_OK;
+}
+
+int swe_cuda_eval_rhs(const void* K, void* Fh) {
+    SWE_TRY(require_ready());
+    if (!K || !Fh) { set_error("null K or F"); return SWE_ERR_ARG; }
+    Plain& P = g_plain;
+    SWE_CUDA_TRY(cudaMemcpyAsync(P.raw, K, P.fbytes(4L * P.rows), cudaMemcpyHostToDevice, P.stream));
+    SWE_TRY(permute_state(P.raw, P.Kx, 0));
+    SWE_TRY(P.launch(kEvalOnly));
+    // F has compute_size rows in the caller's SVM layout (compute-local ids)
+    CallerLayout cl = P.cl;
+    const long total = 4L * P.n;
+    if (P.fsize == 8)
+        permute_state_kernel<double><<<ceil_div(total, 256), 256, 0, P.stream>>>((const double*)P.F, (double*)P.raw, P.n, cl, 1);
+    else
+        permute_state_kernel<float><<<ceil_div(total, 256), 256, 0, P.stream>>>((const float*)P.F, (float*)P.raw, P.n, cl, 1);
+    count_launch();
+    SWE_CUDA_TRY(cudaGetLastError());
+    SWE_CUDA_TRY(cudaMemcpyAsync(Fh, P.raw, P.fbytes(total), cudaMemcpyDeviceToHost, P.stream));
+    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    return SWE_OK;
+}
+
+int swe_cuda_rk_substep(int substep_id) {
+    SWE_TRY(require_ready());
+    if (substep_id < 0 || substep_id > 3) { set_error("substep_id %d not in 0..3", substep_id); return SWE_ERR_ARG; }
+    Plain& P = g_plain;
+    if (P.pid0 != 0 || P.rows != P.n) {
+        set_error("time stepping needs compute_pid_s == 0 and patch_size == compute_size (no halos)");
+        return SWE_ERR_ARG;
+    }
+    return P.launch(substep_id);
+}
+
+int swe_cuda_step(int nsteps) {
+    SWE_TRY(require_ready());
+    Plain& P = g_plain;
+    if (nsteps < 0) { set_error("nsteps < 0"); return SWE_ERR_ARG; }
+    if (P.pid0 != 0 || P.rows != P.n) {
+        set_error("time stepping needs compute_pid_s == 0 and patch_size == compute_size (no halos)");
+        return SWE_ERR_ARG;
+    }
+    if (P.timing) {
+        for (auto& e : P.step_ev) if (!e) SWE_CUDA_TRY(cudaEventCreate(&e));
+        SWE_CUDA_TRY(cudaEventRecord(P.step_ev[0], P.stream));
+    }
+    for (int s = 0; s < nsteps; ++s) SWE_CUDA_TRY(cudaGraphLaunch(P.graph, P.stream));
+    count_launch(4LL * nsteps);
+    if (P.timing) {
+        SWE_CUDA_TRY(cudaEventRecord(P.step_ev[1], P.stream));
+        P.step_timed = true;
+    }
+    return SWE_OK;
+}
+
+int swe_cuda_sync(void) {
+    SWE_TRY(require_ready());
+    SWE_CUDA_TRY(cudaStreamSynchronize(g_plain.stream));
+    return SWE_OK;
+}
+
+int swe_cuda_set_timing(int enabled) {
+    SWE_TRY(require_ready());
+    Plain& P = g_plain;
+    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    P.timing = enabled != 0;
+    P.ev_used = 0;
+    P.step_timed = false;
+    return SWE_OK;
+}
+
+int swe_cuda_last_timings(double* out) {
+    SWE_TRY(require_ready());
+    if (!out) { set_error("null out"); return SWE_ERR_ARG; }
+    Plain& P = g_plain;
+    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    double total = 0.0;
+    for (size_t e = 0; e < P.ev_used; e += 2) {
+        float ms = 0.f;
+        SWE_CUDA_TRY(cudaEventElapsedTime(&ms, P.ev[e], P.ev[e + 1]));
+        total += ms * 1e-3;
+    }
+    out[0] = total;
+    out[1] = (double)(P.ev_used / 2);
+    out[2] = 0.0;
+    if (P.step_timed) {
+        float ms = 0.f;
+        SWE_CUDA_TRY(cudaEventElapsedTime(&ms, P.step_ev[0], P.step_ev[1]));
+        out[2] = ms * 1e-3;
+    }
+    P.ev_used = 0;
+    return SWE_OK;
+}
+
+void* swe_cuda_stream(void) { return g_plain.ready ? (void*)g_plain.stream : nullptr; }
+
+int swe_cuda_invariants(double* me) {
+    SWE_TRY(require_ready());
+    if (!me) { set_error("null out"); return SWE_ERR_ARG; }
+    Plain& P = g_plain;
+    SWE_CUDA_TRY(cudaMemsetAsync(P.inv, 0, 2 * sizeof(double), P.stream));
+    const int blocks = std::min(ceil_div(P.n, 256), 1184);
+    if (P.fsize == 8)
+        invariants_kernel<double><<<blocks, 256, 0, P.stream>>>((const double*)P.H, (const double*)P.PT, P.n, P.gh0, P.inv);
+    else
+        invariants_kernel<float><<<blocks, 256, 0, P.stream>>>((const float*)P.H, (const float*)P.PT, P.n, (double)(float)P.gh0, P.inv);
+    count_launch();
+    SWE_CUDA_TRY(cudaGetLastError());
+    SWE_CUDA_TRY(cudaMemcpyAsync(me, P.inv, 2 * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    const double area = 4.0 * 3.14159265358979323846 / (double)P.n;
+    me[0] *= area;
+    me[1] *= area;
+    return SWE_OK;
+}
+
+int swe_cuda_finalize(void) {
+    if (g_plain.stream) cudaStreamSynchronize(g_plain.stream);
+    g_plain.release();
+    return SWE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,194 @@
+"""ctypes binding of the C ABI in include/swe_b200.h (lib/libswe_b200.so).
+
+This is the Python face of the drop-in boundary: the same entry points a C
+host (the reference's main.c with its SWE_USE_CUDA branch) calls.  Arrays are
+numpy host buffers in the caller's layout.  There is no fallback: if the
+shared library is missing or a call fails, an exception says so.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libswe_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "swe_b200.h")
+
+SWE_LAYOUT_CFDL = 1
+SWE_LAYOUT_SFDL = 2
+STATUS = {0: "SWE_OK", 1: "SWE_ERR_ARG", 2: "SWE_ERR_STATE", 3: "SWE_ERR_CUDA", 4: "SWE_ERR_NOMEM",
+          5: "SWE_ERR_INDEX", 6: "SWE_ERR_TIMEOUT", 7: "SWE_ERR_NONFINITE", 8: "SWE_ERR_CANCELLED"}
+
+_lib = None
+
+
+class SweError(RuntimeError):
+    def __init__(self, fn: str, status: int, msg: str):
+        super().__init__(f"{fn} -> {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def declared_symbols() -> list[str]:
+    """Every function name include/swe_b200.h declares with C linkage."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    body = text.split('extern "C" {', 1)[1].split("#ifdef __cplusplus\n}", 1)[0]
+    return sorted(set(re.findall(r"\b(swe_\w+)\s*\(", body)))
+
+
+def load() -> ctypes.CDLL:
+    """Load lib/libswe_b200.so (once); raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: the sm_100a library was not built "
+                           f"(run __graft_entry__.build() or make -C {PKG_DIR})")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    lib.swe_cuda_last_error.restype = ctypes.c_char_p
+    lib.swe_b200_kernel_launches.restype = ctypes.c_longlong
+    lib.swe_cuda_init.argtypes = [i, i, i, i, i, i, i, i, d, d] + [vp] * 14
+    for name in ("swe_cuda_set_state", "swe_cuda_get_state", "swe_cuda_last_timings", "swe_cuda_invariants"):
+        getattr(lib, name).argtypes = [vp]
+    lib.swe_cuda_eval_rhs.argtypes = [vp, vp]
+    lib.swe_cuda_rk_substep.argtypes = [i]
+    lib.swe_cuda_step.argtypes = [i]
+    lib.swe_cuda_set_timing.argtypes = [i]
+    lib.swe_cuda_stream.restype = vp
+    _lib = lib
+    return lib
+
+
+def check(fn: str, status: int) -> None:
+    if status != 0:
+        raise SweError(fn, status, load().swe_cuda_last_error().decode(errors="replace"))
+
+
+def kernel_launches() -> int:
+    return int(load().swe_b200_kernel_launches())
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class PSMD(ctypes.Structure):
+    """Mirror of the reference's PSMD_struct (swe_config.h:187-233) with pointers
+    left untyped; gh0 and dt are fType, so two variants exist."""
+
+    _common_head = [(n, ctypes.c_int) for n in (
+        "lnbr_rank", "rnbr_rank", "patch_size", "compute_size", "lhalo_size", "rhalo_size",
+        "halo_pid_s", "compute_pid_s", "compute_pid_e", "halo_pid_e", "lnbr_halo_size",
+        "rnbr_halo_size", "lnbr_halo_pid_e", "rnbr_halo_pid_s")] + \
+        [(n, ctypes.c_void_p) for n in ("x", "y", "z", "f")]
+    _common_tail = [(n, ctypes.c_void_p) for n in ("ghm", "gradghm", "p_u", "p_v", "p_w")] + \
+        [("Nnbr", ctypes.c_int), ("padded_Nnbr", ctypes.c_int)] + \
+        [(n, ctypes.c_void_p) for n in ("idx", "Dx", "Dy", "Dz", "L")]
+
+
+class PSMD64(ctypes.Structure):
+    _fields_ = PSMD._common_head + [("gh0", ctypes.c_double), ("dt", ctypes.c_double)] + PSMD._common_tail
+
+
+class PSMD32(ctypes.Structure):
+    _fields_ = PSMD._common_head + [("gh0", ctypes.c_float), ("dt", ctypes.c_float)] + PSMD._common_tail
+
+
+class Plain:
+    """The plain drop-in form (swe_cuda_*), one process-wide instance."""
+
+    def __init__(self):
+        self.lib = load()
+        self.fsize = None
+        self._keep = None
+
+    # -- init ------------------------------------------------------------------------
+    def init(self, fsize: int, layout: int, simd_length: int, compute_size: int, patch_size: int,
+             compute_pid_s: int, nnbr: int, padded_nnbr: int, gh0: float, dt: float, arrays: dict) -> None:
+        names = ("x", "y", "z", "f", "ghm", "p_u", "p_v", "p_w", "gradghm", "idx", "Dx", "Dy", "Dz", "L")
+        ptrs = []
+        for n in names:
+            a = arrays[n]
+            ptrs.append(a if isinstance(a, int) else _p(a))
+        check("swe_cuda_init", self.lib.swe_cuda_init(
+            fsize, layout, simd_length, compute_size, patch_size, compute_pid_s, nnbr, padded_nnbr,
+            float(gh0), float(dt), *ptrs))
+        self.fsize, self.layout, self.S = fsize, layout, simd_length
+        self.compute_size, self.patch_size = compute_size, patch_size
+        self.dtype = np.float64 if fsize == 8 else np.float32
+
+    def init_model(self, model, prec: str = "fp64") -> None:
+        """Canonical CFDL layout from a swe_input.SweModel (node-major, idx 0-based)."""
+        dt = np.float64 if prec == "fp64" else np.float32
+        arrs = {k: np.ascontiguousarray(getattr(model, k), dtype=dt) for k in
+                ("x", "y", "z", "f", "ghm", "p_u", "p_v", "p_w", "gradghm", "Dx", "Dy", "Dz", "L")}
+        arrs["idx"] = np.ascontiguousarray(model.idx, dtype=np.int32)
+        self._keep = arrs
+        fs = np.dtype(dt).itemsize
+        self.init(fs, SWE_LAYOUT_CFDL, 1, model.N, model.N, 0, model.Nnbr, model.Nnbr,
+                  float(model.gh0), float(model.dt), arrs)
+
+    def init_psmd(self, psmd_addr: int, fsize: int, layout: int, simd_length: int) -> None:
+        """Forward a reference PSMD_struct (what swe_cuda_init_psmd does in C)."""
+        p = (PSMD64 if fsize == 8 else PSMD32).from_address(psmd_addr)
+        arrays = {n: getattr(p, n) for n in
+                  ("x", "y", "z", "f", "ghm", "p_u", "p_v", "p_w", "gradghm", "idx", "Dx", "Dy", "Dz", "L")}
+        self.init(fsize, layout, simd_length, p.compute_size, p.patch_size, p.compute_pid_s,
+                  p.Nnbr, p.padded_Nnbr, float(p.gh0), float(p.dt), arrays)
+
+    # -- state / stepping ---------------------------------------------------------------
+    def set_state(self, H: np.ndarray) -> None:
+        H = np.ascontiguousarray(H, dtype=self.dtype)
+        assert H.size == 4 * self.patch_size
+        check("swe_cuda_set_state", self.lib.swe_cuda_set_state(_p(H)))
+        self.lib.swe_cuda_sync()
+
+    def set_state_ptr(self, addr: int) -> None:
+        check("swe_cuda_set_state", self.lib.swe_cuda_set_state(addr))
+
+    def get_state(self) -> np.ndarray:
+        H = np.empty(4 * self.patch_size, dtype=self.dtype)
+        check("swe_cuda_get_state", self.lib.swe_cuda_get_state(_p(H)))
+        return H
+
+    def get_state_ptr(self, addr: int) -> None:
+        check("swe_cuda_get_state", self.lib.swe_cuda_get_state(addr))
+
+    def eval_rhs(self, K: np.ndarray) -> np.ndarray:
+        K = np.ascontiguousarray(K, dtype=self.dtype)
+        assert K.size == 4 * self.patch_size
+        F = np.empty(4 * self.compute_size, dtype=self.dtype)
+        check("swe_cuda_eval_rhs", self.lib.swe_cuda_eval_rhs(_p(K), _p(F)))
+        return F
+
+    def rk_substep(self, substep_id: int) -> None:
+        check("swe_cuda_rk_substep", self.lib.swe_cuda_rk_substep(int(substep_id)))
+
+    def step(self, nsteps: int) -> None:
+        check("swe_cuda_step", self.lib.swe_cuda_step(int(nsteps)))
+
+    def sync(self) -> None:
+        check("swe_cuda_sync", self.lib.swe_cuda_sync())
+
+    def set_timing(self, on: bool) -> None:
+        check("swe_cuda_set_timing", self.lib.swe_cuda_set_timing(1 if on else 0))
+
+    def timings(self) -> tuple[float, int, float]:
+        out = np.zeros(3)
+        check("swe_cuda_last_timings", self.lib.swe_cuda_last_timings(_p(out)))
+        return float(out[0]), int(out[1]), float(out[2])
+
+    def stream(self) -> int:
+        return int(self.lib.swe_cuda_stream() or 0)
+
+    def invariants(self) -> np.ndarray:
+        out = np.zeros(2)
+        check("swe_cuda_invariants", self.lib.swe_cuda_invariants(_p(out)))
+        return out
+
+    def finalize(self) -> None:
+        check("swe_cuda_finalize", self.lib.swe_cuda_finalize())

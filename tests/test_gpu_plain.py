@@ -1,0 +1,172 @@
+"""Plain form on the GPU, called through the C ABI (capi -> libswe_b200.so).
+
+Parity bars:
+* FP64 eval_rhs: <= 1e-12 per-field max-norm relative error against the oracle
+  and against the reference's own eval_RHS_swe on the generated (noised)
+  inputs, plus a condition-normalised bound (conftest.cond_err) that also holds
+  on the balanced shipped input;
+* 100 RK4 steps on an input whose H_100 came from the reference: the
+  reference's own verify_output criterion, |H - H_100| <= 1e-9 (FP64) and
+  <= 4e-2 (FP32) absolute (swe_config.h:80, :88);
+* the stage-by-stage API and the graph-captured step are bit-identical, and
+  reruns are bit-identical.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN, cond_err, generated_input, rel_err
+from swe_b200 import capi, layout, swe_input
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def plain():
+    p = capi.Plain()
+    yield p
+    p.finalize()
+
+
+@pytest.fixture(scope="module")
+def grid_l6():
+    return generated_input(6)
+
+
+def _perturbed(H, seed=5, eps=1e-3):
+    rng = np.random.default_rng(seed)
+    return H * (1.0 + eps * rng.standard_normal(H.shape))
+
+
+@pytest.mark.parametrize("level", [4, 6])
+def test_eval_rhs_fp64_matches_oracle(plain, level):
+    _, d = generated_input(level, fill_fc=(level == 4))
+    m = swe_input.to_model(d)
+    plain.init_model(m, "fp64")
+    port = oracle.Port(m, "fp64")
+    for K in (m.H_init, _perturbed(m.H_init)):
+        F = plain.eval_rhs(K)
+        F_ref = port.eval_rhs(K)
+        assert rel_err(F, F_ref).max() <= 1e-12
+        assert cond_err(F, F_ref, m, K) <= 4e-16
+
+
+@pytest.mark.parametrize("lay", oracle.LAYOUTS)
+@pytest.mark.parametrize("rcm", [0, 1])
+def test_drop_in_all_reference_layouts(plain, lay, rcm, grid_l4):
+    """The reference builds LPSMD in its own layout (and RCM order); the library
+    takes the PSMD_struct as is and must agree with the reference's eval_RHS_swe."""
+    if not oracle.reference_available("fp64", lay):
+        pytest.skip("reference not built")
+    path, d = grid_l4
+    ref = oracle.Ref(path, "fp64", lay, use_rcm=rcm)
+    plain.init_psmd(ref.psmd_ptr(), 8, ref.layout_flags, ref.simd_length)
+    for K in (ref.H_init(), _perturbed(ref.H_init())):
+        F = ref.state_to_canonical(plain.eval_rhs(K))
+        F_ref = ref.state_to_canonical(ref.eval_rhs(K))
+        assert rel_err(F, F_ref).max() <= 1e-12
+
+
+@pytest.mark.parametrize("lay", ["cfdl", "default"])
+def test_shipped_input_100_steps_verify(plain, shipped_input, lay):
+    """The reference's own end-to-end check on its shipped input, through its PSMD."""
+    if not oracle.reference_available("fp64", lay):
+        pytest.skip("reference not built")
+    ref = oracle.Ref(shipped_input, "fp64", lay, use_rcm=1)
+    plain.init_psmd(ref.psmd_ptr(), 8, ref.layout_flags, ref.simd_length)
+    K = ref.H_init()
+    m = swe_input.load_model(shipped_input)
+    F = ref.state_to_canonical(plain.eval_rhs(K))[: m.N]
+    F_ref = ref.state_to_canonical(ref.eval_rhs(K))[: m.N]
+    perm = ref.mapping()
+    assert cond_err(F, F_ref, layout.reorder(m, perm), K=ref.state_to_canonical(K)[: m.N]) <= 4e-16
+    plain.set_state(ref.H_init())
+    plain.step(100)
+    count, max_err = ref.verify(plain.get_state())
+    assert count == 0, max_err
+
+
+def test_generated_input_100_steps_vs_oracle_H100(plain, grid_l4):
+    path, d = grid_l4
+    m, mapping = layout.prepare(swe_input.to_model(d), use_rcm=True, simd_length=32)
+    plain.init_model(m, "fp64")
+    plain.set_state(m.H_init)
+    plain.step(100)
+    H = plain.get_state().reshape(-1, 4)
+    assert np.abs(H - m.H_100).max() <= 1e-9
+
+
+def test_substeps_equal_graph_steps_and_rerun_bitwise(plain, grid_l4):
+    _, d = grid_l4
+    m = swe_input.to_model(d)
+    plain.init_model(m, "fp64")
+    plain.set_state(m.H_init)
+    for _ in range(5):
+        for s in range(4):
+            plain.rk_substep(s)
+    a = plain.get_state()
+    plain.set_state(m.H_init)
+    plain.step(5)
+    b = plain.get_state()
+    plain.set_state(m.H_init)
+    plain.step(5)
+    c = plain.get_state()
+    assert np.array_equal(a, b) and np.array_equal(b, c)
+
+
+def test_fp32_form(plain, grid_l4):
+    _, d = grid_l4
+    m = swe_input.to_model(d)
+    plain.init_model(m, "fp32")
+    K = _perturbed(m.H_init).astype(np.float32)
+    F = plain.eval_rhs(K)
+    assert cond_err(F, oracle.Port(m, "fp32").eval_rhs(K), m, K) <= 4e-6
+    assert cond_err(F, oracle.Port(m, "fp64").eval_rhs(K.astype(np.float64)), m, K) <= 4e-6
+    plain.set_state(m.H_init.astype(np.float32))
+    plain.step(100)
+    H = plain.get_state().reshape(-1, 4)
+    assert np.abs(H - m.H_100).max() <= 4e-2          # the reference's FP32 TOLERANCE
+
+
+def test_padded_weight_columns_are_never_read(plain):
+    """Non-CFDL callers pass [N][32] rows whose column 31 the reference fills by
+    replication (matrix_transformations.c:20-21); garbage there must not matter."""
+    m = swe_input.load_model(os.path.join(GOLDEN, "icos162_seed7.bin"))
+    m = layout.pad(m, 32)
+    arrays = {}
+    for k in ("Dx", "Dy", "Dz", "L"):
+        a = np.zeros((m.N, 32))
+        a[:, :31] = getattr(m, k)
+        a[:, 31] = 1e300
+        arrays[k] = a
+    idx = np.full((m.N, 32), 10 ** 8, dtype=np.int32)
+    idx[:, :31] = m.idx
+    arrays["idx"] = idx
+    for k in ("x", "y", "z", "f", "ghm", "p_u", "p_v", "p_w", "gradghm"):
+        arrays[k] = np.ascontiguousarray(getattr(m, k))
+    plain.init(8, capi.SWE_LAYOUT_CFDL, 32, m.N, m.N, 0, 31, 32, m.gh0, m.dt, arrays)
+    F = plain.eval_rhs(m.H_init)
+    assert np.isfinite(F).all()
+    assert rel_err(F, oracle.Port(m, "fp64").eval_rhs(m.H_init)).max() <= 1e-12
+
+
+def test_out_of_range_index_is_rejected(plain):
+    m = swe_input.load_model(os.path.join(GOLDEN, "icos162_seed7.bin"))
+    m.idx[7, 3] = m.N + 5
+    with pytest.raises(capi.SweError) as e:
+        plain.init_model(m, "fp64")
+    assert e.value.status == 5
+
+
+def test_invariants_match_oracle(plain, grid_l4):
+    _, d = grid_l4
+    m = swe_input.to_model(d)
+    plain.init_model(m, "fp64")
+    plain.set_state(m.H_init)
+    plain.step(3)
+    H = plain.get_state()
+    got = plain.invariants()
+    want = oracle.Port(m, "fp64").invariants(H)[0]
+    assert np.allclose(got, want, rtol=1e-13)

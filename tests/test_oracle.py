@@ -1,0 +1,108 @@
+"""The CPU oracle, pinned against the reference's own results.
+
+* the shipped N=2562 input's H_100 (the reference's only known answer,
+  main.c:439-477 at the FP64 TOLERANCE 1e-9);
+* golden outputs of the reference's eval_RHS_swe / RK_substep built from
+  source (tests/golden/make_golden.py);
+* the reference libraries themselves on generated grids, in all four layouts
+  with and without RCM (skipped where oracle/_ref was not built).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN, cond_err, rel_err
+from swe_b200 import swe_input
+
+GOLDEN_BIN = os.path.join(GOLDEN, "icos162_seed7.bin")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return swe_input.load_model(GOLDEN_BIN), np.load(os.path.join(GOLDEN, "icos162_ref.npz"))
+
+
+def test_port_matches_shipped_H100(shipped_input):
+    m = swe_input.load_model(shipped_input)
+    H = oracle.Port(m, "fp64").run(m.H_init, 100)
+    err = np.abs(H - m.H_100).max()
+    assert err <= 1e-9, err          # swe_config.h:88 FP64 TOLERANCE
+
+
+def test_port_eval_rhs_matches_reference_on_shipped(shipped_input):
+    if not oracle.reference_available("fp64", "cfdl"):
+        pytest.skip("reference not built")
+    ref = oracle.Ref(shipped_input, "fp64", "cfdl", use_rcm=0)
+    m = swe_input.load_model(shipped_input)
+    F_ref = ref.state_to_canonical(ref.eval_rhs(ref.H_init()))[: m.N]
+    F = oracle.Port(m, "fp64").eval_rhs(m.H_init)
+    # The shipped H_init is in geostrophic balance, so F is ~1e5 times smaller
+    # than its terms and max-norm relative agreement is only ~3e-10 even between
+    # two summation orders of the reference; the condition-normalised error is
+    # the meaningful bound here.
+    assert cond_err(F, F_ref, m, m.H_init) <= 1e-15
+
+
+def test_port_eval_rhs_matches_reference_golden(golden):
+    m, g = golden
+    p = oracle.Port(m, "fp64")
+    n = m.N
+    # two FP64 summation orders (OpenMP SIMD in the reference, sequential here)
+    assert rel_err(p.eval_rhs(m.H_init), g["F0"][:n]).max() <= 1e-12
+    assert rel_err(p.eval_rhs(g["K1"][:n]), g["F1"][:n]).max() <= 1e-12
+    assert cond_err(p.eval_rhs(m.H_init), g["F0"][:n], m, m.H_init) <= 1e-15
+
+
+def test_port_steps_match_reference_golden(golden):
+    m, g = golden
+    H = oracle.Port(m, "fp64").run(m.H_init, 10)
+    assert rel_err(H, g["H10"][: m.N]).max() <= 1e-12
+    H100 = oracle.Port(m, "fp64").run(m.H_init, 100)
+    assert np.abs(H100 - m.H_100).max() <= 1e-9
+
+
+def test_port_fp32_matches_reference_fp32_golden(golden):
+    m, g = golden
+    p = oracle.Port(m, "fp32")
+    # FP32 sums in two orders: a few FP32 ulps of the term scale
+    assert cond_err(p.eval_rhs(m.H_init), g["F0_32"][: m.N], m, m.H_init) <= 4e-6
+    assert rel_err(p.run(m.H_init, 10), g["H10_32"][: m.N]).max() <= 1e-5
+
+
+def test_rcm_golden_is_a_permutation(golden):
+    m, g = golden
+    mapping = g["mapping"]
+    assert sorted(mapping.tolist()) == list(range(m.N))
+    H_nat = oracle.Port(m, "fp64").run(m.H_init, 10)
+    # RCM changes only the node order (rcm.c:9-62, reorder_nodes.c:46-87)
+    assert rel_err(g["H10_rcm"][: m.N], H_nat[mapping]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("layout", oracle.LAYOUTS)
+@pytest.mark.parametrize("rcm", [0, 1])
+def test_reference_layouts_agree_with_port(layout, rcm, grid_l3):
+    if not oracle.reference_available("fp64", layout):
+        pytest.skip("reference not built")
+    path, d = grid_l3
+    ref = oracle.Ref(path, "fp64", layout, use_rcm=rcm)
+    m = swe_input.to_model(d)
+    perm = ref.mapping()
+    H0 = ref.state_to_canonical(ref.H_init())
+    assert np.array_equal(H0[: d.N], m.H_init[perm])
+    F_ref = ref.state_to_canonical(ref.eval_rhs(ref.H_init()))[: d.N]
+    F_port = oracle.Port(m, "fp64").eval_rhs(m.H_init)[perm]
+    assert rel_err(F_ref, F_port).max() <= 1e-12
+
+
+def test_invariants_are_fp64_sums(golden):
+    m, _ = golden
+    p = oracle.Port(m, "fp64")
+    inv = p.invariants(m.H_init)[0]
+    A = 4 * np.pi / m.N
+    phi = m.H_init[:, 3] + m.gh0
+    th = phi - m.ghm
+    assert np.isclose(inv[0], A * th.sum(), rtol=1e-14)
+    e = A * (0.5 * th * (m.H_init[:, :3] ** 2).sum(1) + 0.5 * phi ** 2).sum()
+    assert np.isclose(inv[1], e, rtol=1e-13)
