@@ -40,6 +40,7 @@ sys.path.insert(0, os.path.join(ROOT, "rbf-fd-swe_b200"))
 WORKLOADS = {
     # name: (level, precision, description)
     "plain_fp64_n40962": (6, "fp64", "plain FP64, N=40962 (level 6), CFDL, RCM, dt=225 s"),
+    "plain_fp64_n163842": (7, "fp64", "plain FP64, N=163842 (level 7), CFDL, RCM, dt=120 s"),
     "plain_fp64_n655362": (8, "fp64", "plain FP64, N=655362 (level 8), CFDL, RCM, dt=60 s"),
     "plain_fp32_n655362": (8, "fp32", "plain FP32, N=655362 (level 8), CFDL, RCM, dt=60 s"),
 }
@@ -90,7 +91,7 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def _rows(self):
         rows = []
         try:
             for line in open(self.path):
@@ -99,6 +100,22 @@ class ClockSampler:
                     rows.append(f)
         except Exception:
             pass
+        return rows
+
+    def count(self) -> int:
+        return len(self._rows())
+
+    def wait_for(self, n: int, timeout: float, keep_busy=None) -> None:
+        """Until n samples exist (or timeout), calling keep_busy() meanwhile."""
+        t0 = time.time()
+        while self.proc and self.count() < n and time.time() - t0 < timeout:
+            if keep_busy:
+                keep_busy()
+            else:
+                time.sleep(0.05)
+
+    def summary(self, first: int = 0):
+        rows = self._rows()[first:]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -233,6 +250,8 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
+        clocks.wait_for(1, 5.0)
+        first_sample = clocks.count()
         with torch.cuda.stream(stream):
             for s in range(args.steps):
                 flush.zero_()                       # L2 flush between timed steps (not timed)
@@ -243,6 +262,14 @@ def main():
         launches = capi.kernel_launches() - launches0
         t_steps = [a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops)]
         t_total = float(sum(t_steps))
+
+        # The timed region is far shorter than nvidia-smi's 200 ms period: keep
+        # the same step loop running (untimed) until 3 samples cover it.
+        def busy():
+            for _ in range(200):
+                plain.step(1)
+            plain.sync()
+        clocks.wait_for(first_sample + 3, 5.0, keep_busy=busy)
         # ---- per-stage kernel durations for the roofline (same stream, events) -------
         plain.set_timing(True)
         with torch.cuda.stream(stream):
@@ -313,7 +340,7 @@ def main():
             "gpu_launches": int(launches),
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "clocks": clocks.summary(),
+            "clocks": clocks.summary(first_sample),
             "state_finite": finite,
         }
         print(json.dumps(line), flush=True)
