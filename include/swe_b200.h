@@ -115,6 +115,34 @@ int swe_cuda_invariants(double* mass_energy);
 int swe_cuda_finalize(void);
 
 /* ---------------------------------------------------------------------------
+ * Plain form without device allocation
+ * ------------------------------------------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (device memory owned by an outer framework's pool; loops where an
+ * allocation's implicit device synchronisation is not allowed): nsteps RK4
+ * steps of one state, like swe_cuda_step, with every array a device pointer
+ * the caller owns -- idx [n][nnbr] (0-based), Dx, Dy, Dz, L [n][nnbr],
+ * x, y, z, f, ghm [n], p_u, p_v, p_w, gradghm [n][3], and H [n][4]
+ * (u, v, w, h per node; updated in place) -- in fType of fsize bytes, with
+ * Dx, Dy, Dz already divided by a and L multiplied by gamma (the reader's
+ * scaling).  The K and D registers live in a static device array of
+ * SWE_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit, so n <= SWE_NOALLOC_SCRATCH_BYTES / (12 * fsize) nodes (43690 FP64,
+ * 87381 FP32); larger n returns SWE_ERR_ARG.  Nothing here allocates.  The
+ * first call on a device looks up the array's address, so make it before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller.  Kernels go to `stream` (a
+ * cudaStream_t, NULL for the default stream); the call returns once they are
+ * enqueued. */
+#define SWE_NOALLOC_SCRATCH_BYTES (4u << 20)
+int swe_cuda_step_noalloc(int fsize, int n, int nnbr, double gh0, double dt, const int* idx,
+                          const void* Dx, const void* Dy, const void* Dz, const void* L,
+                          const void* x, const void* y, const void* z, const void* f, const void* ghm,
+                          const void* p_u, const void* p_v, const void* p_w, const void* gradghm,
+                          void* H, int nsteps, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Host utilities (no device work)
  * ------------------------------------------------------------------------- */
 
