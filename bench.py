@@ -43,8 +43,14 @@ WORKLOADS = {
     "plain_fp64_n163842": (7, "fp64", "plain FP64, N=163842 (level 7), CFDL, RCM, dt=120 s"),
     "plain_fp64_n655362": (8, "fp64", "plain FP64, N=655362 (level 8), CFDL, RCM, dt=60 s"),
     "plain_fp32_n655362": (8, "fp32", "plain FP32, N=655362 (level 8), CFDL, RCM, dt=60 s"),
+    "ens_tf32_n163842_b64": (7, "tf32x3", "batched ensemble, N=163842 (level 7), 64 members, 3xTF32 on tcgen05, dt=120 s"),
+    "ens_tf32_n40962_b64": (6, "tf32x3", "batched ensemble, N=40962 (level 6), 64 members, 3xTF32 on tcgen05, dt=225 s"),
 }
 ALG_BYTES = {"fp64": 1396, "fp32": 760}      # per node-stage (FP64: 4*31*8+31*4+17*8+4*8+14*8)
+# batched form, per node-stage: shared 4*31*4 (weights) + 31*4 (idx) + 17*4 (pointwise)
+# plus per member 4*4 (K read once) + 14*4 (RK combine) + 4 (FP64 h registers)
+ENS_SHARED_BYTES = 4 * 31 * 4 + 31 * 4 + 17 * 4
+ENS_MEMBER_BYTES = 4 * 4 + 14 * 4 + 4
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -202,6 +208,136 @@ def run_reference(args, level, prec, wl):
     print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args, level, desc, members=64):
+    """member-steps/s of the batched 3xTF32 form, next to the plain FP64 form on the
+    same grid, with the h error of a few members against the plain FP64 run."""
+    import torch
+
+    from swe_b200 import capi, gen
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    d, m, pm = build_workload(level, "fp64", device=f"cuda:{local}")
+    N = d.N
+    H0 = np.stack([gen.perturb_h(m.H_init, 1000 + b) for b in range(members)])
+    ens = capi.Ensemble()
+    capi.check("swe_cuda_select_device", ens.lib.swe_cuda_select_device(local))
+    ens.init(m, members)
+    ens.set_state(H0)
+    tune_ms = ens.tune().tolist()
+    cfg = ens.config()
+    stream = torch.cuda.ExternalStream(ens.stream())
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        ens.step(1)
+    ens.sync()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = capi.kernel_launches()
+    with ClockSampler(local) as clocks:
+        clocks.wait_for(1, 5.0)
+        first = clocks.count()
+        with torch.cuda.stream(stream):
+            for s in range(args.steps):
+                flush.zero_()
+                starts[s].record(stream)
+                ens.step(1)
+                stops[s].record(stream)
+        torch.cuda.synchronize()
+        launches = capi.kernel_launches() - launches0
+        t_total = sum(a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops))
+
+        def busy():
+            for _ in range(20):
+                ens.step(1)
+            ens.sync()
+        clocks.wait_for(first + 3, 5.0, keep_busy=busy)
+    ens.sync()
+    member_steps = members * args.steps * world / t_total
+    t_stage = t_total / (4 * args.steps)
+    ens_bytes = ENS_SHARED_BYTES + members * ENS_MEMBER_BYTES
+    peak, peak_kind = measured_peak_hbm()
+    achieved = ens_bytes * N / t_stage / 1e9
+
+    # e2e through the C ABI: host state in, one step, host state out
+    ens.set_state(H0)
+    e2e_steps = max(3, args.steps // 4)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ens.set_state(H0)
+        ens.step(1)
+        Hout = ens.get_state()
+    t_e2e = time.perf_counter() - t0
+    nbytes = H0.nbytes
+
+    # plain FP64 on the same grid: member-steps/s = steps/s of one state
+    plain = capi.Plain()
+    plain.init_model(pm, "fp64")
+    plain.set_state(pm.H_init)
+    for _ in range(3):
+        plain.step(1)
+    plain.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pstream = torch.cuda.ExternalStream(plain.stream())
+    with torch.cuda.stream(pstream):
+        e0.record(pstream)
+        plain.step(args.steps)
+        e1.record(pstream)
+    torch.cuda.synchronize()
+    plain_steps = args.steps / (e0.elapsed_time(e1) * 1e-3)
+
+    # h error after err_steps steps against the plain FP64 GPU run of the same members
+    # (natural node order, as the ensemble exchanges states)
+    plain.init_model(m, "fp64")
+    err_members = list(range(0, members, max(1, members // args.err_members)))[: args.err_members]
+    ens.set_state(H0)
+    ens.step(args.err_steps)
+    Hens = ens.get_state()
+    errs = []
+    for b in err_members:
+        plain.set_state(H0[b])
+        plain.step(args.err_steps)
+        Hp = plain.get_state().reshape(-1, 4)
+        e = np.abs(Hens[b] - Hp).max(0) / np.abs(Hp).max(0)
+        errs.append(e)
+    errs = np.array(errs)
+    plain.finalize()
+    ens.finalize()
+    if rank == 0:
+        line = {
+            "metric": "member-steps/s (batched ensemble, 3xTF32 tcgen05) and ratio to plain FP64",
+            "value": member_steps, "unit": "member-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "tf32x3 (fp32 state, fp64 h accumulation)",
+            "data": "synthetic (seeded icosahedral grid, PHS RBF-FD weights, TC5 ICs, per-member 1e-3 h noise)",
+            "config": {"workload": args.workload, "description": desc, "nodes": N, "members": members,
+                       "dt": d.dt, "kernel_variant": cfg, "tune_ms_per_step": tune_ms,
+                       "l2": "flushed (256 MB write) between timed steps"},
+            "plain_fp64_member_steps_per_s": plain_steps,
+            "ratio_vs_plain_fp64": member_steps / plain_steps,
+            "h_err_vs_fp64": {"steps": args.err_steps, "members": err_members,
+                              "max_norm_rel_per_field_max": errs.max(0).tolist()},
+            "e2e": {"value": members * e2e_steps / t_e2e, "unit": "member-steps/s",
+                    "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                         "kernel": "swe::ens_stage_kernel", "kernel_us": round(t_stage * 1e6, 2),
+                         "alg_bytes_per_node_stage": ens_bytes},
+            "clocks": clocks.summary(first),
+            "state_finite": bool(np.isfinite(Hout).all()),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -210,11 +346,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain_fp64_n40962", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--err-steps", type=int, default=100)
+    ap.add_argument("--err-members", type=int, default=4)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     level, prec, desc = WORKLOADS[args.workload]
     if args.impl == "reference":
-        return run_reference(args, level, prec, args.workload)
+        return run_reference(args, level, "fp64" if prec == "tf32x3" else prec, args.workload)
+    if prec == "tf32x3":
+        return run_ensemble(args, level, desc)
 
     import torch
     import torch.distributed as dist

@@ -115,6 +115,52 @@ int swe_cuda_invariants(double* mass_energy);
 int swe_cuda_finalize(void);
 
 /* ---------------------------------------------------------------------------
+ * Batched-ensemble form (members share one grid; tcgen05 tensor cores)
+ * ------------------------------------------------------------------------- */
+
+/* No single reference counterpart: the reference steps one state at a time
+ * (RK_substep, rk4_rbffd_swe.c:30-72); this form steps `members` (32 or 64)
+ * states of the same grid together.  Static arrays are the canonical FP64
+ * ones in natural node order -- idx [n][nnbr] 0-based, Dx, Dy, Dz, L [n][nnbr]
+ * already scaled as input.c:314-319 scales them, x, y, z, f, ghm [n],
+ * p_u, p_v, p_w, gradghm [n][3].  The library reorders nodes by the
+ * reference's RCM permutation internally; states are exchanged as
+ * [members][n][4] FP64 in natural order.
+ * Precision: stencil products in 3xTF32 on tcgen05 with FP32 accumulation;
+ * u, v, w and the stage states K in FP32; the RK4 accumulation of h (base
+ * state and D register) in FP64; invariants in FP64. */
+int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int* idx,
+                 const double* Dx, const double* Dy, const double* Dz, const double* L,
+                 const double* x, const double* y, const double* z, const double* f,
+                 const double* ghm, const double* p_u, const double* p_v, const double* p_w,
+                 const double* gradghm);
+int swe_ens_set_state(const double* H);
+int swe_ens_get_state(double* H);
+/* F = RHS(K) for all members (the same stencil math in the same precision);
+ * K and F are [members][n][4] FP64 host arrays in natural order. */
+int swe_ens_eval_rhs(const double* K, double* F);
+/* nsteps RK4 steps of every member (captured CUDA graph of the four stage
+ * kernels); swe_ens_stage runs one stage, same semantics as RK_substep. */
+int swe_ens_step(int nsteps);
+int swe_ens_stage(int substep_id);
+/* Autotuner: times one RK4 step of every kernel variant (tile of 4 or 8 nodes x
+ * 32 or 64 members per CTA) on the live state, restores the state and keeps
+ * the fastest.  ms_per_step[4] (may be NULL) receives the timings, -1 where a
+ * variant does not apply.  config[4] = {tile nodes, members per CTA, largest
+ * neighbour set of a 4-node tile, of an 8-node tile}. */
+int swe_ens_tune(double* ms_per_step);
+int swe_ens_config(int* config);
+/* Forces one variant (tile_nodes 4 or 8, members_per_cta 32 or 64). */
+int swe_ens_use_variant(int tile_nodes, int members_per_cta);
+/* FP64 (mass, energy) per member, [members][2], definitions as swe_cuda_invariants. */
+int swe_ens_invariants(double* mass_energy);
+int swe_ens_sync(void);
+int swe_ens_set_timing(int enabled);
+int swe_ens_last_timings(double* out);
+void* swe_ens_stream(void);
+int swe_ens_finalize(void);
+
+/* ---------------------------------------------------------------------------
  * Plain form without device allocation
  * ------------------------------------------------------------------------- */
 

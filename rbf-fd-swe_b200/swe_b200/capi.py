@@ -59,6 +59,16 @@ def load() -> ctypes.CDLL:
     lib.swe_cuda_step.argtypes = [i]
     lib.swe_cuda_set_timing.argtypes = [i]
     lib.swe_cuda_stream.restype = vp
+    lib.swe_ens_init.argtypes = [i, i, i, d, d] + [vp] * 14
+    for name in ("swe_ens_set_state", "swe_ens_get_state", "swe_ens_tune", "swe_ens_config",
+                 "swe_ens_invariants", "swe_ens_last_timings"):
+        getattr(lib, name).argtypes = [vp]
+    lib.swe_ens_eval_rhs.argtypes = [vp, vp]
+    lib.swe_ens_step.argtypes = [i]
+    lib.swe_ens_stage.argtypes = [i]
+    lib.swe_ens_set_timing.argtypes = [i]
+    lib.swe_ens_use_variant.argtypes = [i, i]
+    lib.swe_ens_stream.restype = vp
     _lib = lib
     return lib
 
@@ -192,3 +202,80 @@ class Plain:
 
     def finalize(self) -> None:
         check("swe_cuda_finalize", self.lib.swe_cuda_finalize())
+
+
+class Ensemble:
+    """The batched-ensemble form (swe_ens_*): `members` states on one grid."""
+
+    def __init__(self):
+        self.lib = load()
+        self._keep = None
+
+    def init(self, model, members: int) -> None:
+        arrs = {k: np.ascontiguousarray(getattr(model, k), dtype=np.float64) for k in
+                ("Dx", "Dy", "Dz", "L", "x", "y", "z", "f", "ghm", "p_u", "p_v", "p_w", "gradghm")}
+        idx = np.ascontiguousarray(model.idx, dtype=np.int32)
+        self._keep = (arrs, idx)
+        check("swe_ens_init", self.lib.swe_ens_init(
+            members, model.N, model.Nnbr, float(model.gh0), float(model.dt), _p(idx),
+            *[_p(arrs[k]) for k in ("Dx", "Dy", "Dz", "L", "x", "y", "z", "f", "ghm",
+                                    "p_u", "p_v", "p_w", "gradghm")]))
+        self.members, self.n = members, model.N
+
+    def set_state(self, H: np.ndarray) -> None:
+        H = np.ascontiguousarray(H, dtype=np.float64).reshape(self.members, self.n, 4)
+        check("swe_ens_set_state", self.lib.swe_ens_set_state(_p(H)))
+        self.sync()
+
+    def get_state(self) -> np.ndarray:
+        H = np.empty((self.members, self.n, 4))
+        check("swe_ens_get_state", self.lib.swe_ens_get_state(_p(H)))
+        return H
+
+    def eval_rhs(self, K: np.ndarray) -> np.ndarray:
+        K = np.ascontiguousarray(K, dtype=np.float64).reshape(self.members, self.n, 4)
+        F = np.empty_like(K)
+        check("swe_ens_eval_rhs", self.lib.swe_ens_eval_rhs(_p(K), _p(F)))
+        return F
+
+    def step(self, nsteps: int) -> None:
+        check("swe_ens_step", self.lib.swe_ens_step(int(nsteps)))
+
+    def stage(self, s: int) -> None:
+        check("swe_ens_stage", self.lib.swe_ens_stage(int(s)))
+
+    def sync(self) -> None:
+        check("swe_ens_sync", self.lib.swe_ens_sync())
+
+    def tune(self) -> np.ndarray:
+        ms = np.zeros(4)
+        check("swe_ens_tune", self.lib.swe_ens_tune(_p(ms)))
+        return ms
+
+    def use_variant(self, tile_nodes: int, members_per_cta: int) -> None:
+        check("swe_ens_use_variant", self.lib.swe_ens_use_variant(tile_nodes, members_per_cta))
+
+    def config(self) -> dict:
+        out = np.zeros(4, dtype=np.int32)
+        check("swe_ens_config", self.lib.swe_ens_config(_p(out)))
+        return {"tile_nodes": int(out[0]), "members_per_cta": int(out[1]),
+                "max_rows_tile4": int(out[2]), "max_rows_tile8": int(out[3])}
+
+    def invariants(self) -> np.ndarray:
+        out = np.zeros((self.members, 2))
+        check("swe_ens_invariants", self.lib.swe_ens_invariants(_p(out)))
+        return out
+
+    def set_timing(self, on: bool) -> None:
+        check("swe_ens_set_timing", self.lib.swe_ens_set_timing(1 if on else 0))
+
+    def last_step_seconds(self) -> float:
+        out = np.zeros(1)
+        check("swe_ens_last_timings", self.lib.swe_ens_last_timings(_p(out)))
+        return float(out[0])
+
+    def stream(self) -> int:
+        return int(self.lib.swe_ens_stream() or 0)
+
+    def finalize(self) -> None:
+        check("swe_ens_finalize", self.lib.swe_ens_finalize())
