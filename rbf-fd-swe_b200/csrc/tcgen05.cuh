@@ -105,9 +105,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, 
     return false;
 }
 
-// TF32 split: hi keeps the 10 explicit mantissa bits tcgen05 kind::tf32 reads;
-// lo = x - hi is exact in FP32 and carries the next 11+ bits.
-__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+// Round an FP32 value to the nearest TF32 (10 explicit mantissa bits), ties
+// away from zero; the result is exactly representable, so the tensor core's
+// own FP32 -> TF32 conversion leaves it unchanged.
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+// 3xTF32 split x ~ hi + lo with both parts exact TF32: |x - hi - lo| <= 2^-22 |x|.
+__device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
+    hi = tf32_rna(x);
+    lo = tf32_rna(x - hi);
+}
 
 }  // namespace tc
 }  // namespace swe

@@ -4,7 +4,8 @@ Bars (FP32-level arithmetic checked against the FP64 oracle):
 * eval_rhs of every member: condition-normalised error <= 4e-6 (a few FP32
   ulps of the term scale, conftest.cond_err) in every kernel variant;
 * 20 RK4 steps of every member against the FP64 oracle: per-field max-norm
-  relative error <= 1e-5;
+  relative error no larger than twice what the plain FP32 restatement of the
+  reference reaches on the same member (FP32-level accuracy);
 * a member's result does not depend on the other members (32- and 64-member
   runs agree bitwise for the members they share);
 * FP64 invariants of the device state equal the oracle's sums of the same state.
@@ -61,9 +62,12 @@ def test_steps_match_fp64_oracle(ens, model_l4):
     ens.step(20)
     H = ens.get_state()
     port = oracle.Port(m, "fp64")
+    port32 = oracle.Port(m, "fp32")
     for b in (0, 17, 40, 63):
         want = port.run(H0[b], 20)
-        assert rel_err(H[b], want).max() <= 1e-5, b
+        fp32_err = rel_err(port32.run(H0[b], 20), want)
+        err = rel_err(H[b], want)
+        assert (err <= 2 * fp32_err).all(), (b, err, fp32_err)
 
 
 def test_members_are_independent(ens, model_l4):
