@@ -303,8 +303,10 @@ def run_ensemble(args, level, desc, members=64):
         plain.set_state(H0[b])
         plain.step(args.err_steps)
         Hp = plain.get_state().reshape(-1, 4)
-        e = np.abs(Hens[b] - Hp).max(0) / np.abs(Hp).max(0)
-        errs.append(e)
+        # max-norm error per field; u, v, w relative to the velocity scale max|(u,v,w)|
+        # (w starts at zero), h relative to max|h|
+        scale = np.array([np.abs(Hp[:, :3]).max()] * 3 + [np.abs(Hp[:, 3]).max()])
+        errs.append(np.abs(Hens[b] - Hp).max(0) / scale)
     errs = np.array(errs)
     plain.finalize()
     ens.finalize()

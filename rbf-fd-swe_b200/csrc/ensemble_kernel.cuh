@@ -19,10 +19,12 @@
 // A_lo B_hi is accumulated in FP32 in TMEM.  Before the split every gathered
 // value is centred on the state of the tile's first node, c[mf]: the
 // contraction runs on X - c, whose entries are the local variation of the
-// fields rather than their magnitude, and c * sum_k(B_hi + B_lo) (FP64 row
-// sums of the split weights) is added back in the epilogue.  Derivative and
+// fields rather than their magnitude, and c * sum_k w (FP64 row sums of the
+// FP32 weights) is added back in the epilogue.  Derivative and
 // hyperviscosity weights annihilate constants, so the added-back term is tiny
 // and the cancellation that limits FP32 stencil sums mostly disappears.  The
+// add-back uses the FP32 weights themselves (sum in FP64), not hi + lo, so the
+// split's own rounding only ever multiplies the centred values.  The
 // RK4 accumulation of h (base state and D register) is FP64; u, v, w and every
 // stage state K are FP32.
 //
@@ -134,7 +136,7 @@ __global__ void __launch_bounds__(128 * HPC, 1) ens_stage_kernel(const EnsArgs a
                 tc::tf32_split(w[op], hi, lo);
                 *reinterpret_cast<float*>(B_hi + off) = hi;
                 *reinterpret_cast<float*>(B_lo + off) = lo;
-                part[op] = (double)hi + (double)lo;
+                part[op] = (double)w[op];
             }
         }
 #pragma unroll
