@@ -45,6 +45,8 @@ WORKLOADS = {
     "plain_fp32_n655362": (8, "fp32", "plain FP32, N=655362 (level 8), CFDL, RCM, dt=60 s"),
     "ens_tf32_n163842_b64": (7, "tf32x3", "batched ensemble, N=163842 (level 7), 64 members, 3xTF32 on tcgen05, dt=120 s"),
     "ens_tf32_n40962_b64": (6, "tf32x3", "batched ensemble, N=40962 (level 6), 64 members, 3xTF32 on tcgen05, dt=225 s"),
+    "serve_mix": (0, "serve", "serving: Poisson arrivals over N in {2562, 10242, 40962, 163842}, 1-32 members, "
+                              "10-500 steps, 80 GB budget, FP64"),
 }
 ALG_BYTES = {"fp64": 1396, "fp32": 760}      # per node-stage (FP64: 4*31*8+31*4+17*8+4*8+14*8)
 # batched form, per node-stage: shared 4*31*4 (weights) + 31*4 (idx) + 17*4 (pointwise)
@@ -340,6 +342,74 @@ def run_ensemble(args, level, desc, members=64):
         dist.destroy_process_group()
 
 
+def run_serving(args, desc):
+    """Seeded Poisson stream of forecast requests through the serving form."""
+    from swe_b200 import capi, gen, swe_input
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(args.seed)
+    levels = [4, 5, 6, 7]
+    models = {}
+    t0 = time.time()
+    for lv in levels:
+        d = gen.generate(lv, seed=1, device=f"cuda:{local}")
+        models[lv] = swe_input.to_model(d)
+    log(f"[bench] serving grids generated in {time.time() - t0:.1f}s")
+    srv = capi.Server(args.budget_gb * 1e9, max_requests=512)
+    capi.check("swe_cuda_select_device", srv.lib.swe_cuda_select_device(local))
+    gids = {lv: srv.add_grid(models[lv]) for lv in levels}
+    nreq = args.requests
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, nreq))
+    reqs = []
+    for k in range(nreq):
+        lv = levels[rng.integers(len(levels))]
+        members = int(rng.integers(1, 33))
+        steps = int(rng.integers(10, 501))
+        seed = int(rng.integers(1 << 30))
+        reqs.append((lv, members, steps, seed))
+    # initial states drawn as in the single-state case, per-request seeds
+    states = [np.stack([gen.perturb_h(models[lv].H_init, seed + b) for b in range(mb)])
+              for lv, mb, st, seed in reqs]
+    launches0 = capi.kernel_launches()
+    ids = []
+    start = time.perf_counter()
+    for k, (lv, mb, st, seed) in enumerate(reqs):
+        delay = arrivals[k] - (time.perf_counter() - start)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(gids[lv], states[k], st))
+    res = srv.wait(ids, timeout=600.0)
+    wall = time.perf_counter() - start
+    stats = srv.stats()
+    outs = [srv.fetch(r) for r in ids]
+    srv.stop()
+    lat = np.array([res[r][2] for r in ids])
+    wait_admit = np.array([res[r][1] for r in ids])
+    member_steps = sum(mb * st for lv, mb, st, seed in reqs)
+    node_stages = sum(4.0 * models[lv].N * mb * st for lv, mb, st, seed in reqs)
+    if rank == 0:
+        line = {
+            "metric": "serving: aggregate member-steps/s with p50/p99 request latency",
+            "value": member_steps / wall, "unit": "member-steps/s", "n_gpus": 1, "steps": None,
+            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded request stream",
+            "config": {"workload": args.workload, "description": desc, "requests": nreq,
+                       "arrival_rate_per_s": args.rate, "seed": args.seed, "budget_bytes": args.budget_gb * 1e9},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+            "admission_wait_s": {"p50": float(np.percentile(wait_admit, 50)),
+                                 "p99": float(np.percentile(wait_admit, 99))},
+            "node_stage_updates_per_s": node_stages / wall,
+            "wall_s": wall, "server": stats,
+            "gpu_launches": int(capi.kernel_launches() - launches0),
+            "state_finite": bool(all(np.isfinite(o).all() for o in outs)),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -350,13 +420,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--err-steps", type=int, default=100)
     ap.add_argument("--err-members", type=int, default=4)
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--rate", type=float, default=4.0)
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--budget-gb", type=float, default=80.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     level, prec, desc = WORKLOADS[args.workload]
     if args.impl == "reference":
-        return run_reference(args, level, "fp64" if prec == "tf32x3" else prec, args.workload)
+        return run_reference(args, level if level else 6, "fp64" if prec in ("tf32x3", "serve") else prec,
+                             args.workload)
     if prec == "tf32x3":
         return run_ensemble(args, level, desc)
+    if prec == "serve":
+        return run_serving(args, desc)
 
     import torch
     import torch.distributed as dist

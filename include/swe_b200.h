@@ -161,6 +161,38 @@ void* swe_ens_stream(void);
 int swe_ens_finalize(void);
 
 /* ---------------------------------------------------------------------------
+ * Serving form (continuous batching of forecast requests)
+ * ------------------------------------------------------------------------- */
+
+/* No reference counterpart (the reference runs one solve per process).
+ * swe_srv_start reserves `budget_bytes` of device memory as the arena that
+ * requests are admitted into, and starts the scheduler thread and the
+ * persistent kernel.  Grids are registered once (canonical FP64 arrays as for
+ * swe_ens_init, in the node order the caller wants them stepped) and stay
+ * resident; swe_srv_add_grid returns a grid id >= 0 or -status.
+ * swe_srv_submit queues a request (1..32 members, nsteps RK4 steps, initial
+ * states [members][n][4] FP64, copied at once) and returns its id >= 0 or
+ * -status; requests run as soon as arena space frees up, stepped together in
+ * the FP64 plain-form arithmetic.  swe_srv_poll returns 0 while queued or
+ * running, 1 when done, 2 when cancelled (times[2] = seconds from submission
+ * to admission and to completion, -1 until known); swe_srv_fetch copies the
+ * final states and forgets the request.  swe_srv_stats fills out[9] =
+ * {kernel launches, admitted, completed, arena bytes in use, peak bytes in
+ * use, budget, work items done, queued requests, running requests}. */
+int swe_srv_start(double budget_bytes, int max_requests);
+int swe_srv_add_grid(int n, int nnbr, double gh0, double dt, const int* idx,
+                     const double* Dx, const double* Dy, const double* Dz, const double* L,
+                     const double* x, const double* y, const double* z, const double* f,
+                     const double* ghm, const double* p_u, const double* p_v, const double* p_w,
+                     const double* gradghm);
+int swe_srv_submit(int grid, int members, int nsteps, const double* H0);
+int swe_srv_poll(int request, double* times);
+int swe_srv_fetch(int request, double* H);
+int swe_srv_cancel(int request);
+int swe_srv_stats(double* out);
+int swe_srv_stop(void);
+
+/* ---------------------------------------------------------------------------
  * Plain form without device allocation
  * ------------------------------------------------------------------------- */
 

@@ -1,0 +1,727 @@
+// Serving form: swe_srv_* entry points of include/swe_b200.h.
+//
+// Forecast requests (a grid, 1-32 members, a number of RK4 steps, initial
+// states) arrive while others run.  A host scheduler thread admits them as
+// device memory frees up (first fit in one arena of the configured HBM budget),
+// uploads their states on a copy stream, and appends their work to a queue in
+// mapped pinned memory: round-robin over the active requests, one RK4 step
+// (4 stages x node chunks) per request per round, so that new requests join
+// the mix at once.  One persistent kernel -- one CTA per SM slot -- claims work
+// items from that queue, waits (bounded) until the request's previous stage
+// has completed everywhere, runs the plain form's fused FP64 stage math on the
+// chunk for every member, and publishes completion counters; the last item of
+// a request raises its completion flag in host memory.  The per-node math is
+// that of the plain stage kernel, with the same packed weight layout and lane
+// split, so a request's result does not depend on what it was mixed with.
+//
+// Waits are bounded (%globaltimer): an idle kernel exits after a while (the
+// scheduler relaunches it when work arrives) and a dependency that is never
+// met ends the kernel with an error flag instead of hanging the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+#include "stage_kernel.cuh"
+
+namespace swe {
+namespace srv {
+
+struct Item {            // one queue entry (16 bytes)
+    int slot;            // request slot
+    int q;               // stage index within the request: step * 4 + stage
+    int begin, end;      // node range
+};
+
+struct alignas(16) ReqDesc {   // device table entry of an admitted request
+    const uint4* W;      // grid: packed weights
+    const int4* idx;     // grid: packed stencil indices
+    const double* PT;    // grid: pointwise records
+    int n;               // nodes
+    int members;
+    int nchunks;         // items per stage
+    int total;           // items of the whole request
+    int id;              // request id (written into the completion flag)
+    int cancelled;
+    double gh0, dt;
+    double* H;           // [members][n][4]
+    double* Ka;
+    double* Kb;
+    double* D;
+};
+
+struct Shared {          // host-mapped control block
+    volatile long long tail;       // items published by the host
+    volatile int stop;             // host asks the kernel to exit
+    volatile int error;            // kernel-side error code
+    volatile long long progress;   // items completed (approximate mirror)
+};
+
+constexpr int kThreads = kStageThreads;         // 8 warps x 4 nodes
+static_assert(sizeof(ReqDesc) % 16 == 0 && sizeof(ReqDesc) / 16 <= kStageThreads, "descriptor copy");
+constexpr unsigned long long kIdleNs = 20ull * 1000 * 1000;          // idle exit after 20 ms
+constexpr unsigned long long kDepNs = 10ull * 1000 * 1000 * 1000;    // dependency wait limit 10 s
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void load_row_cg(const double* p, double (&v)[4]) {
+    const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+// One warp, 4 nodes [base, base+4) of one member and one stage; the plain
+// stage kernel's math with L2-coherent loads of everything the kernel itself
+// writes (states change between stages inside one launch).
+__device__ void serve_group(const ReqDesc& r, int stage, long base, long end, double* __restrict__ Hm,
+                            double* __restrict__ Kam, double* __restrict__ Kbm, double* __restrict__ Dm,
+                            double (*red)[16], int k, int g) {
+    const long i = base + g;
+    const bool valid = i < end;
+    const long ii = valid ? i : end - 1;
+    const double* Kin = stage == 0 ? Hm : stage == 1 ? Kam : stage == 2 ? Kbm : Kam;
+    double* Kout = stage == 0 ? Kam : stage == 1 ? Kbm : Kam;
+    const int4 nb = __ldg(r.idx + ii * 8 + k);
+    const int nbr[4] = {nb.x, nb.y, nb.z, nb.w};
+    double w[kSlotChunks][4], kv[kSlotChunks][4];
+#pragma unroll
+    for (int m = 0; m < kSlotChunks; ++m) Quad<double>::load(r.W, ((ii * kSlotChunks + m) * 2) * 8 + k, w[m]);
+#pragma unroll
+    for (int m = 0; m < kSlotChunks; ++m) load_row_cg(Kin + 4L * nbr[m], kv[m]);
+    double acc[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) acc[t] = 0.0;
+#pragma unroll
+    for (int m = 0; m < kSlotChunks; ++m)
+#pragma unroll
+        for (int op = 0; op < 4; ++op)
+#pragma unroll
+            for (int f = 0; f < 4; ++f) acc[op * 4 + f] += w[m][op] * kv[m][f];
+    double r0, r1;
+    reduce_scatter8(acc, k, r0, r1);
+    red[g][2 * k] = r0;
+    red[g][2 * k + 1] = r1;
+    __syncwarp();
+    if (k == 0 && valid) {
+        double s[16], q[4], F[4];
+#pragma unroll
+        for (int t = 0; t < 16; ++t) s[t] = red[g][t];
+        load_row_cg(Kin + 4 * i, q);
+        pointwise_rhs(s, q, r.PT + i * kPointStride, r.gh0, F);
+        const double dt = r.dt;
+        if (stage == 0) {
+            double kn[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) kn[t] = Quad<double>::axpy(q[t], dt / 2.0, F[t]);
+            Quad<double>::store_row(Dm + 4 * i, F);
+            Quad<double>::store_row(Kout + 4 * i, kn);
+        } else if (stage < 3) {
+            double h[4], d[4], kn[4];
+            load_row_cg(Hm + 4 * i, h);
+            load_row_cg(Dm + 4 * i, d);
+            const double c = stage == 1 ? dt / 2.0 : dt;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                d[t] = Quad<double>::axpy(d[t], 2.0, F[t]);
+                kn[t] = Quad<double>::axpy(h[t], c, F[t]);
+            }
+            Quad<double>::store_row(Dm + 4 * i, d);
+            Quad<double>::store_row(Kout + 4 * i, kn);
+        } else {
+            double h[4], d[4];
+            load_row_cg(Hm + 4 * i, h);
+            load_row_cg(Dm + 4 * i, d);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                d[t] = Quad<double>::axpy(d[t], 1.0, F[t]);
+                h[t] = Quad<double>::update_h(h[t], dt / 6.0, d[t]);
+            }
+            Quad<double>::store_row(Hm + 4 * i, h);
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, unsigned long long* head,
+             const ReqDesc* __restrict__ reqs, int* done, int* flags, unsigned long long* items_done) {
+    __shared__ double red[kStageWarps][4][16];
+    __shared__ long long s_pos;
+    __shared__ Item s_item;
+    __shared__ int s_ok;
+    __shared__ ReqDesc s_req;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 3, k = lane & 7;
+    unsigned long long idle_since = globaltimer();
+    while (true) {
+        if (threadIdx.x == 0) {
+            long long got = -1;
+            while (true) {
+                if (ctl->stop || ctl->error) break;
+                const unsigned long long h = *(volatile unsigned long long*)head;
+                const long long t = ctl->tail;
+                if ((long long)h < t) {
+                    if (atomicCAS(head, h, h + 1) == h) { got = (long long)h; break; }
+                    continue;
+                }
+                if (globaltimer() - idle_since > kIdleNs) break;     // idle: let the host relaunch later
+                __nanosleep(2000);
+            }
+            s_pos = got;
+            if (got >= 0) {
+                const volatile Item* vi = ring + got % ring_cap;
+                s_item.slot = vi->slot;
+                s_item.q = vi->q;
+                s_item.begin = vi->begin;
+                s_item.end = vi->end;
+            }
+        }
+        __syncthreads();
+        if (s_pos < 0) return;
+        const Item it = s_item;
+        // slots are reused by later requests: read the descriptor through L2
+        if (threadIdx.x < (int)(sizeof(ReqDesc) / 16))
+            reinterpret_cast<uint4*>(&s_req)[threadIdx.x] =
+                __ldcg(reinterpret_cast<const uint4*>(reqs + it.slot) + threadIdx.x);
+        __syncthreads();
+        const ReqDesc& r = s_req;
+        // dependency: every chunk of the previous stage index has completed
+        if (threadIdx.x == 0) {
+            s_ok = 1;
+            const int need = it.q * r.nchunks;
+            const unsigned long long t0 = globaltimer();
+            while (atomicAdd(done + it.slot, 0) < need) {
+                if (ctl->stop) { s_ok = 0; break; }
+                if (globaltimer() - t0 > kDepNs) {
+                    s_ok = 0;
+                    ctl->error = 2;
+                    break;
+                }
+                __nanosleep(500);
+            }
+            __threadfence();
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        if (!r.cancelled) {
+            const int stage = it.q & 3;
+            const long nmem = 4L * r.n;
+            for (int mbr = 0; mbr < r.members; ++mbr) {
+                double* Hm = r.H + mbr * nmem;
+                double* Kam = r.Ka + mbr * nmem;
+                double* Kbm = r.Kb + mbr * nmem;
+                double* Dm = r.D + mbr * nmem;
+                for (long base = it.begin + warp * 4L; base < it.end; base += kStageWarps * 4L)
+                    serve_group(r, stage, base, it.end, Hm, Kam, Kbm, Dm, red[warp], k, g);
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int c = atomicAdd(done + it.slot, 1) + 1;
+            const unsigned long long d = atomicAdd(items_done, 1ull) + 1;
+            if ((d & 63) == 0) ctl->progress = (long long)d;
+            if (c == r.total) {
+                __threadfence_system();
+                ((volatile int*)flags)[it.slot] = r.id;
+                __threadfence_system();
+            }
+        }
+        idle_since = globaltimer();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+
+struct Grid {
+    int n, nnbr;
+    double gh0, dt;
+    void* W = nullptr;
+    int* idx = nullptr;
+    void* PT = nullptr;
+};
+
+struct Request {
+    int id, grid, members, nsteps, slot = -1;
+    size_t offset = 0, bytes = 0;
+    std::vector<double> h0;              // host copy of the initial state
+    std::vector<double> result;
+    int next_step = 0;                   // steps appended so far
+    enum State { PENDING, RUNNING, DRAINING, DONE, CANCELLED, FAILED } state = PENDING;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    bool cancel_req = false;
+};
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Server {
+    bool running = false;
+    int device = 0, sms = 0, per_sm = 0, max_slots = 0;
+    size_t budget = 0, in_use = 0, peak = 0;
+    char* arena = nullptr;
+    std::map<size_t, size_t> free_blocks;         // offset -> size
+    Shared* ctl = nullptr;                        // mapped
+    Item* ring = nullptr;                         // mapped
+    long long ring_cap = 0, tail = 0;
+    int* flags = nullptr;                         // mapped [max_slots]
+    unsigned long long* head = nullptr;           // device
+    unsigned long long* items_done = nullptr;     // device
+    ReqDesc* reqs_d = nullptr;                    // device
+    int* done_d = nullptr;                        // device
+    std::vector<int> free_slots;
+    std::vector<Grid> grids;
+    std::map<int, Request> requests;
+    std::deque<int> pending;
+    std::vector<int> active;                      // slots order for round-robin
+    int next_id = 0;
+    cudaStream_t kstream = nullptr, cstream = nullptr;
+    long long launches = 0, admitted = 0, completed = 0;
+    std::thread worker;
+    std::mutex mu;
+    std::atomic<bool> quit{false};
+    std::string fatal;
+
+    // first-fit allocation in the arena
+    bool alloc(size_t bytes, size_t& off) {
+        for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
+            if (it->second >= bytes) {
+                off = it->first;
+                const size_t rest = it->second - bytes;
+                const size_t noff = it->first + bytes;
+                free_blocks.erase(it);
+                if (rest) free_blocks[noff] = rest;
+                in_use += bytes;
+                peak = std::max(peak, in_use);
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes) {
+        in_use -= bytes;
+        auto it = free_blocks.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_blocks.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_blocks.erase(nx);
+        }
+        if (it != free_blocks.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_blocks.erase(it);
+            }
+        }
+    }
+
+    static size_t state_bytes(int n, int members) {
+        const size_t one = (size_t)n * 4 * sizeof(double) * members;
+        return ((one + 255) / 256 * 256) * 4;      // H, Ka, Kb, D
+    }
+    static int chunk_nodes(int n, int members) {
+        int c = std::max(1024, 65536 / std::max(members, 1));
+        c = (c + 31) / 32 * 32;
+        return std::min(c, n);
+    }
+
+    bool kernel_running() { return cudaStreamQuery(kstream) == cudaErrorNotReady; }
+
+    void launch_kernel() {
+        serve_kernel<<<sms * std::max(per_sm, 1), kThreads, 0, kstream>>>(ctl, ring, ring_cap, head, reqs_d, done_d,
+                                                                         flags, items_done);
+        ++launches;
+        count_launch();
+    }
+
+    // append one RK4 step (4 stage indices x chunks) of request r
+    void append_step(Request& r) {
+        const Grid& G = grids[r.grid];
+        const int cn = chunk_nodes(G.n, r.members);
+        const int nch = (G.n + cn - 1) / cn;
+        for (int st = 0; st < 4; ++st) {
+            const int q = r.next_step * 4 + st;
+            for (int c = 0; c < nch; ++c) {
+                Item& it = ring[tail % ring_cap];
+                it.slot = r.slot;
+                it.q = q;
+                it.begin = c * cn;
+                it.end = std::min(G.n, (c + 1) * cn);
+                ++tail;
+            }
+        }
+        ++r.next_step;
+    }
+
+    int admit(Request& r) {
+        size_t off;
+        if (free_slots.empty() || !alloc(r.bytes, off)) return 0;
+        const Grid& G = grids[r.grid];
+        r.offset = off;
+        r.slot = free_slots.back();
+        free_slots.pop_back();
+        const size_t one = r.bytes / 4;
+        ReqDesc d{};
+        d.W = reinterpret_cast<const uint4*>(G.W);
+        d.idx = reinterpret_cast<const int4*>(G.idx);
+        d.PT = reinterpret_cast<const double*>(G.PT);
+        d.n = G.n;
+        d.members = r.members;
+        const int cn = chunk_nodes(G.n, r.members);
+        d.nchunks = (G.n + cn - 1) / cn;
+        d.total = d.nchunks * 4 * r.nsteps;
+        d.id = r.id;
+        d.cancelled = 0;
+        d.gh0 = G.gh0;
+        d.dt = G.dt;
+        d.H = reinterpret_cast<double*>(arena + off);
+        d.Ka = reinterpret_cast<double*>(arena + off + one);
+        d.Kb = reinterpret_cast<double*>(arena + off + 2 * one);
+        d.D = reinterpret_cast<double*>(arena + off + 3 * one);
+        int zero = 0;
+        flags[r.slot] = -1;
+        cudaMemcpyAsync(d.H, r.h0.data(), r.h0.size() * sizeof(double), cudaMemcpyHostToDevice, cstream);
+        cudaMemcpyAsync(reqs_d + r.slot, &d, sizeof(d), cudaMemcpyHostToDevice, cstream);
+        cudaMemcpyAsync(done_d + r.slot, &zero, sizeof(int), cudaMemcpyHostToDevice, cstream);
+        if (cudaStreamSynchronize(cstream) != cudaSuccess) {
+            fatal = "request upload failed";
+            return -1;
+        }
+        std::vector<double>().swap(r.h0);
+        r.state = Request::RUNNING;
+        r.t_admit = now_s();
+        active.push_back(r.id);
+        ++admitted;
+        return 1;
+    }
+
+    void finish(Request& r, Request::State st) {
+        const Grid& G = grids[r.grid];
+        r.result.resize((size_t)r.members * G.n * 4);
+        if (st == Request::DONE) {
+            cudaMemcpyAsync(r.result.data(), arena + r.offset, r.result.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, cstream);
+            cudaStreamSynchronize(cstream);
+        }
+        release(r.offset, r.bytes);
+        free_slots.push_back(r.slot);
+        r.slot = -1;
+        r.t_done = now_s();
+        r.state = st;
+        ++completed;
+    }
+
+    // one scheduler pass (called with mu held)
+    void pass() {
+        // completions
+        for (size_t a = 0; a < active.size();) {
+            Request& r = requests[active[a]];
+            if (r.slot >= 0 && ((volatile int*)flags)[r.slot] == r.id) {
+                finish(r, r.cancel_req ? Request::CANCELLED : Request::DONE);
+                active.erase(active.begin() + a);
+            } else {
+                ++a;
+            }
+        }
+        // admissions: FIFO, later requests may overtake one that does not fit yet
+        for (auto it = pending.begin(); it != pending.end();) {
+            Request& r = requests[*it];
+            const int st = admit(r);
+            if (st < 0) return;
+            if (st == 1) it = pending.erase(it);
+            else ++it;
+        }
+        // work: one step per active request per round while the queue is short
+        const long long done_items = ctl->progress;
+        bool appended = false;
+        for (int round = 0; round < 4 && tail - done_items < (long long)sms * 64; ++round) {
+            bool any = false;
+            for (int id : active) {
+                Request& r = requests[id];
+                if (r.next_step < r.nsteps) {
+                    if (tail + 4LL * 4096 > ring_cap + done_items) break;   // ring full
+                    append_step(r);
+                    any = appended = true;
+                }
+            }
+            if (!any) break;
+        }
+        if (appended) {
+            std::atomic_thread_fence(std::memory_order_seq_cst);
+            ctl->tail = tail;
+        }
+        const bool work = ctl->tail > (long long)ctl->progress || !active.empty();
+        if (ctl->error) {
+            fatal = ctl->error == 2 ? "serving kernel: a dependency wait ran out" : "serving kernel error";
+            return;
+        }
+        if (work && !kernel_running()) launch_kernel();
+    }
+
+    void loop() {
+        while (!quit.load()) {
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                if (fatal.empty()) pass();
+            }
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+    }
+};
+
+Server* g_srv = nullptr;
+
+}  // namespace srv
+}  // namespace swe
+
+using namespace swe;
+using namespace swe::srv;
+
+extern "C" {
+
+int swe_srv_start(double budget_bytes, int max_requests) {
+    if (g_srv) { set_error("swe_srv_start: server already running"); return SWE_ERR_STATE; }
+    if (budget_bytes < (1 << 20) || max_requests <= 0 || max_requests > 4096) {
+        set_error("swe_srv_start: need budget >= 1 MiB and 1 <= max_requests <= 4096");
+        return SWE_ERR_ARG;
+    }
+    Server* S = new Server();
+    S->budget = (size_t)budget_bytes;
+    S->max_slots = max_requests;
+    cudaError_t e;
+    auto fail = [&](const char* what) {
+        set_error("swe_srv_start: %s: %s", what, cudaGetErrorString(e));
+        delete S;
+        return SWE_ERR_CUDA;
+    };
+    if ((e = cudaGetDevice(&S->device)) != cudaSuccess) return fail("cudaGetDevice");
+    cudaDeviceGetAttribute(&S->sms, cudaDevAttrMultiProcessorCount, S->device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&S->per_sm, serve_kernel, kThreads, 0);
+    if ((e = cudaMalloc(&S->arena, S->budget)) != cudaSuccess) {
+        set_error("swe_srv_start: cannot reserve the %.3g-byte HBM budget: %s", budget_bytes, cudaGetErrorString(e));
+        delete S;
+        return SWE_ERR_NOMEM;
+    }
+    S->free_blocks[0] = S->budget;
+    S->ring_cap = 1LL << 22;
+    if ((e = cudaHostAlloc(&S->ctl, sizeof(Shared), cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc");
+    if ((e = cudaHostAlloc(&S->ring, sizeof(Item) * S->ring_cap, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc ring");
+    if ((e = cudaHostAlloc(&S->flags, sizeof(int) * max_requests, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc flags");
+    memset((void*)S->ctl, 0, sizeof(Shared));
+    for (int i = 0; i < max_requests; ++i) S->flags[i] = -1;
+    if ((e = cudaMalloc(&S->head, sizeof(unsigned long long))) != cudaSuccess) return fail("cudaMalloc head");
+    if ((e = cudaMalloc(&S->items_done, sizeof(unsigned long long))) != cudaSuccess) return fail("cudaMalloc counter");
+    if ((e = cudaMalloc(&S->reqs_d, sizeof(ReqDesc) * max_requests)) != cudaSuccess) return fail("cudaMalloc table");
+    if ((e = cudaMalloc(&S->done_d, sizeof(int) * max_requests)) != cudaSuccess) return fail("cudaMalloc done");
+    cudaMemset(S->head, 0, sizeof(unsigned long long));
+    cudaMemset(S->items_done, 0, sizeof(unsigned long long));
+    cudaMemset(S->reqs_d, 0, sizeof(ReqDesc) * max_requests);
+    cudaMemset(S->done_d, 0, sizeof(int) * max_requests);
+    cudaStreamCreateWithFlags(&S->kstream, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&S->cstream, cudaStreamNonBlocking);
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail("setup");
+    for (int i = max_requests - 1; i >= 0; --i) S->free_slots.push_back(i);
+    S->running = true;
+    g_srv = S;
+    S->worker = std::thread([S]() {
+        cudaSetDevice(S->device);
+        S->loop();
+    });
+    return SWE_OK;
+}
+
+int swe_srv_add_grid(int n, int nnbr, double gh0, double dt, const int* idx, const double* Dx, const double* Dy,
+                     const double* Dz, const double* L, const double* x, const double* y, const double* z,
+                     const double* f, const double* ghm, const double* p_u, const double* p_v, const double* p_w,
+                     const double* gradghm) {
+    if (!g_srv) { set_error("swe_srv_add_grid: server not started"); return -SWE_ERR_STATE; }
+    if (n <= 0 || nnbr <= 0 || nnbr > kSlots) { set_error("swe_srv_add_grid: bad sizes"); return -SWE_ERR_ARG; }
+    // pack exactly as the plain form packs a CFDL patch (node order as given)
+    std::vector<double> wbuf((size_t)n * kSlotChunks * 2 * 8 * 2, 0.0), pbuf((size_t)n * kPointStride, 0.0);
+    std::vector<int> ibuf((size_t)n * kSlots, 0);
+    const double* ops[4] = {Dx, Dy, Dz, L};
+    for (long i = 0; i < n; ++i) {
+        for (int j = 0; j < kSlots; ++j) {
+            int p = (int)i;
+            if (j < nnbr) {
+                p = idx[i * nnbr + j];
+                if (p < 0 || p >= n) { set_error("swe_srv_add_grid: idx out of range"); return -SWE_ERR_INDEX; }
+                for (int op = 0; op < 4; ++op) {
+                    const size_t unit = (((size_t)i * kSlotChunks + j / 8) * 2 + op / 2) * 8 + j % 8;
+                    wbuf[unit * 2 + op % 2] = ops[op][i * nnbr + j];
+                }
+            }
+            ibuf[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)] = p;
+        }
+        double* r = &pbuf[(size_t)i * kPointStride];
+        r[PT_X] = x[i]; r[PT_Y] = y[i]; r[PT_Z] = z[i]; r[PT_F] = f[i]; r[PT_GHM] = ghm[i];
+        for (int c = 0; c < 3; ++c) {
+            r[PT_PU + c] = p_u[i * 3 + c]; r[PT_PV + c] = p_v[i * 3 + c];
+            r[PT_PW + c] = p_w[i * 3 + c]; r[PT_GG + c] = gradghm[i * 3 + c];
+        }
+    }
+    Grid G;
+    G.n = n; G.nnbr = nnbr; G.gh0 = gh0; G.dt = dt;
+    cudaError_t e;
+    if ((e = cudaMalloc(&G.W, wbuf.size() * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&G.idx, ibuf.size() * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&G.PT, pbuf.size() * 8)) != cudaSuccess) {
+        set_error("swe_srv_add_grid: %s", cudaGetErrorString(e));
+        return -SWE_ERR_NOMEM;
+    }
+    cudaMemcpy(G.W, wbuf.data(), wbuf.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(G.idx, ibuf.data(), ibuf.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(G.PT, pbuf.data(), pbuf.size() * 8, cudaMemcpyHostToDevice);
+    std::lock_guard<std::mutex> lock(g_srv->mu);
+    g_srv->grids.push_back(G);
+    return (int)g_srv->grids.size() - 1;
+}
+
+int swe_srv_submit(int grid, int members, int nsteps, const double* H0) {
+    if (!g_srv) { set_error("swe_srv_submit: server not started"); return -SWE_ERR_STATE; }
+    Server& S = *g_srv;
+    std::lock_guard<std::mutex> lock(S.mu);
+    if (!S.fatal.empty()) { set_error("%s", S.fatal.c_str()); return -SWE_ERR_TIMEOUT; }
+    if (grid < 0 || grid >= (int)S.grids.size()) { set_error("swe_srv_submit: unknown grid %d", grid); return -SWE_ERR_ARG; }
+    if (members < 1 || members > 32 || nsteps < 1 || !H0) {
+        set_error("swe_srv_submit: need 1 <= members <= 32, nsteps >= 1 and initial states");
+        return -SWE_ERR_ARG;
+    }
+    const Grid& G = S.grids[grid];
+    Request r;
+    r.id = S.next_id++;
+    r.grid = grid;
+    r.members = members;
+    r.nsteps = nsteps;
+    r.bytes = Server::state_bytes(G.n, members);
+    if (r.bytes > S.budget) {
+        set_error("swe_srv_submit: request needs %zu bytes, more than the whole budget", r.bytes);
+        return -SWE_ERR_NOMEM;
+    }
+    r.h0.assign(H0, H0 + (size_t)members * G.n * 4);
+    r.t_submit = now_s();
+    S.requests[r.id] = std::move(r);
+    S.pending.push_back(S.requests.rbegin()->first);
+    return S.requests.rbegin()->first;
+}
+
+int swe_srv_poll(int id, double* times) {
+    if (!g_srv) { set_error("swe_srv_poll: server not started"); return -SWE_ERR_STATE; }
+    Server& S = *g_srv;
+    std::lock_guard<std::mutex> lock(S.mu);
+    if (!S.fatal.empty()) { set_error("%s", S.fatal.c_str()); return -SWE_ERR_TIMEOUT; }
+    auto it = S.requests.find(id);
+    if (it == S.requests.end()) { set_error("swe_srv_poll: unknown request %d", id); return -SWE_ERR_ARG; }
+    const Request& r = it->second;
+    if (times) {
+        times[0] = r.t_admit > 0 ? r.t_admit - r.t_submit : -1.0;
+        times[1] = r.t_done > 0 ? r.t_done - r.t_submit : -1.0;
+    }
+    switch (r.state) {
+        case Request::DONE: return 1;
+        case Request::CANCELLED: return 2;
+        default: return 0;
+    }
+}
+
+int swe_srv_fetch(int id, double* H) {
+    if (!g_srv) { set_error("swe_srv_fetch: server not started"); return SWE_ERR_STATE; }
+    Server& S = *g_srv;
+    std::lock_guard<std::mutex> lock(S.mu);
+    auto it = S.requests.find(id);
+    if (it == S.requests.end()) { set_error("swe_srv_fetch: unknown request %d", id); return SWE_ERR_ARG; }
+    Request& r = it->second;
+    if (r.state != Request::DONE) { set_error("swe_srv_fetch: request %d has not completed", id); return SWE_ERR_STATE; }
+    if (H) memcpy(H, r.result.data(), r.result.size() * sizeof(double));
+    S.requests.erase(it);
+    return SWE_OK;
+}
+
+int swe_srv_cancel(int id) {
+    if (!g_srv) { set_error("swe_srv_cancel: server not started"); return SWE_ERR_STATE; }
+    Server& S = *g_srv;
+    std::lock_guard<std::mutex> lock(S.mu);
+    auto it = S.requests.find(id);
+    if (it == S.requests.end()) { set_error("swe_srv_cancel: unknown request %d", id); return SWE_ERR_ARG; }
+    Request& r = it->second;
+    r.cancel_req = true;
+    if (r.state == Request::PENDING) {
+        S.pending.erase(std::remove(S.pending.begin(), S.pending.end(), id), S.pending.end());
+        r.state = Request::CANCELLED;
+        r.t_done = now_s();
+        return SWE_OK;
+    }
+    if (r.state == Request::RUNNING && r.slot >= 0) {
+        // the kernel skips the compute of a cancelled request's remaining items
+        const int one = 1;
+        cudaMemcpyAsync(&S.reqs_d[r.slot].cancelled, &one, sizeof(int), cudaMemcpyHostToDevice, S.cstream);
+        cudaStreamSynchronize(S.cstream);
+        // the rest of its steps still have to pass through the queue to retire it
+    }
+    return SWE_OK;
+}
+
+int swe_srv_stats(double* out) {
+    if (!g_srv) { set_error("swe_srv_stats: server not started"); return SWE_ERR_STATE; }
+    Server& S = *g_srv;
+    std::lock_guard<std::mutex> lock(S.mu);
+    out[0] = (double)S.launches;
+    out[1] = (double)S.admitted;
+    out[2] = (double)S.completed;
+    out[3] = (double)S.in_use;
+    out[4] = (double)S.peak;
+    out[5] = (double)S.budget;
+    out[6] = (double)S.ctl->progress;
+    out[7] = (double)S.pending.size();
+    out[8] = (double)S.active.size();
+    return SWE_OK;
+}
+
+int swe_srv_stop(void) {
+    if (!g_srv) return SWE_OK;
+    Server* S = g_srv;
+    S->quit = true;
+    if (S->worker.joinable()) S->worker.join();
+    S->ctl->stop = 1;
+    cudaStreamSynchronize(S->kstream);
+    cudaStreamSynchronize(S->cstream);
+    for (auto& G : S->grids) {
+        cudaFree(G.W);
+        cudaFree(G.idx);
+        cudaFree(G.PT);
+    }
+    cudaFree(S->arena);
+    cudaFree(S->head);
+    cudaFree(S->items_done);
+    cudaFree(S->reqs_d);
+    cudaFree(S->done_d);
+    cudaFreeHost((void*)S->ctl);
+    cudaFreeHost(S->ring);
+    cudaFreeHost(S->flags);
+    cudaStreamDestroy(S->kstream);
+    cudaStreamDestroy(S->cstream);
+    const bool err = !S->fatal.empty();
+    std::string msg = S->fatal;
+    delete S;
+    g_srv = nullptr;
+    if (err) { set_error("%s", msg.c_str()); return SWE_ERR_TIMEOUT; }
+    return SWE_OK;
+}
+
+}  // extern "C"

@@ -69,6 +69,13 @@ def load() -> ctypes.CDLL:
     lib.swe_ens_set_timing.argtypes = [i]
     lib.swe_ens_use_variant.argtypes = [i, i]
     lib.swe_ens_stream.restype = vp
+    lib.swe_srv_start.argtypes = [d, i]
+    lib.swe_srv_add_grid.argtypes = [i, i, d, d] + [vp] * 14
+    lib.swe_srv_submit.argtypes = [i, i, i, vp]
+    lib.swe_srv_poll.argtypes = [i, vp]
+    lib.swe_srv_fetch.argtypes = [i, vp]
+    lib.swe_srv_cancel.argtypes = [i]
+    lib.swe_srv_stats.argtypes = [vp]
     _lib = lib
     return lib
 
@@ -279,3 +286,79 @@ class Ensemble:
 
     def finalize(self) -> None:
         check("swe_ens_finalize", self.lib.swe_ens_finalize())
+
+
+class Server:
+    """The serving form (swe_srv_*): continuous batching of forecast requests."""
+
+    STAT_NAMES = ("kernel_launches", "admitted", "completed", "bytes_in_use", "peak_bytes", "budget",
+                  "items_done", "queued", "running")
+
+    def __init__(self, budget_bytes: float, max_requests: int = 256):
+        self.lib = load()
+        check("swe_srv_start", self.lib.swe_srv_start(float(budget_bytes), int(max_requests)))
+        self.grids = {}
+        self.meta = {}
+        self._keep = []
+
+    def add_grid(self, model) -> int:
+        arrs = {k: np.ascontiguousarray(getattr(model, k), dtype=np.float64) for k in
+                ("Dx", "Dy", "Dz", "L", "x", "y", "z", "f", "ghm", "p_u", "p_v", "p_w", "gradghm")}
+        idx = np.ascontiguousarray(model.idx, dtype=np.int32)
+        gid = self.lib.swe_srv_add_grid(model.N, model.Nnbr, float(model.gh0), float(model.dt), _p(idx),
+                                        *[_p(arrs[k]) for k in ("Dx", "Dy", "Dz", "L", "x", "y", "z", "f",
+                                                                "ghm", "p_u", "p_v", "p_w", "gradghm")])
+        if gid < 0:
+            check("swe_srv_add_grid", -gid)
+        self.grids[gid] = model.N
+        return gid
+
+    def submit(self, grid: int, H0: np.ndarray, nsteps: int) -> int:
+        H0 = np.ascontiguousarray(H0, dtype=np.float64).reshape(-1, self.grids[grid], 4)
+        rid = self.lib.swe_srv_submit(grid, H0.shape[0], int(nsteps), _p(H0))
+        if rid < 0:
+            check("swe_srv_submit", -rid)
+        self.meta[rid] = (grid, H0.shape[0])
+        return rid
+
+    def poll(self, rid: int):
+        """(state, admit_s, done_s): state 0 queued/running, 1 done, 2 cancelled."""
+        t = np.zeros(2)
+        st = self.lib.swe_srv_poll(rid, _p(t))
+        if st < 0:
+            check("swe_srv_poll", -st)
+        return st, float(t[0]), float(t[1])
+
+    def fetch(self, rid: int) -> np.ndarray:
+        grid, members = self.meta.pop(rid)
+        H = np.empty((members, self.grids[grid], 4))
+        check("swe_srv_fetch", self.lib.swe_srv_fetch(rid, _p(H)))
+        return H
+
+    def cancel(self, rid: int) -> None:
+        check("swe_srv_cancel", self.lib.swe_srv_cancel(rid))
+
+    def stats(self) -> dict:
+        out = np.zeros(9)
+        check("swe_srv_stats", self.lib.swe_srv_stats(_p(out)))
+        return dict(zip(self.STAT_NAMES, out.tolist()))
+
+    def wait(self, rids, timeout: float = 120.0) -> dict:
+        """Poll until every request in rids is done or cancelled; {rid: (state, admit_s, done_s)}."""
+        import time as _t
+
+        t0 = _t.time()
+        res = {}
+        while len(res) < len(rids):
+            for r in rids:
+                if r not in res:
+                    st = self.poll(r)
+                    if st[0] != 0:
+                        res[r] = st
+            if _t.time() - t0 > timeout:
+                raise TimeoutError(f"requests not done after {timeout}s: {sorted(set(rids) - set(res))}")
+            _t.sleep(0.0005)
+        return res
+
+    def stop(self) -> None:
+        check("swe_srv_stop", self.lib.swe_srv_stop())
