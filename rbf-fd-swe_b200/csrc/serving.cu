@@ -156,9 +156,14 @@ __device__ void serve_group(const ReqDesc& r, int stage, long base, long end, do
     __syncwarp();
 }
 
+// Exit is collective: the first CTA that has found the queue empty for kIdleNs
+// raises *exiting; from then on no CTA claims work (items already claimed are
+// finished), so every launch runs at full width and the host relaunches, with
+// *exiting cleared, once the kernel has ended and work is queued again.
 __global__ void __launch_bounds__(kThreads, 2)
 serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, unsigned long long* head,
-             const ReqDesc* __restrict__ reqs, int* done, int* flags, unsigned long long* items_done) {
+             const ReqDesc* __restrict__ reqs, int* done, int* flags, unsigned long long* items_done,
+             int* exiting) {
     __shared__ double red[kStageWarps][4][16];
     __shared__ long long s_pos;
     __shared__ Item s_item;
@@ -170,14 +175,17 @@ serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, uns
         if (threadIdx.x == 0) {
             long long got = -1;
             while (true) {
-                if (ctl->stop || ctl->error) break;
+                if (ctl->stop || ctl->error || *(volatile int*)exiting) break;
                 const unsigned long long h = *(volatile unsigned long long*)head;
                 const long long t = ctl->tail;
                 if ((long long)h < t) {
                     if (atomicCAS(head, h, h + 1) == h) { got = (long long)h; break; }
                     continue;
                 }
-                if (globaltimer() - idle_since > kIdleNs) break;     // idle: let the host relaunch later
+                if (globaltimer() - idle_since > kIdleNs) {           // idle: end this launch everywhere
+                    atomicExch(exiting, 1);
+                    break;
+                }
                 __nanosleep(2000);
             }
             s_pos = got;
@@ -283,6 +291,7 @@ struct Server {
     int* flags = nullptr;                         // mapped [max_slots]
     unsigned long long* head = nullptr;           // device
     unsigned long long* items_done = nullptr;     // device
+    int* exiting = nullptr;                       // device
     ReqDesc* reqs_d = nullptr;                    // device
     int* done_d = nullptr;                        // device
     std::vector<int> free_slots;
@@ -344,8 +353,9 @@ struct Server {
     bool kernel_running() { return cudaStreamQuery(kstream) == cudaErrorNotReady; }
 
     void launch_kernel() {
+        cudaMemsetAsync(exiting, 0, sizeof(int), kstream);
         serve_kernel<<<sms * std::max(per_sm, 1), kThreads, 0, kstream>>>(ctl, ring, ring_cap, head, reqs_d, done_d,
-                                                                         flags, items_done);
+                                                                         flags, items_done, exiting);
         ++launches;
         count_launch();
     }
@@ -529,6 +539,7 @@ int swe_srv_start(double budget_bytes, int max_requests) {
     if ((e = cudaMalloc(&S->items_done, sizeof(unsigned long long))) != cudaSuccess) return fail("cudaMalloc counter");
     if ((e = cudaMalloc(&S->reqs_d, sizeof(ReqDesc) * max_requests)) != cudaSuccess) return fail("cudaMalloc table");
     if ((e = cudaMalloc(&S->done_d, sizeof(int) * max_requests)) != cudaSuccess) return fail("cudaMalloc done");
+    if ((e = cudaMalloc(&S->exiting, sizeof(int))) != cudaSuccess) return fail("cudaMalloc exiting");
     cudaMemset(S->head, 0, sizeof(unsigned long long));
     cudaMemset(S->items_done, 0, sizeof(unsigned long long));
     cudaMemset(S->reqs_d, 0, sizeof(ReqDesc) * max_requests);
@@ -711,6 +722,7 @@ int swe_srv_stop(void) {
     cudaFree(S->items_done);
     cudaFree(S->reqs_d);
     cudaFree(S->done_d);
+    cudaFree(S->exiting);
     cudaFreeHost((void*)S->ctl);
     cudaFreeHost(S->ring);
     cudaFreeHost(S->flags);
