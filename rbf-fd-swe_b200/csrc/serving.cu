@@ -40,7 +40,8 @@ namespace srv {
 struct Item {            // one queue entry (16 bytes)
     int slot;            // request slot
     int q;               // stage index within the request: step * 4 + stage
-    int begin, end;      // node range
+    int chunk;           // node chunk [chunk * chunk_nodes, ...)
+    int member;          // ensemble member
 };
 
 struct alignas(16) ReqDesc {   // device table entry of an admitted request
@@ -49,7 +50,8 @@ struct alignas(16) ReqDesc {   // device table entry of an admitted request
     const double* PT;    // grid: pointwise records
     int n;               // nodes
     int members;
-    int nchunks;         // items per stage
+    int chunk_nodes;     // nodes per work item
+    int per_stage;       // items per stage: chunks x members
     int total;           // items of the whole request
     int id;              // request id (written into the completion flag)
     int cancelled;
@@ -162,7 +164,7 @@ __device__ void serve_group(const ReqDesc& r, int stage, long base, long end, do
 // *exiting cleared, once the kernel has ended and work is queued again.
 __global__ void __launch_bounds__(kThreads, 2)
 serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, unsigned long long* head,
-             const ReqDesc* __restrict__ reqs, int* done, int* flags, unsigned long long* items_done,
+             const ReqDesc* __restrict__ reqs, int* done, int* flags, int* mdone, unsigned long long* items_done,
              int* exiting) {
     __shared__ double red[kStageWarps][4][16];
     __shared__ long long s_pos;
@@ -193,8 +195,8 @@ serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, uns
                 const volatile Item* vi = ring + got % ring_cap;
                 s_item.slot = vi->slot;
                 s_item.q = vi->q;
-                s_item.begin = vi->begin;
-                s_item.end = vi->end;
+                s_item.chunk = vi->chunk;
+                s_item.member = vi->member;
             }
         }
         __syncthreads();
@@ -209,7 +211,7 @@ serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, uns
         // dependency: every chunk of the previous stage index has completed
         if (threadIdx.x == 0) {
             s_ok = 1;
-            const int need = it.q * r.nchunks;
+            const int need = it.q * r.per_stage;
             const unsigned long long t0 = globaltimer();
             while (atomicAdd(done + it.slot, 0) < need) {
                 if (ctl->stop) { s_ok = 0; break; }
@@ -226,20 +228,17 @@ serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, uns
         if (!s_ok) return;
         if (!r.cancelled) {
             const int stage = it.q & 3;
-            const long nmem = 4L * r.n;
-            for (int mbr = 0; mbr < r.members; ++mbr) {
-                double* Hm = r.H + mbr * nmem;
-                double* Kam = r.Ka + mbr * nmem;
-                double* Kbm = r.Kb + mbr * nmem;
-                double* Dm = r.D + mbr * nmem;
-                for (long base = it.begin + warp * 4L; base < it.end; base += kStageWarps * 4L)
-                    serve_group(r, stage, base, it.end, Hm, Kam, Kbm, Dm, red[warp], k, g);
-            }
+            const long off = 4L * r.n * it.member;
+            const long begin = (long)it.chunk * r.chunk_nodes;
+            const long end = min((long)r.n, begin + r.chunk_nodes);
+            for (long base = begin + warp * 4L; base < end; base += kStageWarps * 4L)
+                serve_group(r, stage, base, end, r.H + off, r.Ka + off, r.Kb + off, r.D + off, red[warp], k, g);
         }
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
             const int c = atomicAdd(done + it.slot, 1) + 1;
+            ((volatile int*)mdone)[it.slot] = c;          // monotonic mirror for the scheduler
             const unsigned long long d = atomicAdd(items_done, 1ull) + 1;
             if ((d & 63) == 0) ctl->progress = (long long)d;
             if (c == r.total) {
@@ -269,6 +268,7 @@ struct Request {
     std::vector<double> h0;              // host copy of the initial state
     std::vector<double> result;
     int next_step = 0;                   // steps appended so far
+    long long appended = 0;              // items appended so far
     enum State { PENDING, RUNNING, DRAINING, DONE, CANCELLED, FAILED } state = PENDING;
     double t_submit = 0, t_admit = 0, t_done = 0;
     bool cancel_req = false;
@@ -289,6 +289,7 @@ struct Server {
     Item* ring = nullptr;                         // mapped
     long long ring_cap = 0, tail = 0;
     int* flags = nullptr;                         // mapped [max_slots]
+    int* mdone = nullptr;                         // mapped [max_slots]: items done per slot
     unsigned long long* head = nullptr;           // device
     unsigned long long* items_done = nullptr;     // device
     int* exiting = nullptr;                       // device
@@ -344,37 +345,47 @@ struct Server {
         const size_t one = (size_t)n * 4 * sizeof(double) * members;
         return ((one + 255) / 256 * 256) * 4;      // H, Ka, Kb, D
     }
-    static int chunk_nodes(int n, int members) {
-        int c = std::max(1024, 65536 / std::max(members, 1));
+    // nodes per work item: about 2048 (tens of microseconds of FP64 stage work),
+    // fewer on small grids so that they still split into several items
+    static int chunk_nodes(int n) {
+        int c = std::min(2048, std::max(256, n / 8));
         c = (c + 31) / 32 * 32;
         return std::min(c, n);
     }
+    static constexpr int kLookaheadSteps = 2;
 
     bool kernel_running() { return cudaStreamQuery(kstream) == cudaErrorNotReady; }
 
     void launch_kernel() {
         cudaMemsetAsync(exiting, 0, sizeof(int), kstream);
         serve_kernel<<<sms * std::max(per_sm, 1), kThreads, 0, kstream>>>(ctl, ring, ring_cap, head, reqs_d, done_d,
-                                                                         flags, items_done, exiting);
+                                                                         flags, mdone, items_done, exiting);
         ++launches;
         count_launch();
     }
 
-    // append one RK4 step (4 stage indices x chunks) of request r
+    int items_per_step(const Request& r) const {
+        const int n = grids[r.grid].n, cn = chunk_nodes(n);
+        return 4 * ((n + cn - 1) / cn) * r.members;
+    }
+
+    // append one RK4 step (4 stage indices x chunks x members) of request r
     void append_step(Request& r) {
         const Grid& G = grids[r.grid];
-        const int cn = chunk_nodes(G.n, r.members);
+        const int cn = chunk_nodes(G.n);
         const int nch = (G.n + cn - 1) / cn;
         for (int st = 0; st < 4; ++st) {
             const int q = r.next_step * 4 + st;
-            for (int c = 0; c < nch; ++c) {
-                Item& it = ring[tail % ring_cap];
-                it.slot = r.slot;
-                it.q = q;
-                it.begin = c * cn;
-                it.end = std::min(G.n, (c + 1) * cn);
-                ++tail;
-            }
+            for (int c = 0; c < nch; ++c)
+                for (int mb = 0; mb < r.members; ++mb) {
+                    Item& it = ring[tail % ring_cap];
+                    it.slot = r.slot;
+                    it.q = q;
+                    it.chunk = c;
+                    it.member = mb;
+                    ++tail;
+                    ++r.appended;
+                }
         }
         ++r.next_step;
     }
@@ -393,9 +404,9 @@ struct Server {
         d.PT = reinterpret_cast<const double*>(G.PT);
         d.n = G.n;
         d.members = r.members;
-        const int cn = chunk_nodes(G.n, r.members);
-        d.nchunks = (G.n + cn - 1) / cn;
-        d.total = d.nchunks * 4 * r.nsteps;
+        d.chunk_nodes = chunk_nodes(G.n);
+        d.per_stage = ((G.n + d.chunk_nodes - 1) / d.chunk_nodes) * r.members;
+        d.total = d.per_stage * 4 * r.nsteps;
         d.id = r.id;
         d.cancelled = 0;
         d.gh0 = G.gh0;
@@ -406,6 +417,7 @@ struct Server {
         d.D = reinterpret_cast<double*>(arena + off + 3 * one);
         int zero = 0;
         flags[r.slot] = -1;
+        mdone[r.slot] = 0;
         cudaMemcpyAsync(d.H, r.h0.data(), r.h0.size() * sizeof(double), cudaMemcpyHostToDevice, cstream);
         cudaMemcpyAsync(reqs_d + r.slot, &d, sizeof(d), cudaMemcpyHostToDevice, cstream);
         cudaMemcpyAsync(done_d + r.slot, &zero, sizeof(int), cudaMemcpyHostToDevice, cstream);
@@ -457,18 +469,22 @@ struct Server {
             if (st == 1) it = pending.erase(it);
             else ++it;
         }
-        // work: one step per active request per round while the queue is short
+        // work: round-robin, one RK4 step per request per round, at most
+        // kLookaheadSteps steps queued or in flight per request (so that CTAs
+        // waiting on a request's previous stage stay few)
         const long long done_items = ctl->progress;
         bool appended = false;
-        for (int round = 0; round < 4 && tail - done_items < (long long)sms * 64; ++round) {
+        for (int round = 0; round < kLookaheadSteps; ++round) {
             bool any = false;
             for (int id : active) {
                 Request& r = requests[id];
-                if (r.next_step < r.nsteps) {
-                    if (tail + 4LL * 4096 > ring_cap + done_items) break;   // ring full
-                    append_step(r);
-                    any = appended = true;
-                }
+                if (r.next_step >= r.nsteps) continue;
+                const int ips = items_per_step(r);
+                const long long outstanding = r.appended - ((volatile int*)mdone)[r.slot];
+                if (outstanding >= (long long)kLookaheadSteps * ips) continue;
+                if (tail + ips > ring_cap + done_items - 1024) break;       // ring full
+                append_step(r);
+                any = appended = true;
             }
             if (!any) break;
         }
@@ -533,6 +549,8 @@ int swe_srv_start(double budget_bytes, int max_requests) {
     if ((e = cudaHostAlloc(&S->ctl, sizeof(Shared), cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc");
     if ((e = cudaHostAlloc(&S->ring, sizeof(Item) * S->ring_cap, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc ring");
     if ((e = cudaHostAlloc(&S->flags, sizeof(int) * max_requests, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc flags");
+    if ((e = cudaHostAlloc(&S->mdone, sizeof(int) * max_requests, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc mdone");
+    for (int i = 0; i < max_requests; ++i) S->mdone[i] = 0;
     memset((void*)S->ctl, 0, sizeof(Shared));
     for (int i = 0; i < max_requests; ++i) S->flags[i] = -1;
     if ((e = cudaMalloc(&S->head, sizeof(unsigned long long))) != cudaSuccess) return fail("cudaMalloc head");
@@ -726,6 +744,7 @@ int swe_srv_stop(void) {
     cudaFreeHost((void*)S->ctl);
     cudaFreeHost(S->ring);
     cudaFreeHost(S->flags);
+    cudaFreeHost(S->mdone);
     cudaStreamDestroy(S->kstream);
     cudaStreamDestroy(S->cstream);
     const bool err = !S->fatal.empty();
