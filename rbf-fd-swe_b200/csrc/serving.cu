@@ -3,11 +3,12 @@
 // Forecast requests (a grid, 1-32 members, a number of RK4 steps, initial
 // states) arrive while others run.  A host scheduler thread admits them as
 // device memory frees up (first fit in one arena of the configured HBM budget),
-// uploads their states on a copy stream, and appends their work to a queue in
-// mapped pinned memory: round-robin over the active requests, one RK4 step
-// (4 stages x node chunks) per request per round, so that new requests join
-// the mix at once.  One persistent kernel -- one CTA per SM slot -- claims work
-// items from that queue, waits (bounded) until the request's previous stage
+// uploads their states on a copy stream, and appends their work to a queue:
+// round-robin over the active requests, one RK4 step (4 stages x node chunks x
+// members) per request per round, at most two steps ahead of a request's
+// progress, so that new requests join the mix at once.  One persistent kernel -- one CTA per SM slot -- claims work
+// items from that queue (kept in device memory and published by copies on the
+// copy stream, so nothing polls across PCIe), waits (bounded) until the request's previous stage
 // has completed everywhere, runs the plain form's fused FP64 stage math on the
 // chunk for every member, and publishes completion counters; the last item of
 // a request raises its completion flag in host memory.  The per-node math is
@@ -62,11 +63,15 @@ struct alignas(16) ReqDesc {   // device table entry of an admitted request
     double* D;
 };
 
-struct Shared {          // host-mapped control block
-    volatile long long tail;       // items published by the host
-    volatile int stop;             // host asks the kernel to exit
+struct Shared {          // host-mapped block the kernel writes (posted stores only)
     volatile int error;            // kernel-side error code
     volatile long long progress;   // items completed (approximate mirror)
+};
+
+struct DevCtl {          // device-resident control words the host sets by async copies
+    long long tail;      // items published by the host
+    int stop;            // host asks the kernel to exit
+    int pad;
 };
 
 constexpr int kThreads = kStageThreads;         // 8 warps x 4 nodes
@@ -162,10 +167,14 @@ __device__ void serve_group(const ReqDesc& r, int stage, long base, long end, do
 // raises *exiting; from then on no CTA claims work (items already claimed are
 // finished), so every launch runs at full width and the host relaunches, with
 // *exiting cleared, once the kernel has ended and work is queued again.
+// The queue, its tail and the stop word live in device memory (the host
+// publishes them with copies on its copy stream), so polling CTAs never read
+// host memory across PCIe; the kernel only posts stores to host memory
+// (completion flags and counters).
 __global__ void __launch_bounds__(kThreads, 2)
-serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, unsigned long long* head,
-             const ReqDesc* __restrict__ reqs, int* done, int* flags, int* mdone, unsigned long long* items_done,
-             int* exiting) {
+serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, long long ring_cap,
+             unsigned long long* head, const ReqDesc* __restrict__ reqs, int* done, int* flags, int* mdone,
+             unsigned long long* items_done, int* exiting, int* kerr) {
     __shared__ double red[kStageWarps][4][16];
     __shared__ long long s_pos;
     __shared__ Item s_item;
@@ -177,9 +186,9 @@ serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, uns
         if (threadIdx.x == 0) {
             long long got = -1;
             while (true) {
-                if (ctl->stop || ctl->error || *(volatile int*)exiting) break;
+                if (*(volatile const int*)&dctl->stop || *(volatile int*)kerr || *(volatile int*)exiting) break;
                 const unsigned long long h = *(volatile unsigned long long*)head;
-                const long long t = ctl->tail;
+                const long long t = *(volatile const long long*)&dctl->tail;
                 if ((long long)h < t) {
                     if (atomicCAS(head, h, h + 1) == h) { got = (long long)h; break; }
                     continue;
@@ -192,11 +201,11 @@ serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, uns
             }
             s_pos = got;
             if (got >= 0) {
-                const volatile Item* vi = ring + got % ring_cap;
-                s_item.slot = vi->slot;
-                s_item.q = vi->q;
-                s_item.chunk = vi->chunk;
-                s_item.member = vi->member;
+                const int4 v = __ldcg(reinterpret_cast<const int4*>(ring + got % ring_cap));
+                s_item.slot = v.x;
+                s_item.q = v.y;
+                s_item.chunk = v.z;
+                s_item.member = v.w;
             }
         }
         __syncthreads();
@@ -214,9 +223,10 @@ serve_kernel(Shared* ctl, const Item* __restrict__ ring, long long ring_cap, uns
             const int need = it.q * r.per_stage;
             const unsigned long long t0 = globaltimer();
             while (atomicAdd(done + it.slot, 0) < need) {
-                if (ctl->stop) { s_ok = 0; break; }
+                if (*(volatile const int*)&dctl->stop) { s_ok = 0; break; }
                 if (globaltimer() - t0 > kDepNs) {
                     s_ok = 0;
+                    atomicExch(kerr, 2);
                     ctl->error = 2;
                     break;
                 }
@@ -285,9 +295,13 @@ struct Server {
     size_t budget = 0, in_use = 0, peak = 0;
     char* arena = nullptr;
     std::map<size_t, size_t> free_blocks;         // offset -> size
-    Shared* ctl = nullptr;                        // mapped
-    Item* ring = nullptr;                         // mapped
-    long long ring_cap = 0, tail = 0;
+    Shared* ctl = nullptr;                        // mapped (kernel -> host)
+    DevCtl* dctl = nullptr;                       // device (host -> kernel by copies)
+    DevCtl* hctl = nullptr;                       // pinned staging of dctl
+    Item* ring = nullptr;                         // device queue
+    Item* ring_h = nullptr;                       // pinned staging of the queue
+    int* kerr = nullptr;                          // device error word
+    long long ring_cap = 0, tail = 0, published = 0;
     int* flags = nullptr;                         // mapped [max_slots]
     int* mdone = nullptr;                         // mapped [max_slots]: items done per slot
     unsigned long long* head = nullptr;           // device
@@ -358,8 +372,9 @@ struct Server {
 
     void launch_kernel() {
         cudaMemsetAsync(exiting, 0, sizeof(int), kstream);
-        serve_kernel<<<sms * std::max(per_sm, 1), kThreads, 0, kstream>>>(ctl, ring, ring_cap, head, reqs_d, done_d,
-                                                                         flags, mdone, items_done, exiting);
+        serve_kernel<<<sms * std::max(per_sm, 1), kThreads, 0, kstream>>>(ctl, dctl, ring, ring_cap, head, reqs_d,
+                                                                         done_d, flags, mdone, items_done, exiting,
+                                                                         kerr);
         ++launches;
         count_launch();
     }
@@ -378,7 +393,7 @@ struct Server {
             const int q = r.next_step * 4 + st;
             for (int c = 0; c < nch; ++c)
                 for (int mb = 0; mb < r.members; ++mb) {
-                    Item& it = ring[tail % ring_cap];
+                    Item& it = ring_h[tail % ring_cap];
                     it.slot = r.slot;
                     it.q = q;
                     it.chunk = c;
@@ -449,6 +464,21 @@ struct Server {
         ++completed;
     }
 
+    // copy the new queue entries, then the tail, to the device (copy stream)
+    void publish() {
+        long long from = published;
+        while (from < tail) {
+            const long long s0 = from % ring_cap;
+            const long long cnt = std::min(tail - from, ring_cap - s0);
+            cudaMemcpyAsync(ring + s0, ring_h + s0, cnt * sizeof(Item), cudaMemcpyHostToDevice, cstream);
+            from += cnt;
+        }
+        hctl->tail = tail;
+        cudaMemcpyAsync(&dctl->tail, &hctl->tail, sizeof(long long), cudaMemcpyHostToDevice, cstream);
+        cudaStreamSynchronize(cstream);
+        published = tail;
+    }
+
     // one scheduler pass (called with mu held)
     void pass() {
         // completions
@@ -488,11 +518,8 @@ struct Server {
             }
             if (!any) break;
         }
-        if (appended) {
-            std::atomic_thread_fence(std::memory_order_seq_cst);
-            ctl->tail = tail;
-        }
-        const bool work = ctl->tail > (long long)ctl->progress || !active.empty();
+        if (appended) publish();
+        const bool work = tail > (long long)ctl->progress || !active.empty();
         if (ctl->error) {
             fatal = ctl->error == 2 ? "serving kernel: a dependency wait ran out" : "serving kernel error";
             return;
@@ -547,7 +574,14 @@ int swe_srv_start(double budget_bytes, int max_requests) {
     S->free_blocks[0] = S->budget;
     S->ring_cap = 1LL << 22;
     if ((e = cudaHostAlloc(&S->ctl, sizeof(Shared), cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc");
-    if ((e = cudaHostAlloc(&S->ring, sizeof(Item) * S->ring_cap, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc ring");
+    if ((e = cudaMalloc(&S->ring, sizeof(Item) * S->ring_cap)) != cudaSuccess) return fail("cudaMalloc ring");
+    if ((e = cudaHostAlloc(&S->ring_h, sizeof(Item) * S->ring_cap, cudaHostAllocDefault)) != cudaSuccess) return fail("cudaHostAlloc ring");
+    if ((e = cudaHostAlloc(&S->hctl, sizeof(DevCtl), cudaHostAllocDefault)) != cudaSuccess) return fail("cudaHostAlloc ctl");
+    if ((e = cudaMalloc(&S->dctl, sizeof(DevCtl))) != cudaSuccess) return fail("cudaMalloc ctl");
+    if ((e = cudaMalloc(&S->kerr, sizeof(int))) != cudaSuccess) return fail("cudaMalloc err");
+    memset(S->hctl, 0, sizeof(DevCtl));
+    cudaMemset(S->dctl, 0, sizeof(DevCtl));
+    cudaMemset(S->kerr, 0, sizeof(int));
     if ((e = cudaHostAlloc(&S->flags, sizeof(int) * max_requests, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc flags");
     if ((e = cudaHostAlloc(&S->mdone, sizeof(int) * max_requests, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc mdone");
     for (int i = 0; i < max_requests; ++i) S->mdone[i] = 0;
@@ -727,7 +761,9 @@ int swe_srv_stop(void) {
     Server* S = g_srv;
     S->quit = true;
     if (S->worker.joinable()) S->worker.join();
-    S->ctl->stop = 1;
+    S->hctl->stop = 1;
+    cudaMemcpyAsync(&S->dctl->stop, &S->hctl->stop, sizeof(int), cudaMemcpyHostToDevice, S->cstream);
+    cudaStreamSynchronize(S->cstream);
     cudaStreamSynchronize(S->kstream);
     cudaStreamSynchronize(S->cstream);
     for (auto& G : S->grids) {
@@ -742,7 +778,11 @@ int swe_srv_stop(void) {
     cudaFree(S->done_d);
     cudaFree(S->exiting);
     cudaFreeHost((void*)S->ctl);
-    cudaFreeHost(S->ring);
+    cudaFree(S->ring);
+    cudaFreeHost(S->ring_h);
+    cudaFreeHost(S->hctl);
+    cudaFree(S->dctl);
+    cudaFree(S->kerr);
     cudaFreeHost(S->flags);
     cudaFreeHost(S->mdone);
     cudaStreamDestroy(S->kstream);
