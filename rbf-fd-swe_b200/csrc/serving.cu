@@ -222,7 +222,10 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
             s_ok = 1;
             const int need = it.q * r.per_stage;
             const unsigned long long t0 = globaltimer();
-            while (atomicAdd(done + it.slot, 0) < need) {
+            // plain loads (served by L2, no atomic serialisation against the
+            // increments on the critical path) with exponential backoff
+            unsigned ns = 64;
+            while (*(volatile const int*)(done + it.slot) < need) {
                 if (*(volatile const int*)&dctl->stop) { s_ok = 0; break; }
                 if (globaltimer() - t0 > kDepNs) {
                     s_ok = 0;
@@ -230,7 +233,8 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
                     ctl->error = 2;
                     break;
                 }
-                __nanosleep(500);
+                __nanosleep(ns);
+                ns = ns < 4096 ? 2 * ns : ns;
             }
             __threadfence();
         }
