@@ -255,6 +255,9 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
             ((volatile int*)mdone)[it.slot] = c;          // monotonic mirror for the scheduler
             const unsigned long long d = atomicAdd(items_done, 1ull) + 1;
             if ((d & 63) == 0) ctl->progress = (long long)d;
+            // push the mirrors out of the GPU's caches to host memory now:
+            // the scheduler paces its appends on them
+            __threadfence_system();
             if (c == r.total) {
                 __threadfence_system();
                 ((volatile int*)flags)[it.slot] = r.id;
