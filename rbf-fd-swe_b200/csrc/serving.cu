@@ -24,6 +24,8 @@
 #include <atomic>
 #include <chrono>
 
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -282,11 +284,14 @@ struct Grid {
 struct Request {
     int id, grid, members, nsteps, slot = -1;
     size_t offset = 0, bytes = 0;
-    std::vector<double> h0;              // host copy of the initial state
-    std::vector<double> result;
+    size_t state_bytes = 0;              // members * n * 4 doubles
+    std::vector<double> host;            // pageable copy of the states (when the pinned pool is full)
+    double* pinned = nullptr;            // states in the pinned pool (initial, later final)
+    size_t pin_off = 0;
+    cudaEvent_t ev = nullptr;            // completion of its current upload / download
     int next_step = 0;                   // steps appended so far
     long long appended = 0;              // items appended so far
-    enum State { PENDING, RUNNING, DRAINING, DONE, CANCELLED, FAILED } state = PENDING;
+    enum State { PENDING, UPLOADING, RUNNING, DRAINING, DONE, CANCELLED, FAILED } state = PENDING;
     double t_submit = 0, t_admit = 0, t_done = 0;
     bool cancel_req = false;
 };
@@ -302,6 +307,9 @@ struct Server {
     size_t budget = 0, in_use = 0, peak = 0;
     char* arena = nullptr;
     std::map<size_t, size_t> free_blocks;         // offset -> size
+    char* pin = nullptr;                          // pinned staging pool for state transfers
+    size_t pin_size = 0;
+    std::map<size_t, size_t> pin_free;
     Shared* ctl = nullptr;                        // mapped (kernel -> host)
     DevCtl* dctl = nullptr;                       // device (host -> kernel by copies)
     DevCtl* hctl = nullptr;                       // pinned staging of dctl
@@ -322,45 +330,72 @@ struct Server {
     std::deque<int> pending;
     std::vector<int> active;                      // slots order for round-robin
     int next_id = 0;
-    cudaStream_t kstream = nullptr, cstream = nullptr;
+    cudaStream_t kstream = nullptr, cstream = nullptr, pstream = nullptr;
     long long launches = 0, admitted = 0, completed = 0;
     std::thread worker;
     std::mutex mu;
     std::atomic<bool> quit{false};
     std::string fatal;
+    bool trace = getenv("SWE_SRV_TRACE") != nullptr;   // scheduler trace on stderr
+    double t0 = now_s(), last_trace = 0.0;
 
-    // first-fit allocation in the arena
-    bool alloc(size_t bytes, size_t& off) {
-        for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
+    // first-fit allocation in a free list (offset -> size)
+    static bool fl_alloc(std::map<size_t, size_t>& fl, size_t bytes, size_t& off) {
+        for (auto it = fl.begin(); it != fl.end(); ++it) {
             if (it->second >= bytes) {
                 off = it->first;
                 const size_t rest = it->second - bytes;
                 const size_t noff = it->first + bytes;
-                free_blocks.erase(it);
-                if (rest) free_blocks[noff] = rest;
-                in_use += bytes;
-                peak = std::max(peak, in_use);
+                fl.erase(it);
+                if (rest) fl[noff] = rest;
                 return true;
             }
         }
         return false;
     }
-    void release(size_t off, size_t bytes) {
-        in_use -= bytes;
-        auto it = free_blocks.emplace(off, bytes).first;
+    static void fl_release(std::map<size_t, size_t>& fl, size_t off, size_t bytes) {
+        auto it = fl.emplace(off, bytes).first;
         auto nx = std::next(it);
-        if (nx != free_blocks.end() && it->first + it->second == nx->first) {
+        if (nx != fl.end() && it->first + it->second == nx->first) {
             it->second += nx->second;
-            free_blocks.erase(nx);
+            fl.erase(nx);
         }
-        if (it != free_blocks.begin()) {
+        if (it != fl.begin()) {
             auto pv = std::prev(it);
             if (pv->first + pv->second == it->first) {
                 pv->second += it->second;
-                free_blocks.erase(it);
+                fl.erase(it);
             }
         }
     }
+    bool alloc(size_t bytes, size_t& off) {
+        if (!fl_alloc(free_blocks, bytes, off)) return false;
+        in_use += bytes;
+        peak = std::max(peak, in_use);
+        return true;
+    }
+    void release(size_t off, size_t bytes) {
+        in_use -= bytes;
+        fl_release(free_blocks, off, bytes);
+    }
+    // pinned staging of one request's states (falls back to pageable memory)
+    void stage_host(Request& r, const double* src) {
+        const size_t b = (r.state_bytes + 255) / 256 * 256;
+        if (pin && fl_alloc(pin_free, b, r.pin_off)) {
+            r.pinned = reinterpret_cast<double*>(pin + r.pin_off);
+            if (src) memcpy(r.pinned, src, r.state_bytes);
+        } else {
+            r.pinned = nullptr;
+            if (src) r.host.assign(src, src + r.state_bytes / sizeof(double));
+            else r.host.resize(r.state_bytes / sizeof(double));
+        }
+    }
+    void unstage_host(Request& r) {
+        if (r.pinned) fl_release(pin_free, r.pin_off, (r.state_bytes + 255) / 256 * 256);
+        r.pinned = nullptr;
+        std::vector<double>().swap(r.host);
+    }
+    const double* host_states(const Request& r) const { return r.pinned ? r.pinned : r.host.data(); }
 
     static size_t state_bytes(int n, int members) {
         const size_t one = (size_t)n * 4 * sizeof(double) * members;
@@ -440,34 +475,36 @@ struct Server {
         int zero = 0;
         flags[r.slot] = -1;
         mdone[r.slot] = 0;
-        cudaMemcpyAsync(d.H, r.h0.data(), r.h0.size() * sizeof(double), cudaMemcpyHostToDevice, cstream);
+        // descriptor and counter first, then the states; work is queued once
+        // the upload event has completed (pass()), so the GPU keeps running
+        // other requests meanwhile
         cudaMemcpyAsync(reqs_d + r.slot, &d, sizeof(d), cudaMemcpyHostToDevice, cstream);
         cudaMemcpyAsync(done_d + r.slot, &zero, sizeof(int), cudaMemcpyHostToDevice, cstream);
-        if (cudaStreamSynchronize(cstream) != cudaSuccess) {
+        cudaMemcpyAsync(d.H, host_states(r), r.state_bytes, cudaMemcpyHostToDevice, cstream);
+        if (cudaEventRecord(r.ev, cstream) != cudaSuccess) {
             fatal = "request upload failed";
             return -1;
         }
-        std::vector<double>().swap(r.h0);
-        r.state = Request::RUNNING;
-        r.t_admit = now_s();
+        r.state = Request::UPLOADING;
         active.push_back(r.id);
         ++admitted;
         return 1;
     }
 
-    void finish(Request& r, Request::State st) {
-        const Grid& G = grids[r.grid];
-        r.result.resize((size_t)r.members * G.n * 4);
-        if (st == Request::DONE) {
-            cudaMemcpyAsync(r.result.data(), arena + r.offset, r.result.size() * sizeof(double),
-                            cudaMemcpyDeviceToHost, cstream);
-            cudaStreamSynchronize(cstream);
-        }
+    // the kernel has finished the request: copy its final states back (async)
+    void drain(Request& r) {
+        cudaMemcpyAsync(const_cast<double*>(host_states(r)), arena + r.offset, r.state_bytes,
+                        cudaMemcpyDeviceToHost, cstream);
+        cudaEventRecord(r.ev, cstream);
+        r.state = Request::DRAINING;
+    }
+    void retire(Request& r, Request::State st) {
         release(r.offset, r.bytes);
         free_slots.push_back(r.slot);
         r.slot = -1;
         r.t_done = now_s();
         r.state = st;
+        if (st != Request::DONE) unstage_host(r);
         ++completed;
     }
 
@@ -477,26 +514,35 @@ struct Server {
         while (from < tail) {
             const long long s0 = from % ring_cap;
             const long long cnt = std::min(tail - from, ring_cap - s0);
-            cudaMemcpyAsync(ring + s0, ring_h + s0, cnt * sizeof(Item), cudaMemcpyHostToDevice, cstream);
+            cudaMemcpyAsync(ring + s0, ring_h + s0, cnt * sizeof(Item), cudaMemcpyHostToDevice, pstream);
             from += cnt;
         }
         hctl->tail = tail;
-        cudaMemcpyAsync(&dctl->tail, &hctl->tail, sizeof(long long), cudaMemcpyHostToDevice, cstream);
-        cudaStreamSynchronize(cstream);
+        cudaMemcpyAsync(&dctl->tail, &hctl->tail, sizeof(long long), cudaMemcpyHostToDevice, pstream);
+        cudaStreamSynchronize(pstream);
         published = tail;
     }
 
     // one scheduler pass (called with mu held)
     void pass() {
-        // completions
+        // uploads done -> running; kernel done -> draining; drained -> done
         for (size_t a = 0; a < active.size();) {
             Request& r = requests[active[a]];
-            if (r.slot >= 0 && ((volatile int*)flags)[r.slot] == r.id) {
-                finish(r, r.cancel_req ? Request::CANCELLED : Request::DONE);
-                active.erase(active.begin() + a);
-            } else {
-                ++a;
+            bool gone = false;
+            if (r.state == Request::UPLOADING && cudaEventQuery(r.ev) == cudaSuccess) {
+                r.state = Request::RUNNING;
+                r.t_admit = now_s();
             }
+            if (r.state == Request::RUNNING && ((volatile int*)flags)[r.slot] == r.id) {
+                if (r.cancel_req) { retire(r, Request::CANCELLED); gone = true; }
+                else drain(r);
+            }
+            if (r.state == Request::DRAINING && cudaEventQuery(r.ev) == cudaSuccess) {
+                retire(r, Request::DONE);
+                gone = true;
+            }
+            if (gone) active.erase(active.begin() + a);
+            else ++a;
         }
         // admissions: FIFO, later requests may overtake one that does not fit yet
         for (auto it = pending.begin(); it != pending.end();) {
@@ -515,7 +561,7 @@ struct Server {
             bool any = false;
             for (int id : active) {
                 Request& r = requests[id];
-                if (r.next_step >= r.nsteps) continue;
+                if (r.state != Request::RUNNING || r.next_step >= r.nsteps) continue;
                 const int ips = items_per_step(r);
                 const long long outstanding = r.appended - ((volatile int*)mdone)[r.slot];
                 if (outstanding >= (long long)kLookaheadSteps * ips) continue;
@@ -531,7 +577,23 @@ struct Server {
             fatal = ctl->error == 2 ? "serving kernel: a dependency wait ran out" : "serving kernel error";
             return;
         }
-        if (work && !kernel_running()) launch_kernel();
+        const bool was_running = kernel_running();
+        if (work && !was_running) launch_kernel();
+        if (trace) {
+            const double t = now_s() - t0;
+            if (t - last_trace > 0.002 || (work && !was_running)) {
+                last_trace = t;
+                fprintf(stderr, "[srv %.4f] tail %lld progress %lld active %zu pending %zu launches %lld%s",
+                        t, tail, (long long)ctl->progress, active.size(), pending.size(), launches,
+                        (work && !was_running) ? " RELAUNCH" : "");
+                for (int id : active) {
+                    const Request& r = requests[id];
+                    fprintf(stderr, " | r%d st%d step %d/%d app %lld done %d", id, (int)r.state, r.next_step, r.nsteps,
+                            r.appended, r.slot >= 0 ? ((volatile int*)mdone)[r.slot] : -1);
+                }
+                fprintf(stderr, "\n");
+            }
+        }
     }
 
     void loop() {
@@ -605,6 +667,11 @@ int swe_srv_start(double budget_bytes, int max_requests) {
     cudaMemset(S->done_d, 0, sizeof(int) * max_requests);
     cudaStreamCreateWithFlags(&S->kstream, cudaStreamNonBlocking);
     cudaStreamCreateWithFlags(&S->cstream, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&S->pstream, cudaStreamNonBlocking);
+    // pinned staging pool for state transfers: a quarter of the budget, 64 MiB .. 4 GiB
+    S->pin_size = std::min<size_t>(std::max<size_t>(S->budget / 4, (size_t)64 << 20), (size_t)4 << 30);
+    if (cudaHostAlloc(&S->pin, S->pin_size, cudaHostAllocDefault) == cudaSuccess) S->pin_free[0] = S->pin_size;
+    else { S->pin = nullptr; cudaGetLastError(); }
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail("setup");
     for (int i = max_requests - 1; i >= 0; --i) S->free_slots.push_back(i);
     S->running = true;
@@ -684,7 +751,13 @@ int swe_srv_submit(int grid, int members, int nsteps, const double* H0) {
         set_error("swe_srv_submit: request needs %zu bytes, more than the whole budget", r.bytes);
         return -SWE_ERR_NOMEM;
     }
-    r.h0.assign(H0, H0 + (size_t)members * G.n * 4);
+    r.state_bytes = (size_t)members * G.n * 4 * sizeof(double);
+    S.stage_host(r, H0);
+    if (cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming) != cudaSuccess) {
+        S.unstage_host(r);
+        set_error("swe_srv_submit: cudaEventCreate failed");
+        return -SWE_ERR_CUDA;
+    }
     r.t_submit = now_s();
     S.requests[r.id] = std::move(r);
     S.pending.push_back(S.requests.rbegin()->first);
@@ -718,7 +791,9 @@ int swe_srv_fetch(int id, double* H) {
     if (it == S.requests.end()) { set_error("swe_srv_fetch: unknown request %d", id); return SWE_ERR_ARG; }
     Request& r = it->second;
     if (r.state != Request::DONE) { set_error("swe_srv_fetch: request %d has not completed", id); return SWE_ERR_STATE; }
-    if (H) memcpy(H, r.result.data(), r.result.size() * sizeof(double));
+    if (H) memcpy(H, S.host_states(r), r.state_bytes);
+    S.unstage_host(r);
+    if (r.ev) cudaEventDestroy(r.ev);
     S.requests.erase(it);
     return SWE_OK;
 }
@@ -735,6 +810,7 @@ int swe_srv_cancel(int id) {
         S.pending.erase(std::remove(S.pending.begin(), S.pending.end(), id), S.pending.end());
         r.state = Request::CANCELLED;
         r.t_done = now_s();
+        S.unstage_host(r);
         return SWE_OK;
     }
     if (r.state == Request::RUNNING && r.slot >= 0) {
@@ -771,6 +847,7 @@ int swe_srv_stop(void) {
     S->hctl->stop = 1;
     cudaMemcpyAsync(&S->dctl->stop, &S->hctl->stop, sizeof(int), cudaMemcpyHostToDevice, S->cstream);
     cudaStreamSynchronize(S->cstream);
+    cudaStreamSynchronize(S->pstream);
     cudaStreamSynchronize(S->kstream);
     cudaStreamSynchronize(S->cstream);
     for (auto& G : S->grids) {
@@ -792,8 +869,12 @@ int swe_srv_stop(void) {
     cudaFree(S->kerr);
     cudaFreeHost(S->flags);
     cudaFreeHost(S->mdone);
+    for (auto& kv : S->requests)
+        if (kv.second.ev) cudaEventDestroy(kv.second.ev);
+    if (S->pin) cudaFreeHost(S->pin);
     cudaStreamDestroy(S->kstream);
     cudaStreamDestroy(S->cstream);
+    cudaStreamDestroy(S->pstream);
     const bool err = !S->fatal.empty();
     std::string msg = S->fatal;
     delete S;
