@@ -15,6 +15,7 @@
 
 #include "common.cuh"
 #include "stage_kernel.cuh"
+#include "stage_tma.cuh"
 
 namespace swe {
 
@@ -91,6 +92,56 @@ static void pack_points(const CallerLayout& cl, int n, const T* x, const T* y, c
     }
 }
 
+// Neighbour windows of the TMA kernel: for each 32-node tile, the patch rows
+// its stencils touch merged into at most kMaxRanges contiguous ranges (gaps
+// of up to G rows are copied too; G doubles until the ranges fit) and at most
+// kWinRows rows in total; idxl holds each slot's row inside that window.
+// Returns false when some tile cannot be covered (e.g. an unordered patch).
+static bool build_windows(int n, int nnbr, const std::vector<int>& ibuf, std::vector<uint16_t>& idxl,
+                          std::vector<int2>& ranges) {
+    const int ntiles = (n + kTmaTile - 1) / kTmaTile;
+    idxl.assign((size_t)n * kSlots, 0);
+    ranges.assign((size_t)ntiles * (1 + kMaxRanges), make_int2(0, 0));
+    std::vector<int> u;
+    std::vector<int2> rg;
+    for (int tile = 0; tile < ntiles; ++tile) {
+        u.clear();
+        const int n0 = tile * kTmaTile, n1 = std::min(n, n0 + kTmaTile);
+        for (int i = n0; i < n1; ++i)
+            for (int j = 0; j < nnbr; ++j) u.push_back(ibuf[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)]);
+        std::sort(u.begin(), u.end());
+        u.erase(std::unique(u.begin(), u.end()), u.end());
+        int total = 0;
+        for (int gap = 8;; gap *= 2) {
+            rg.clear();
+            for (int r : u) {
+                if (!rg.empty() && r - (rg.back().x + rg.back().y) <= gap) rg.back().y = r - rg.back().x + 1;
+                else rg.push_back(make_int2(r, 1));
+            }
+            if ((int)rg.size() <= kMaxRanges || gap > kWinRows) break;
+        }
+        for (auto& r : rg) total += r.y;
+        if ((int)rg.size() > kMaxRanges || total > kWinRows) return false;
+        int2* dst = &ranges[(size_t)tile * (1 + kMaxRanges)];
+        dst[0] = make_int2((int)rg.size(), total);
+        for (size_t r = 0; r < rg.size(); ++r) dst[1 + r] = rg[r];
+        // window position of every slot (padded slots keep position 0: zero weight)
+        for (int i = n0; i < n1; ++i)
+            for (int j = 0; j < nnbr; ++j) {
+                const int row = ibuf[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)];
+                int off = 0;
+                for (auto& r : rg) {
+                    if (row >= r.x && row < r.x + r.y) {
+                        idxl[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)] = (uint16_t)(off + row - r.x);
+                        break;
+                    }
+                    off += r.y;
+                }
+            }
+    }
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // Device helpers ---------------------------------------------------------------
 
@@ -150,6 +201,12 @@ struct Plain {
          *Kx = nullptr, *raw = nullptr;
     int* idx = nullptr;
     double* inv = nullptr;
+    uint16_t* idxl = nullptr;       // TMA kernel: window-local indices
+    int2* ranges = nullptr;         // TMA kernel: neighbour windows per tile
+    int* err = nullptr;             // TMA kernel: bounded-wait error word
+    bool tma_ok = false;            // every tile's window fits
+    int kernel_choice = 0;          // 0 = TMA kernel when possible, 1 = register-streaming kernel
+    int ntiles = 0, grid_tma = 0;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int grid = 0;
@@ -168,9 +225,16 @@ struct Plain {
         for (void* p : {W, PT, H, Ka, Kb, D, F, Kx, raw}) if (p) cudaFree(p);
         if (idx) cudaFree(idx);
         if (inv) cudaFree(inv);
+        if (idxl) cudaFree(idxl);
+        if (ranges) cudaFree(ranges);
+        if (err) cudaFree(err);
         W = PT = H = Ka = Kb = D = F = Kx = raw = nullptr;
         idx = nullptr;
         inv = nullptr;
+        idxl = nullptr;
+        ranges = nullptr;
+        err = nullptr;
+        tma_ok = false;
         for (auto e : ev) cudaEventDestroy(e);
         ev.clear();
         ev_used = 0;
@@ -220,9 +284,23 @@ struct Plain {
         return a;
     }
 
+    bool use_tma() const { return tma_ok && kernel_choice == 0; }
+
     template <typename T>
     void launch_t(int mode) {
         const StageArgs<T> a = args<T>(mode);
+        if (use_tma()) {
+            TmaArgs<T> ta{a, ntiles, idxl, ranges, err};
+            const int sm = TmaLayout<T>::kSmem;
+            switch (mode) {
+                case 0: stage_tma_kernel<T, kStage0><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
+                case 1: stage_tma_kernel<T, kStage1><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
+                case 2: stage_tma_kernel<T, kStage2><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
+                case 3: stage_tma_kernel<T, kStage3><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
+                default: stage_tma_kernel<T, kEvalOnly><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
+            }
+            return;
+        }
         switch (mode) {
             case 0: stage_kernel<T, kStage0><<<grid, kStageThreads, 0, stream>>>(a); break;
             case 1: stage_kernel<T, kStage1><<<grid, kStageThreads, 0, stream>>>(a); break;
@@ -283,6 +361,37 @@ static int upload_static(Plain& P, const void* x, const void* y, const void* z, 
     SWE_CUDA_TRY(cudaMemcpy(P.W, wbuf.data(), wbuf.size() * sizeof(T), cudaMemcpyHostToDevice));
     SWE_CUDA_TRY(cudaMemcpy(P.idx, ibuf.data(), ibuf.size() * sizeof(int), cudaMemcpyHostToDevice));
     SWE_CUDA_TRY(cudaMemcpy(P.PT, pbuf.data(), pbuf.size() * sizeof(T), cudaMemcpyHostToDevice));
+    std::vector<uint16_t> idxl;
+    std::vector<int2> ranges;
+    P.tma_ok = build_windows(P.n, P.nnbr, ibuf, idxl, ranges);
+    if (P.tma_ok) {
+        P.ntiles = (P.n + kTmaTile - 1) / kTmaTile;
+        SWE_CUDA_TRY(cudaMalloc(&P.idxl, idxl.size() * sizeof(uint16_t)));
+        SWE_CUDA_TRY(cudaMalloc(&P.ranges, ranges.size() * sizeof(int2)));
+        SWE_CUDA_TRY(cudaMalloc(&P.err, sizeof(int)));
+        SWE_CUDA_TRY(cudaMemset(P.err, 0, sizeof(int)));
+        SWE_CUDA_TRY(cudaMemcpy(P.idxl, idxl.data(), idxl.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+        SWE_CUDA_TRY(cudaMemcpy(P.ranges, ranges.data(), ranges.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        const int sm = TmaLayout<T>::kSmem;
+        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kEvalOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    }
+    return SWE_OK;
+}
+
+static int check_tma_err() {
+    Plain& P = g_plain;
+    if (!P.err) return SWE_OK;
+    int h = 0;
+    SWE_CUDA_TRY(cudaMemcpyAsync(&h, P.err, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    if (h) {
+        set_error("stage kernel: a bounded wait on the bulk-copy pipeline ran out (code %d)", h);
+        return SWE_ERR_TIMEOUT;
+    }
     return SWE_OK;
 }
 
@@ -386,6 +495,7 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
         SWE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel<float, kStage1>, kStageThreads, 0));
     const int want = ceil_div(P.n, 4 * kStageWarps);
     P.grid = std::max(1, std::min(want, sms * std::max(per_sm, 1)));
+    P.grid_tma = std::max(1, std::min(P.ntiles, sms));
     P.ready = true;
     if ((st = P.build_graph()) != SWE_OK) return st;
     return SWE_OK;
@@ -411,7 +521,7 @@ int swe_cuda_get_state(void* Hh) {
     SWE_TRY(permute_state(P.H, P.raw, 1));
     SWE_CUDA_TRY(cudaMemcpyAsync(Hh, P.raw, bytes, cudaMemcpyDeviceToHost, P.stream));
     SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
-    return SWE_OK;
+    return check_tma_err();
 }
 
 int swe_cuda_eval_rhs(const void* K, void* Fh) {
@@ -470,6 +580,25 @@ int swe_cuda_step(int nsteps) {
 int swe_cuda_sync(void) {
     SWE_TRY(require_ready());
     SWE_CUDA_TRY(cudaStreamSynchronize(g_plain.stream));
+    return check_tma_err();
+}
+
+int swe_cuda_select_kernel(int which) {
+    SWE_TRY(require_ready());
+    if (which != 0 && which != 1) { set_error("swe_cuda_select_kernel: 0 (bulk-copy pipeline) or 1"); return SWE_ERR_ARG; }
+    Plain& P = g_plain;
+    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    P.kernel_choice = which;
+    if (P.graph) cudaGraphExecDestroy(P.graph);
+    P.graph = nullptr;
+    return P.build_graph();
+}
+
+int swe_cuda_kernel_info(int* out) {
+    SWE_TRY(require_ready());
+    if (!out) { set_error("null out"); return SWE_ERR_ARG; }
+    out[0] = g_plain.use_tma() ? 0 : 1;
+    out[1] = g_plain.tma_ok ? 1 : 0;
     return SWE_OK;
 }
 

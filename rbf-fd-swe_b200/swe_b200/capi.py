@@ -59,6 +59,8 @@ def load() -> ctypes.CDLL:
     lib.swe_cuda_step.argtypes = [i]
     lib.swe_cuda_set_timing.argtypes = [i]
     lib.swe_cuda_stream.restype = vp
+    lib.swe_cuda_select_kernel.argtypes = [i]
+    lib.swe_cuda_kernel_info.argtypes = [vp]
     lib.swe_ens_init.argtypes = [i, i, i, d, d] + [vp] * 14
     for name in ("swe_ens_set_state", "swe_ens_get_state", "swe_ens_tune", "swe_ens_config",
                  "swe_ens_invariants", "swe_ens_last_timings"):
@@ -201,6 +203,15 @@ class Plain:
 
     def stream(self) -> int:
         return int(self.lib.swe_cuda_stream() or 0)
+
+    def select_kernel(self, which: int) -> None:
+        """0: bulk-copy pipelined stage kernel when the patch allows it, 1: register-streaming kernel."""
+        check("swe_cuda_select_kernel", self.lib.swe_cuda_select_kernel(int(which)))
+
+    def kernel_info(self) -> dict:
+        out = np.zeros(2, dtype=np.int32)
+        check("swe_cuda_kernel_info", self.lib.swe_cuda_kernel_info(_p(out)))
+        return {"in_use": "pipelined" if out[0] == 0 else "register", "pipelined_available": bool(out[1])}
 
     def invariants(self) -> np.ndarray:
         out = np.zeros(2)

@@ -170,3 +170,34 @@ def test_invariants_match_oracle(plain, grid_l4):
     got = plain.invariants()
     want = oracle.Port(m, "fp64").invariants(H)[0]
     assert np.allclose(got, want, rtol=1e-13)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_pipelined_and_register_kernels_agree_bitwise(plain, prec):
+    """The bulk-copy pipelined kernel (RCM-ordered patches) and the
+    register-streaming kernel do the same arithmetic in the same order."""
+    _, d = generated_input(6)
+    m, _ = layout.prepare(swe_input.to_model(d), use_rcm=True, simd_length=32)
+    plain.init_model(m, prec)
+    assert plain.kernel_info() == {"in_use": "pipelined", "pipelined_available": True}
+    dt = np.float64 if prec == "fp64" else np.float32
+    K = _perturbed(m.H_init).astype(dt)
+    F0 = plain.eval_rhs(K)
+    plain.set_state(m.H_init.astype(dt))
+    plain.step(7)
+    H0 = plain.get_state()
+    plain.select_kernel(1)
+    assert plain.kernel_info()["in_use"] == "register"
+    F1 = plain.eval_rhs(K)
+    plain.set_state(m.H_init.astype(dt))
+    plain.step(7)
+    H1 = plain.get_state()
+    assert np.array_equal(F0, F1) and np.array_equal(H0, H1)
+    if prec == "fp64":
+        assert rel_err(F0, oracle.Port(m, "fp64").eval_rhs(K)).max() <= 1e-12
+
+
+def test_unordered_patch_uses_register_kernel(plain, grid_l4):
+    _, d = grid_l4
+    plain.init_model(swe_input.to_model(d), "fp64")        # natural (unordered) node order
+    assert plain.kernel_info()["pipelined_available"] is False
