@@ -235,6 +235,7 @@ struct Plain {
         ranges = nullptr;
         err = nullptr;
         tma_ok = false;
+        kernel_choice = 0;
         for (auto e : ev) cudaEventDestroy(e);
         ev.clear();
         ev_used = 0;
