@@ -25,7 +25,7 @@
 namespace swe {
 
 constexpr int kTmaTile = 32;           // nodes per tile
-constexpr int kMaxRanges = 40;         // contiguous row ranges per neighbour window
+constexpr int kMaxRanges = 40;         // contiguous row ranges per neighbour window (<= 64)
 constexpr int kWinRows = 512;          // max rows per neighbour window
 constexpr int kTmaConsumerWarps = 8;
 constexpr int kTmaThreads = 32 * (kTmaConsumerWarps + 1);
@@ -93,47 +93,67 @@ __global__ void __launch_bounds__(kTmaThreads, 1) stage_tma_kernel(const TmaArgs
     const bool need_hd = MODE == kStage1 || MODE == kStage2 || MODE == kStage3;
 
     if (warp == kTmaConsumerWarps) {
-        // ---------------- producer ----------------
-        if (lane == 0) {
-            int it = 0, issued = 0;
-            for (int tile = blockIdx.x; tile < ta.ntiles; tile += gridDim.x, ++it) {
-                const int s = it % Lay::kStages;
-                if (it >= Lay::kStages &&
-                    !tc::mbar_wait_bounded(&empty[s], ((it / Lay::kStages) - 1) & 1, kTmaWaitTries)) {
-                    atomicExch(ta.err, 1);
-                    s_abort = 1;
-                    break;
-                }
-                if (*(volatile int*)&s_abort) break;
-                unsigned char* slot = smem + s * Lay::kSlotBytes;
-                const long n0 = (long)tile * kTmaTile;
-                const int nn = (int)min((long)kTmaTile, (long)a.n - n0);
-                const int2 hdr = __ldg(ta.ranges + (long)tile * (1 + kMaxRanges));
-                uint32_t tx = nn * (kSlots * 4 * sizeof(T) + kSlots * 2 + kPointStride * sizeof(T) + Lay::kRow) +
-                              (need_hd ? 2 * nn * Lay::kRow : 0) + hdr.y * Lay::kRow;
-                tma::arrive_expect_tx(&full[s], tx);
-                tma::bulk_g2s(slot + Lay::oW, a.W + n0 * kSlotChunks * Quad<T>::kUnits * 8,
-                              nn * kSlots * 4 * sizeof(T), &full[s]);
-                tma::bulk_g2s(slot + Lay::oIdx, ta.idxl + n0 * kSlots, nn * kSlots * 2, &full[s]);
-                tma::bulk_g2s(slot + Lay::oPt, a.PT + n0 * kPointStride, nn * kPointStride * sizeof(T), &full[s]);
-                tma::bulk_g2s(slot + Lay::oOwn, a.Kin + 4L * (n0 + a.pid0), nn * Lay::kRow, &full[s]);
-                if (need_hd) {
-                    tma::bulk_g2s(slot + Lay::oH, a.H + 4L * n0, nn * Lay::kRow, &full[s]);
-                    tma::bulk_g2s(slot + Lay::oD, a.D + 4L * n0, nn * Lay::kRow, &full[s]);
-                }
-                int off = 0;
-                for (int r = 0; r < hdr.x; ++r) {
-                    const int2 rg = __ldg(ta.ranges + (long)tile * (1 + kMaxRanges) + 1 + r);
-                    tma::bulk_g2s(slot + Lay::oWin + off * Lay::kRow, a.Kin + 4L * rg.x, rg.y * Lay::kRow,
-                                  &full[s]);
-                    off += rg.y;
-                }
-                ++issued;
+        // ---------------- producer (whole warp issues) ----------------
+        // The tile's range list is loaded by all lanes at once, window offsets
+        // come from a warp prefix sum, lane 0 posts the expected bytes and
+        // every lane issues its share of the bulk copies.  complete_tx may
+        // precede expect_tx inside a phase: the phase cannot close before
+        // lane 0's single arrive.
+        int it = 0, issued = 0;
+        for (int tile = blockIdx.x; tile < ta.ntiles; tile += gridDim.x, ++it) {
+            const int s = it % Lay::kStages;
+            int wait_ok = 1;
+            if (lane == 0 && it >= Lay::kStages)
+                wait_ok = tc::mbar_wait_bounded(&empty[s], ((it / Lay::kStages) - 1) & 1, kTmaWaitTries);
+            wait_ok = __shfl_sync(0xffffffffu, wait_ok, 0);
+            if (!wait_ok || *(volatile int*)&s_abort) {
+                if (lane == 0) { atomicExch(ta.err, 1); s_abort = 1; }
+                break;
             }
-            // drain: every issued slot must have landed before the CTA exits
+            unsigned char* slot = smem + s * Lay::kSlotBytes;
+            const long n0 = (long)tile * kTmaTile;
+            const int nn = (int)min((long)kTmaTile, (long)a.n - n0);
+            const int2* tab = ta.ranges + (long)tile * (1 + kMaxRanges);
+            const int2 hdr = __ldg(tab);
+            // ranges r = lane and r = lane + 32 (kMaxRanges <= 64)
+            int2 r0 = make_int2(0, 0), r1 = make_int2(0, 0);
+            if (lane < hdr.x) r0 = __ldg(tab + 1 + lane);
+            if (lane + 32 < hdr.x) r1 = __ldg(tab + 1 + lane + 32);
+            int p0 = r0.y, p1 = r1.y;                       // inclusive prefix sums of the lengths
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t0 = __shfl_up_sync(0xffffffffu, p0, o);
+                const int t1 = __shfl_up_sync(0xffffffffu, p1, o);
+                if (lane >= o) { p0 += t0; p1 += t1; }
+            }
+            const int first_total = __shfl_sync(0xffffffffu, p0, 31);
+            const int off0 = p0 - r0.y, off1 = first_total + p1 - r1.y;
+            if (lane == 0) {
+                const uint32_t tx = nn * (kSlots * 4 * sizeof(T) + kSlots * 2 + kPointStride * sizeof(T) + Lay::kRow) +
+                                    (need_hd ? 2 * nn * Lay::kRow : 0) + hdr.y * Lay::kRow;
+                tma::arrive_expect_tx(&full[s], tx);
+            }
+            switch (lane) {
+                case 0: tma::bulk_g2s(slot + Lay::oW, a.W + n0 * kSlotChunks * Quad<T>::kUnits * 8,
+                                      nn * kSlots * 4 * sizeof(T), &full[s]); break;
+                case 1: tma::bulk_g2s(slot + Lay::oIdx, ta.idxl + n0 * kSlots, nn * kSlots * 2, &full[s]); break;
+                case 2: tma::bulk_g2s(slot + Lay::oPt, a.PT + n0 * kPointStride, nn * kPointStride * sizeof(T),
+                                      &full[s]); break;
+                case 3: tma::bulk_g2s(slot + Lay::oOwn, a.Kin + 4L * (n0 + a.pid0), nn * Lay::kRow, &full[s]); break;
+                case 4: if (need_hd) tma::bulk_g2s(slot + Lay::oH, a.H + 4L * n0, nn * Lay::kRow, &full[s]); break;
+                case 5: if (need_hd) tma::bulk_g2s(slot + Lay::oD, a.D + 4L * n0, nn * Lay::kRow, &full[s]); break;
+                default: break;
+            }
+            if (lane < hdr.x)
+                tma::bulk_g2s(slot + Lay::oWin + off0 * Lay::kRow, a.Kin + 4L * r0.x, r0.y * Lay::kRow, &full[s]);
+            if (lane + 32 < hdr.x)
+                tma::bulk_g2s(slot + Lay::oWin + off1 * Lay::kRow, a.Kin + 4L * r1.x, r1.y * Lay::kRow, &full[s]);
+            ++issued;
+        }
+        // drain: every issued slot must have landed before the CTA exits
+        if (lane == 0)
             for (int j = max(0, issued - Lay::kStages); j < issued; ++j)
                 tc::mbar_wait_bounded(&full[j % Lay::kStages], (j / Lay::kStages) & 1, kTmaWaitTries);
-        }
         return;
     }
 
