@@ -96,11 +96,11 @@ int swe_cuda_step(int nsteps);
 /* Waits for all work of the library's stream. */
 int swe_cuda_sync(void);
 
-/* Kernel choice: 0 (default) = the bulk-copy pipelined stage kernel when every
- * 32-node tile's neighbour rows form at most 40 contiguous ranges of <= 512
- * rows (true for RCM-ordered patches), else the register-streaming kernel;
- * 1 = always the register-streaming kernel.  info[2] = {kernel in use (0/1),
- * pipelined kernel available (0/1)}. */
+/* Kernel choice: 0 (default) = the bulk-copy pipelined stage kernel (a
+ * producer warp streams each 64-node tile's weights, indices, pointwise data
+ * and state rows into shared memory with cp.async.bulk); 1 = the
+ * register-streaming kernel.  Both do the same arithmetic in the same order.
+ * info[2] = {kernel in use (0/1), pipelined kernel available (0/1)}. */
 int swe_cuda_select_kernel(int which);
 int swe_cuda_kernel_info(int* info);
 

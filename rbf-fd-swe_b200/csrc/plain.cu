@@ -92,56 +92,6 @@ static void pack_points(const CallerLayout& cl, int n, const T* x, const T* y, c
     }
 }
 
-// Neighbour windows of the TMA kernel: for each 32-node tile, the patch rows
-// its stencils touch merged into at most kMaxRanges contiguous ranges (gaps
-// of up to G rows are copied too; G doubles until the ranges fit) and at most
-// kWinRows rows in total; idxl holds each slot's row inside that window.
-// Returns false when some tile cannot be covered (e.g. an unordered patch).
-static bool build_windows(int n, int nnbr, const std::vector<int>& ibuf, std::vector<uint16_t>& idxl,
-                          std::vector<int2>& ranges) {
-    const int ntiles = (n + kTmaTile - 1) / kTmaTile;
-    idxl.assign((size_t)n * kSlots, 0);
-    ranges.assign((size_t)ntiles * (1 + kMaxRanges), make_int2(0, 0));
-    std::vector<int> u;
-    std::vector<int2> rg;
-    for (int tile = 0; tile < ntiles; ++tile) {
-        u.clear();
-        const int n0 = tile * kTmaTile, n1 = std::min(n, n0 + kTmaTile);
-        for (int i = n0; i < n1; ++i)
-            for (int j = 0; j < nnbr; ++j) u.push_back(ibuf[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)]);
-        std::sort(u.begin(), u.end());
-        u.erase(std::unique(u.begin(), u.end()), u.end());
-        int total = 0;
-        for (int gap = 8;; gap *= 2) {
-            rg.clear();
-            for (int r : u) {
-                if (!rg.empty() && r - (rg.back().x + rg.back().y) <= gap) rg.back().y = r - rg.back().x + 1;
-                else rg.push_back(make_int2(r, 1));
-            }
-            if ((int)rg.size() <= kMaxRanges || gap > kWinRows) break;
-        }
-        for (auto& r : rg) total += r.y;
-        if ((int)rg.size() > kMaxRanges || total > kWinRows) return false;
-        int2* dst = &ranges[(size_t)tile * (1 + kMaxRanges)];
-        dst[0] = make_int2((int)rg.size(), total);
-        for (size_t r = 0; r < rg.size(); ++r) dst[1 + r] = rg[r];
-        // window position of every slot (padded slots keep position 0: zero weight)
-        for (int i = n0; i < n1; ++i)
-            for (int j = 0; j < nnbr; ++j) {
-                const int row = ibuf[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)];
-                int off = 0;
-                for (auto& r : rg) {
-                    if (row >= r.x && row < r.x + r.y) {
-                        idxl[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)] = (uint16_t)(off + row - r.x);
-                        break;
-                    }
-                    off += r.y;
-                }
-            }
-    }
-    return true;
-}
-
 // ---------------------------------------------------------------------------
 // Device helpers ---------------------------------------------------------------
 
@@ -201,11 +151,9 @@ struct Plain {
          *Kx = nullptr, *raw = nullptr;
     int* idx = nullptr;
     double* inv = nullptr;
-    uint16_t* idxl = nullptr;       // TMA kernel: window-local indices
-    int2* ranges = nullptr;         // TMA kernel: neighbour windows per tile
-    int* err = nullptr;             // TMA kernel: bounded-wait error word
-    bool tma_ok = false;            // every tile's window fits
-    int kernel_choice = 0;          // 0 = TMA kernel when possible, 1 = register-streaming kernel
+    int* err = nullptr;             // pipelined kernel: bounded-wait error word
+    bool tma_ok = false;            // pipelined kernel set up
+    int kernel_choice = 0;          // 0 = bulk-copy pipelined kernel, 1 = register-streaming kernel
     int ntiles = 0, grid_tma = 0;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -225,14 +173,10 @@ struct Plain {
         for (void* p : {W, PT, H, Ka, Kb, D, F, Kx, raw}) if (p) cudaFree(p);
         if (idx) cudaFree(idx);
         if (inv) cudaFree(inv);
-        if (idxl) cudaFree(idxl);
-        if (ranges) cudaFree(ranges);
         if (err) cudaFree(err);
         W = PT = H = Ka = Kb = D = F = Kx = raw = nullptr;
         idx = nullptr;
         inv = nullptr;
-        idxl = nullptr;
-        ranges = nullptr;
         err = nullptr;
         tma_ok = false;
         kernel_choice = 0;
@@ -291,7 +235,7 @@ struct Plain {
     void launch_t(int mode) {
         const StageArgs<T> a = args<T>(mode);
         if (use_tma()) {
-            TmaArgs<T> ta{a, ntiles, idxl, ranges, err};
+            TmaArgs<T> ta{a, ntiles, err};
             const int sm = TmaLayout<T>::kSmem;
             switch (mode) {
                 case 0: stage_tma_kernel<T, kStage0><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
@@ -362,17 +306,11 @@ static int upload_static(Plain& P, const void* x, const void* y, const void* z, 
     SWE_CUDA_TRY(cudaMemcpy(P.W, wbuf.data(), wbuf.size() * sizeof(T), cudaMemcpyHostToDevice));
     SWE_CUDA_TRY(cudaMemcpy(P.idx, ibuf.data(), ibuf.size() * sizeof(int), cudaMemcpyHostToDevice));
     SWE_CUDA_TRY(cudaMemcpy(P.PT, pbuf.data(), pbuf.size() * sizeof(T), cudaMemcpyHostToDevice));
-    std::vector<uint16_t> idxl;
-    std::vector<int2> ranges;
-    P.tma_ok = build_windows(P.n, P.nnbr, ibuf, idxl, ranges);
-    if (P.tma_ok) {
+    P.tma_ok = true;
+    {
         P.ntiles = (P.n + kTmaTile - 1) / kTmaTile;
-        SWE_CUDA_TRY(cudaMalloc(&P.idxl, idxl.size() * sizeof(uint16_t)));
-        SWE_CUDA_TRY(cudaMalloc(&P.ranges, ranges.size() * sizeof(int2)));
         SWE_CUDA_TRY(cudaMalloc(&P.err, sizeof(int)));
         SWE_CUDA_TRY(cudaMemset(P.err, 0, sizeof(int)));
-        SWE_CUDA_TRY(cudaMemcpy(P.idxl, idxl.data(), idxl.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
-        SWE_CUDA_TRY(cudaMemcpy(P.ranges, ranges.data(), ranges.size() * sizeof(int2), cudaMemcpyHostToDevice));
         const int sm = TmaLayout<T>::kSmem;
         SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
         SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));

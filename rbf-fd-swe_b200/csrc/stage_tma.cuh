@@ -1,22 +1,19 @@
-// Fused RK4 stage kernel, TMA-pipelined (plain form, FP64 / FP32).
+// Fused RK4 stage kernel, bulk-copy pipelined (plain form, FP64 / FP32).
 //
-// Same math and lane split as stage_kernel.cuh, restructured for B200's bulk
-// copy engine.  A persistent CTA per SM runs one producer warp and 8 consumer
-// warps over tiles of 32 consecutive nodes.  For every tile the producer
-// issues cp.async.bulk copies (global -> shared, completing on an mbarrier)
-// into one of kStages ring slots:
-//   * the tile's packed weights (32 x 1 KB FP64) and pointwise records,
-//   * its 16-bit window-local stencil indices,
-//   * the tile's own state rows, and H / D rows for stages 1-3,
-//   * the neighbour window: the state rows the tile's stencils touch, as up to
-//     kMaxRanges contiguous row ranges of the RCM-ordered state, precomputed
-//     at init.  In RCM order a 32-node tile's ~290 neighbour rows fall into
-//     7-11 runs (at most 37 on the icosahedral grids up to N = 655362) once
-//     gaps of up to 8 rows are bridged, about 310 rows (at most 468) in all.
-// Consumers wait on the slot's mbarrier, run the stencil sums, reduction and
-// pointwise/RK combine entirely from shared memory, store their outputs, and
-// release the slot.  Every wait is bounded; a timeout sets an error word and
-// the kernel drains its outstanding copies and returns.
+// Same math and lane split as stage_kernel.cuh, restructured around B200's
+// bulk copy engine.  A persistent CTA per SM runs one producer warp and 16
+// consumer warps over tiles of 64 consecutive nodes.  For every tile the
+// producer issues six cp.async.bulk copies (global -> shared, completing on an
+// mbarrier) into one of kStages ring slots: the tile's packed weights
+// (64 x 1 KB in FP64), packed stencil indices, pointwise records, own state
+// rows, and the H / D rows for stages 1-3 -- every contiguous per-node stream
+// of the stage.  Consumers wait on the slot's mbarrier, gather the neighbour
+// states through L1/L2 (the state arrays are L2-resident; a tile's neighbours
+// are scattered rows, which suits plain loads better than many small bulk
+// copies), run the stencil sums, reduction and pointwise/RK combine with
+// every other operand in shared memory, store their outputs and release the
+// slot.  Every wait is bounded; a timeout sets an error word and the kernel
+// drains its outstanding copies and returns.
 #pragma once
 
 #include "stage_kernel.cuh"
@@ -24,10 +21,8 @@
 
 namespace swe {
 
-constexpr int kTmaTile = 32;           // nodes per tile
-constexpr int kMaxRanges = 40;         // contiguous row ranges per neighbour window (<= 64)
-constexpr int kWinRows = 512;          // max rows per neighbour window
-constexpr int kTmaConsumerWarps = 8;
+constexpr int kTmaTile = 64;           // nodes per tile
+constexpr int kTmaConsumerWarps = kTmaTile / 4;
 constexpr int kTmaThreads = 32 * (kTmaConsumerWarps + 1);
 constexpr uint32_t kTmaWaitTries = 1u << 24;
 
@@ -50,16 +45,14 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 
 template <typename T>
 struct TmaLayout {
-    static constexpr int kW = kTmaTile * kSlots * 4 * (int)sizeof(T);    // weights
-    static constexpr int kIdx = kTmaTile * kSlots * 2;                     // uint16 local indices
-    static constexpr int kPt = kTmaTile * kPointStride * (int)sizeof(T);  // pointwise
-    static constexpr int kRow = 4 * (int)sizeof(T);                       // one state row
-    static constexpr int kRows = kTmaTile * kRow;                         // own / H / D rows
-    static constexpr int kWin = kWinRows * kRow;
-    static constexpr int oW = 0, oIdx = oW + kW, oPt = oIdx + kIdx, oOwn = oPt + kPt, oH = oOwn + kRows,
-                         oD = oH + kRows, oWin = oD + kRows;
-    static constexpr int kSlotBytes = ((oWin + kWin) + 127) / 128 * 128;
-    static constexpr int kStages = (sizeof(T) == 8) ? 3 : 5;
+    static constexpr int kWn = kSlots * 4 * (int)sizeof(T);     // weight bytes per node
+    static constexpr int kIdxn = kSlots * 4;                      // index bytes per node
+    static constexpr int kPtn = kPointStride * (int)sizeof(T);   // pointwise bytes per node
+    static constexpr int kRow = 4 * (int)sizeof(T);               // one state row
+    static constexpr int oW = 0, oIdx = oW + kTmaTile * kWn, oPt = oIdx + kTmaTile * kIdxn,
+                         oOwn = oPt + kTmaTile * kPtn, oH = oOwn + kTmaTile * kRow, oD = oH + kTmaTile * kRow;
+    static constexpr int kSlotBytes = ((oD + kTmaTile * kRow) + 127) / 128 * 128;
+    static constexpr int kStages = (sizeof(T) == 8) ? 2 : 4;
     static constexpr int kSmem = kStages * kSlotBytes;
 };
 
@@ -67,8 +60,6 @@ template <typename T>
 struct TmaArgs {
     StageArgs<T> s;
     int ntiles;
-    const uint16_t* idxl;   // [n][8 lanes][4] window-local indices
-    const int2* ranges;     // [ntiles][1 + kMaxRanges]: {count, rows} then {start, nrows}
     int* err;
 };
 
@@ -93,12 +84,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1) stage_tma_kernel(const TmaArgs
     const bool need_hd = MODE == kStage1 || MODE == kStage2 || MODE == kStage3;
 
     if (warp == kTmaConsumerWarps) {
-        // ---------------- producer (whole warp issues) ----------------
-        // The tile's range list is loaded by all lanes at once, window offsets
-        // come from a warp prefix sum, lane 0 posts the expected bytes and
-        // every lane issues its share of the bulk copies.  complete_tx may
-        // precede expect_tx inside a phase: the phase cannot close before
-        // lane 0's single arrive.
+        // ---------------- producer: lanes 0-5 each issue one stream ----------------
         int it = 0, issued = 0;
         for (int tile = blockIdx.x; tile < ta.ntiles; tile += gridDim.x, ++it) {
             const int s = it % Lay::kStages;
@@ -113,41 +99,21 @@ __global__ void __launch_bounds__(kTmaThreads, 1) stage_tma_kernel(const TmaArgs
             unsigned char* slot = smem + s * Lay::kSlotBytes;
             const long n0 = (long)tile * kTmaTile;
             const int nn = (int)min((long)kTmaTile, (long)a.n - n0);
-            const int2* tab = ta.ranges + (long)tile * (1 + kMaxRanges);
-            const int2 hdr = __ldg(tab);
-            // ranges r = lane and r = lane + 32 (kMaxRanges <= 64)
-            int2 r0 = make_int2(0, 0), r1 = make_int2(0, 0);
-            if (lane < hdr.x) r0 = __ldg(tab + 1 + lane);
-            if (lane + 32 < hdr.x) r1 = __ldg(tab + 1 + lane + 32);
-            int p0 = r0.y, p1 = r1.y;                       // inclusive prefix sums of the lengths
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t0 = __shfl_up_sync(0xffffffffu, p0, o);
-                const int t1 = __shfl_up_sync(0xffffffffu, p1, o);
-                if (lane >= o) { p0 += t0; p1 += t1; }
-            }
-            const int first_total = __shfl_sync(0xffffffffu, p0, 31);
-            const int off0 = p0 - r0.y, off1 = first_total + p1 - r1.y;
             if (lane == 0) {
-                const uint32_t tx = nn * (kSlots * 4 * sizeof(T) + kSlots * 2 + kPointStride * sizeof(T) + Lay::kRow) +
-                                    (need_hd ? 2 * nn * Lay::kRow : 0) + hdr.y * Lay::kRow;
+                const uint32_t tx = nn * (Lay::kWn + Lay::kIdxn + Lay::kPtn + Lay::kRow) + (need_hd ? 2 * nn * Lay::kRow : 0);
                 tma::arrive_expect_tx(&full[s], tx);
             }
+            __syncwarp();
             switch (lane) {
-                case 0: tma::bulk_g2s(slot + Lay::oW, a.W + n0 * kSlotChunks * Quad<T>::kUnits * 8,
-                                      nn * kSlots * 4 * sizeof(T), &full[s]); break;
-                case 1: tma::bulk_g2s(slot + Lay::oIdx, ta.idxl + n0 * kSlots, nn * kSlots * 2, &full[s]); break;
-                case 2: tma::bulk_g2s(slot + Lay::oPt, a.PT + n0 * kPointStride, nn * kPointStride * sizeof(T),
+                case 0: tma::bulk_g2s(slot + Lay::oW, a.W + n0 * kSlotChunks * Quad<T>::kUnits * 8, nn * Lay::kWn,
                                       &full[s]); break;
+                case 1: tma::bulk_g2s(slot + Lay::oIdx, a.idx + n0 * 8, nn * Lay::kIdxn, &full[s]); break;
+                case 2: tma::bulk_g2s(slot + Lay::oPt, a.PT + n0 * kPointStride, nn * Lay::kPtn, &full[s]); break;
                 case 3: tma::bulk_g2s(slot + Lay::oOwn, a.Kin + 4L * (n0 + a.pid0), nn * Lay::kRow, &full[s]); break;
                 case 4: if (need_hd) tma::bulk_g2s(slot + Lay::oH, a.H + 4L * n0, nn * Lay::kRow, &full[s]); break;
                 case 5: if (need_hd) tma::bulk_g2s(slot + Lay::oD, a.D + 4L * n0, nn * Lay::kRow, &full[s]); break;
                 default: break;
             }
-            if (lane < hdr.x)
-                tma::bulk_g2s(slot + Lay::oWin + off0 * Lay::kRow, a.Kin + 4L * r0.x, r0.y * Lay::kRow, &full[s]);
-            if (lane + 32 < hdr.x)
-                tma::bulk_g2s(slot + Lay::oWin + off1 * Lay::kRow, a.Kin + 4L * r1.x, r1.y * Lay::kRow, &full[s]);
             ++issued;
         }
         // drain: every issued slot must have landed before the CTA exits
@@ -157,7 +123,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1) stage_tma_kernel(const TmaArgs
         return;
     }
 
-    // ---------------- consumers ----------------
+// ---------------- consumers ----------------
     const int g = lane >> 3, k = lane & 7;
     constexpr int U = Quad<T>::kUnits;
     int it = 0;
@@ -170,13 +136,15 @@ __global__ void __launch_bounds__(kTmaThreads, 1) stage_tma_kernel(const TmaArgs
         }
         const unsigned char* slot = smem + s * Lay::kSlotBytes;
         const uint4* Ws = reinterpret_cast<const uint4*>(slot + Lay::oW);
-        const T* win = reinterpret_cast<const T*>(slot + Lay::oWin);
         const int t = warp * 4 + g;                       // node within the tile
         const long i = (long)tile * kTmaTile + t;
         const bool valid = i < a.n;
         const int tt = valid ? t : 0;
-        const ushort4 nb = *reinterpret_cast<const ushort4*>(slot + Lay::oIdx + (tt * 8 + k) * 8);
+        const int4 nb = *reinterpret_cast<const int4*>(slot + Lay::oIdx + (tt * 8 + k) * 16);
         const int nbr[4] = {nb.x, nb.y, nb.z, nb.w};
+        T kg[kSlotChunks][4];
+#pragma unroll
+        for (int m = 0; m < kSlotChunks; ++m) Quad<T>::load_row(a.Kin + 4L * nbr[m], kg[m]);
         T acc[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) acc[q] = T(0);
@@ -188,15 +156,12 @@ __global__ void __launch_bounds__(kTmaThreads, 1) stage_tma_kernel(const TmaArgs
                 const double2 w0 = *reinterpret_cast<const double2*>(wu);
                 const double2 w1 = *reinterpret_cast<const double2*>(wu + 8);
                 w[0] = w0.x; w[1] = w0.y; w[2] = w1.x; w[3] = w1.y;
-                const double2 k0 = *reinterpret_cast<const double2*>(win + 4 * nbr[m]);
-                const double2 k1 = *reinterpret_cast<const double2*>(win + 4 * nbr[m] + 2);
-                kv[0] = k0.x; kv[1] = k0.y; kv[2] = k1.x; kv[3] = k1.y;
             } else {
                 const float4 w0 = *reinterpret_cast<const float4*>(wu);
                 w[0] = w0.x; w[1] = w0.y; w[2] = w0.z; w[3] = w0.w;
-                const float4 k0 = *reinterpret_cast<const float4*>(win + 4 * nbr[m]);
-                kv[0] = k0.x; kv[1] = k0.y; kv[2] = k0.z; kv[3] = k0.w;
             }
+#pragma unroll
+            for (int f = 0; f < 4; ++f) kv[f] = kg[m][f];
 #pragma unroll
             for (int op = 0; op < 4; ++op)
 #pragma unroll

@@ -174,8 +174,8 @@ def test_invariants_match_oracle(plain, grid_l4):
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_pipelined_and_register_kernels_agree_bitwise(plain, prec):
-    """The bulk-copy pipelined kernel (RCM-ordered patches) and the
-    register-streaming kernel do the same arithmetic in the same order."""
+    """The bulk-copy pipelined kernel and the register-streaming kernel do the
+    same arithmetic in the same order."""
     _, d = generated_input(6)
     m, _ = layout.prepare(swe_input.to_model(d), use_rcm=True, simd_length=32)
     plain.init_model(m, prec)
@@ -197,7 +197,8 @@ def test_pipelined_and_register_kernels_agree_bitwise(plain, prec):
         assert rel_err(F0, oracle.Port(m, "fp64").eval_rhs(K)).max() <= 1e-12
 
 
-def test_unordered_patch_uses_register_kernel(plain, grid_l4):
+def test_select_kernel_rejects_unknown_choice(plain, grid_l4):
     _, d = grid_l4
-    plain.init_model(swe_input.to_model(d), "fp64")        # natural (unordered) node order
-    assert plain.kernel_info()["pipelined_available"] is False
+    plain.init_model(swe_input.to_model(d), "fp64")
+    with pytest.raises(capi.SweError):
+        plain.select_kernel(7)
