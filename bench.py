@@ -532,10 +532,12 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     t_kernel = k_time / max(k_launches, 1)
     achieved = ALG_BYTES[prec] * N / t_kernel / 1e9
+    kinfo = plain.kernel_info()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
-                "kernel": "swe::stage_kernel", "kernel_us": round(t_kernel * 1e6, 2),
-                "alg_bytes_per_node_stage": ALG_BYTES[prec]}
+                "kernel": "swe::stage_tma_kernel" if kinfo["in_use"] == "pipelined" else "swe::stage_kernel",
+                "kernel_us": round(t_kernel * 1e6, 2), "alg_bytes_per_node_stage": ALG_BYTES[prec],
+                "kernel_choice": kinfo}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

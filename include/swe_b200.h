@@ -96,11 +96,12 @@ int swe_cuda_step(int nsteps);
 /* Waits for all work of the library's stream. */
 int swe_cuda_sync(void);
 
-/* Kernel choice: 0 (default) = the bulk-copy pipelined stage kernel (a
- * producer warp streams each 64-node tile's weights, indices, pointwise data
- * and state rows into shared memory with cp.async.bulk); 1 = the
- * register-streaming kernel.  Both do the same arithmetic in the same order.
- * info[2] = {kernel in use (0/1), pipelined kernel available (0/1)}. */
+/* Kernel choice.  0 = the bulk-copy pipelined stage kernel (a producer warp
+ * streams each 64-node tile's weights, indices, pointwise data and state rows
+ * into shared memory with cp.async.bulk); 1 = the register-streaming kernel.
+ * Both do the same arithmetic in the same order; swe_cuda_init times both on
+ * the patch and keeps the faster.  info[4] = {kernel in use (0/1), pipelined
+ * kernel available (0/1), ns per eval launch of kernel 0, of kernel 1}. */
 int swe_cuda_select_kernel(int which);
 int swe_cuda_kernel_info(int* info);
 

@@ -17,7 +17,12 @@
 // sums of each of the 16 dot products are combined with a 3-step recursive-
 // halving shuffle (14 exchanges per lane instead of 80 for naive butterflies),
 // after which lane k holds sums 2k and 2k+1; they meet in shared memory and
-// lane 0 of the node runs the pointwise part and the stage combine.
+// lane 0 of the node runs the pointwise part and the stage combine.  The
+// operands of that epilogue (pointwise record, own state, H and D rows) are
+// fetched by the node's 8 lanes together with the gather and staged in
+// shared memory, and the next group's stencil indices are prefetched, so one
+// global round trip (the neighbour gather) remains on each group's critical
+// path.
 #pragma once
 
 #include "common.cuh"
@@ -152,27 +157,57 @@ constexpr int kStageWarps = kStageThreads / 32;
 
 template <typename T, int MODE>
 __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs<T> a) {
+    // per warp and node: 16 sums, then the epilogue operands staged by the
+    // node's 8 lanes (pointwise record, own state, H and D rows)
+    constexpr int kEp = kPointStride + 12;
     __shared__ __align__(16) T red[kStageWarps][4][16];
+    __shared__ __align__(16) T ep[kStageWarps][4][kEp];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int g = lane >> 3;       // node of this lane within the warp
     const int k = lane & 7;        // lane within the node
     const long warps_total = (long)gridDim.x * kStageWarps;
     constexpr int U = Quad<T>::kUnits;
+    constexpr bool kHD = MODE == kStage1 || MODE == kStage2 || MODE == kStage3;
 
-    for (long base = ((long)blockIdx.x * kStageWarps + warp) * 4; base < a.n; base += warps_total * 4) {
+    long base = ((long)blockIdx.x * kStageWarps + warp) * 4;
+    // indices of the first group; later groups' indices are prefetched one
+    // group ahead so that only the neighbour gather is on the critical path
+    int4 nb = __ldg(a.idx + min(base + g, (long)a.n - 1) * 8 + k);
+    for (; base < a.n; base += warps_total * 4) {
         const long i = base + g;
         const bool valid = i < a.n;
         const long ii = valid ? i : (long)a.n - 1;
-        const int4 nb = __ldg(a.idx + ii * 8 + k);
         const int nbr[4] = {nb.x, nb.y, nb.z, nb.w};
-
-        T w[kSlotChunks][4];
-#pragma unroll
-        for (int m = 0; m < kSlotChunks; ++m) Quad<T>::load(a.W, ((ii * kSlotChunks + m) * U) * 8 + k, w[m]);
         T kv[kSlotChunks][4];
 #pragma unroll
         for (int m = 0; m < kSlotChunks; ++m) Quad<T>::load_row(a.Kin + 4L * nbr[m], kv[m]);
+        T w[kSlotChunks][4];
+#pragma unroll
+        for (int m = 0; m < kSlotChunks; ++m) Quad<T>::load(a.W, ((ii * kSlotChunks + m) * U) * 8 + k, w[m]);
+        // epilogue operands: lanes 0-4 fetch the pointwise record (4 values
+        // each), lanes 5-7 the own state and the H and D rows
+        {
+            T* e = ep[warp][g];
+            if (k < 5) {
+                T p[4];
+                Quad<T>::load_row(a.PT + ii * kPointStride + 4 * k, p);
+#pragma unroll
+                for (int x = 0; x < 4; ++x) e[4 * k + x] = p[x];
+            } else if (k == 5) {
+                T q[4];
+                Quad<T>::load_row(a.Kin + 4L * (ii + a.pid0), q);
+#pragma unroll
+                for (int x = 0; x < 4; ++x) e[kPointStride + x] = q[x];
+            } else if (kHD) {
+                T r[4];
+                Quad<T>::load_row_rw((k == 6 ? a.H : a.D) + 4 * ii, r);
+#pragma unroll
+                for (int x = 0; x < 4; ++x) e[kPointStride + 4 * (k - 5) + x] = r[x];
+            }
+        }
+        const long nbase = base + warps_total * 4;
+        if (nbase < a.n) nb = __ldg(a.idx + min(nbase + g, (long)a.n - 1) * 8 + k);
 
         T acc[16];
 #pragma unroll
@@ -191,13 +226,15 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         __syncwarp();
 
         if (k == 0 && valid) {
+            const T* e = ep[warp][g];
             T s[16];
 #pragma unroll
             for (int t = 0; t < 16; ++t) s[t] = red[warp][g][t];
             T q[4];
-            Quad<T>::load_row(a.Kin + 4L * (i + a.pid0), q);
+#pragma unroll
+            for (int x = 0; x < 4; ++x) q[x] = e[kPointStride + x];
             T F[4];
-            pointwise_rhs(s, q, a.PT + i * kPointStride, a.gh0, F);
+            pointwise_rhs(s, q, e, a.gh0, F);
             if (MODE == kEvalOnly) {
                 Quad<T>::store_row(a.F + 4 * i, F);
             } else if (MODE == kStage0) {
@@ -209,25 +246,21 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
                 Quad<T>::store_row(a.Kout + 4 * i, kn);
             } else if (MODE == kStage1 || MODE == kStage2) {
                 // update_D(D, F, 2) and eval_K(H, K, F, c)
-                T h[4], d[4], kn[4];
-                Quad<T>::load_row(a.H + 4 * i, h);
-                Quad<T>::load_row_rw(a.D + 4 * i, d);
+                T kn[4], d[4];
 #pragma unroll
                 for (int t = 0; t < 4; ++t) {
-                    d[t] = Quad<T>::axpy(d[t], T(2), F[t]);
-                    kn[t] = Quad<T>::axpy(h[t], a.c, F[t]);
+                    d[t] = Quad<T>::axpy(e[kPointStride + 8 + t], T(2), F[t]);
+                    kn[t] = Quad<T>::axpy(e[kPointStride + 4 + t], a.c, F[t]);
                 }
                 Quad<T>::store_row(a.D + 4 * i, d);
                 Quad<T>::store_row(a.Kout + 4 * i, kn);
             } else {
                 // update_D(D, F, 1) and update_H(H, D, dt)
-                T h[4], d[4];
-                Quad<T>::load_row_rw(a.H + 4 * i, h);
-                Quad<T>::load_row_rw(a.D + 4 * i, d);
+                T h[4];
 #pragma unroll
                 for (int t = 0; t < 4; ++t) {
-                    d[t] = Quad<T>::axpy(d[t], T(1), F[t]);
-                    h[t] = Quad<T>::update_h(h[t], a.dt6, d[t]);
+                    const T d = Quad<T>::axpy(e[kPointStride + 8 + t], T(1), F[t]);
+                    h[t] = Quad<T>::update_h(e[kPointStride + 4 + t], a.dt6, d);
                 }
                 Quad<T>::store_row(a.H + 4 * i, h);
             }
