@@ -232,23 +232,6 @@ struct Plain {
 
     bool use_tma() const { return tma_ok && kernel_choice == 0; }
 
-    // Every stage kernel is launched with programmatic stream serialization:
-    // it may start while the previous stage drains (see pdl_wait()).
-    template <typename T, typename K, typename A>
-    void launch_pdl(K kernel, int grid_, int threads, int smem, const A& args) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(grid_);
-        cfg.blockDim = dim3(threads);
-        cfg.dynamicSmemBytes = smem;
-        cfg.stream = stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, kernel, args);
-    }
-
     template <typename T>
     void launch_t(int mode) {
         const StageArgs<T> a = args<T>(mode);
@@ -256,20 +239,20 @@ struct Plain {
             TmaArgs<T> ta{a, ntiles, err};
             const int sm = TmaLayout<T>::kSmem;
             switch (mode) {
-                case 0: launch_pdl<T>(stage_tma_kernel<T, kStage0>, grid_tma, kTmaThreads, sm, ta); break;
-                case 1: launch_pdl<T>(stage_tma_kernel<T, kStage1>, grid_tma, kTmaThreads, sm, ta); break;
-                case 2: launch_pdl<T>(stage_tma_kernel<T, kStage2>, grid_tma, kTmaThreads, sm, ta); break;
-                case 3: launch_pdl<T>(stage_tma_kernel<T, kStage3>, grid_tma, kTmaThreads, sm, ta); break;
-                default: launch_pdl<T>(stage_tma_kernel<T, kEvalOnly>, grid_tma, kTmaThreads, sm, ta); break;
+                case 0: stage_tma_kernel<T, kStage0><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
+                case 1: stage_tma_kernel<T, kStage1><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
+                case 2: stage_tma_kernel<T, kStage2><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
+                case 3: stage_tma_kernel<T, kStage3><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
+                default: stage_tma_kernel<T, kEvalOnly><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
             }
             return;
         }
         switch (mode) {
-            case 0: launch_pdl<T>(stage_kernel<T, kStage0>, grid, kStageThreads, 0, a); break;
-            case 1: launch_pdl<T>(stage_kernel<T, kStage1>, grid, kStageThreads, 0, a); break;
-            case 2: launch_pdl<T>(stage_kernel<T, kStage2>, grid, kStageThreads, 0, a); break;
-            case 3: launch_pdl<T>(stage_kernel<T, kStage3>, grid, kStageThreads, 0, a); break;
-            default: launch_pdl<T>(stage_kernel<T, kEvalOnly>, grid, kStageThreads, 0, a); break;
+            case 0: stage_kernel<T, kStage0><<<grid, kStageThreads, 0, stream>>>(a); break;
+            case 1: stage_kernel<T, kStage1><<<grid, kStageThreads, 0, stream>>>(a); break;
+            case 2: stage_kernel<T, kStage2><<<grid, kStageThreads, 0, stream>>>(a); break;
+            case 3: stage_kernel<T, kStage3><<<grid, kStageThreads, 0, stream>>>(a); break;
+            default: stage_kernel<T, kEvalOnly><<<grid, kStageThreads, 0, stream>>>(a); break;
         }
     }
 

@@ -104,13 +104,6 @@ struct Quad<float> {
     }
 };
 
-// Programmatic dependent launch: a stage kernel is launched while the
-// previous stage is still running; it may read static data (weights, indices,
-// pointwise records) at once but must wait for the previous grid before it
-// touches the states that grid writes.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
 // 8-lane recursive-halving reduce-scatter of 16 partial sums: on return lane
 // k (0..7 within its group) holds the group totals of sums 2k and 2k+1.
 template <typename T>
@@ -178,45 +171,40 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
     constexpr bool kHD = MODE == kStage1 || MODE == kStage2 || MODE == kStage3;
 
     long base = ((long)blockIdx.x * kStageWarps + warp) * 4;
-    pdl_launch_dependents();
     // indices of the first group; later groups' indices are prefetched one
     // group ahead so that only the neighbour gather is on the critical path
     int4 nb = __ldg(a.idx + min(base + g, (long)a.n - 1) * 8 + k);
-    bool waited = false;
     for (; base < a.n; base += warps_total * 4) {
         const long i = base + g;
         const bool valid = i < a.n;
         const long ii = valid ? i : (long)a.n - 1;
         const int nbr[4] = {nb.x, nb.y, nb.z, nb.w};
-        // static operands first: they do not depend on the previous stage
-        T w[kSlotChunks][4];
-#pragma unroll
-        for (int m = 0; m < kSlotChunks; ++m) Quad<T>::load(a.W, ((ii * kSlotChunks + m) * U) * 8 + k, w[m]);
-        T* e = ep[warp][g];
-        if (k < 5) {
-            T p[4];
-            Quad<T>::load_row(a.PT + ii * kPointStride + 4 * k, p);
-#pragma unroll
-            for (int x = 0; x < 4; ++x) e[4 * k + x] = p[x];
-        }
-        if (!waited) {
-            pdl_wait();
-            waited = true;
-        }
         T kv[kSlotChunks][4];
 #pragma unroll
         for (int m = 0; m < kSlotChunks; ++m) Quad<T>::load_row(a.Kin + 4L * nbr[m], kv[m]);
-        // epilogue operands from the states: own row (lane 5), H and D rows (lanes 6, 7)
-        if (k == 5) {
-            T q[4];
-            Quad<T>::load_row(a.Kin + 4L * (ii + a.pid0), q);
+        T w[kSlotChunks][4];
 #pragma unroll
-            for (int x = 0; x < 4; ++x) e[kPointStride + x] = q[x];
-        } else if (k > 5 && kHD) {
-            T r[4];
-            Quad<T>::load_row_rw((k == 6 ? a.H : a.D) + 4 * ii, r);
+        for (int m = 0; m < kSlotChunks; ++m) Quad<T>::load(a.W, ((ii * kSlotChunks + m) * U) * 8 + k, w[m]);
+        // epilogue operands: lanes 0-4 fetch the pointwise record (4 values
+        // each), lanes 5-7 the own state and the H and D rows
+        {
+            T* e = ep[warp][g];
+            if (k < 5) {
+                T p[4];
+                Quad<T>::load_row(a.PT + ii * kPointStride + 4 * k, p);
 #pragma unroll
-            for (int x = 0; x < 4; ++x) e[kPointStride + 4 * (k - 5) + x] = r[x];
+                for (int x = 0; x < 4; ++x) e[4 * k + x] = p[x];
+            } else if (k == 5) {
+                T q[4];
+                Quad<T>::load_row(a.Kin + 4L * (ii + a.pid0), q);
+#pragma unroll
+                for (int x = 0; x < 4; ++x) e[kPointStride + x] = q[x];
+            } else if (kHD) {
+                T r[4];
+                Quad<T>::load_row_rw((k == 6 ? a.H : a.D) + 4 * ii, r);
+#pragma unroll
+                for (int x = 0; x < 4; ++x) e[kPointStride + 4 * (k - 5) + x] = r[x];
+            }
         }
         const long nbase = base + warps_total * 4;
         if (nbase < a.n) nb = __ldg(a.idx + min(nbase + g, (long)a.n - 1) * 8 + k);

@@ -82,7 +82,6 @@ __global__ void __launch_bounds__(kTmaThreads, 1) stage_tma_kernel(const TmaArgs
     }
     __syncthreads();
     const bool need_hd = MODE == kStage1 || MODE == kStage2 || MODE == kStage3;
-    pdl_launch_dependents();
 
     if (warp == kTmaConsumerWarps) {
         // ---------------- producer: lanes 0-5 each issue one stream ----------------
@@ -105,19 +104,14 @@ __global__ void __launch_bounds__(kTmaThreads, 1) stage_tma_kernel(const TmaArgs
                 tma::arrive_expect_tx(&full[s], tx);
             }
             __syncwarp();
-            // static streams first (lanes 0-2); the state rows (lanes 3-5) wait
-            // for the previous stage's grid on the first tile
             switch (lane) {
                 case 0: tma::bulk_g2s(slot + Lay::oW, a.W + n0 * kSlotChunks * Quad<T>::kUnits * 8, nn * Lay::kWn,
                                       &full[s]); break;
                 case 1: tma::bulk_g2s(slot + Lay::oIdx, a.idx + n0 * 8, nn * Lay::kIdxn, &full[s]); break;
                 case 2: tma::bulk_g2s(slot + Lay::oPt, a.PT + n0 * kPointStride, nn * Lay::kPtn, &full[s]); break;
-                case 3: if (it == 0) pdl_wait();
-                        tma::bulk_g2s(slot + Lay::oOwn, a.Kin + 4L * (n0 + a.pid0), nn * Lay::kRow, &full[s]); break;
-                case 4: if (it == 0) pdl_wait();
-                        if (need_hd) tma::bulk_g2s(slot + Lay::oH, a.H + 4L * n0, nn * Lay::kRow, &full[s]); break;
-                case 5: if (it == 0) pdl_wait();
-                        if (need_hd) tma::bulk_g2s(slot + Lay::oD, a.D + 4L * n0, nn * Lay::kRow, &full[s]); break;
+                case 3: tma::bulk_g2s(slot + Lay::oOwn, a.Kin + 4L * (n0 + a.pid0), nn * Lay::kRow, &full[s]); break;
+                case 4: if (need_hd) tma::bulk_g2s(slot + Lay::oH, a.H + 4L * n0, nn * Lay::kRow, &full[s]); break;
+                case 5: if (need_hd) tma::bulk_g2s(slot + Lay::oD, a.D + 4L * n0, nn * Lay::kRow, &full[s]); break;
                 default: break;
             }
             ++issued;
