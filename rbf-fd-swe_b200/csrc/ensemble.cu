@@ -1,75 +1,137 @@
 // Batched-ensemble form: swe_ens_* entry points of include/swe_b200.h.
 //
-// B members (a multiple of 32, at most 64) share one grid.  The library
-// orders nodes by the reference's RCM permutation (rcm/rcm.c:9-62, restated in
-// host_layout.cu) so that tiles of consecutive nodes have compact neighbour
-// sets, builds per-tile neighbour tables once, keeps all member states
-// device-resident, and runs each RK4 stage as one tcgen05 kernel
-// (ensemble_kernel.cuh).  An autotuner times every (tile nodes T, members per
-// CTA) variant on the live state and keeps the fastest; whole steps replay a
-// captured CUDA graph.
+// B members (32 or 64) share one grid.  The library orders nodes along a
+// Hilbert curve on the six faces of the cube around the sphere, so that 32
+// consecutive nodes form a compact patch, and builds per-tile tables once:
+// the tile's unique neighbour rows (ascending, padded to 16-row chunks), its
+// stencil weights as entries sorted by chunk, the node that centres it, and
+// the operators' row sums.  All member states stay device-resident; each RK4
+// stage is one persistent tcgen05 kernel (ensemble_kernel.cuh).  An autotuner
+// times each members-per-CTA variant on the live state and keeps the fastest;
+// whole steps replay a captured CUDA graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <numeric>
 #include <vector>
 
 #include "common.cuh"
 #include "ensemble_kernel.cuh"
 
-extern "C" int swe_host_rcm_mapping(int n, int nnbr, const int* idx, int* mapping);
-
 namespace swe {
 namespace {
 
-// Per-tile neighbour tables for one tile size T.
-struct Tables {
-    bool ok = false;
-    int ntiles = 0, kmax_seen = 0;
-    int* rows = nullptr;
-    int* kcount = nullptr;
-    uint8_t* local = nullptr;
-};
-
-struct Variant {
-    int T = 4, hpc = 1;
-    bool usable = false;
-};
-
-template <int T>
-bool build_tiles(int n, int nnbr, const std::vector<int>& idx, std::vector<int>& rows, std::vector<int>& kcount,
-                 std::vector<uint8_t>& local, int& ntiles, int& kmax_seen) {
-    using G = EnsTile<T>;
-    ntiles = (n + T - 1) / T;
-    rows.assign((size_t)ntiles * G::kKmax, -1);
-    kcount.assign(ntiles, 0);
-    local.assign((size_t)ntiles * T * 32, 255);
-    std::vector<int> u;
-    kmax_seen = 0;
-    for (int tile = 0; tile < ntiles; ++tile) {
-        u.clear();
-        for (int t = 0; t < T; ++t) {
-            const long node = (long)tile * T + t;
-            if (node >= n) break;
-            for (int j = 0; j < nnbr; ++j) u.push_back(idx[node * nnbr + j]);
-        }
-        std::sort(u.begin(), u.end());
-        u.erase(std::unique(u.begin(), u.end()), u.end());
-        kmax_seen = std::max(kmax_seen, (int)u.size());
-        if ((int)u.size() > G::kKmax) return false;
-        kcount[tile] = (int)u.size();
-        std::copy(u.begin(), u.end(), rows.begin() + (size_t)tile * G::kKmax);
-        for (int t = 0; t < T; ++t) {
-            const long node = (long)tile * T + t;
-            if (node >= n) break;
-            for (int j = 0; j < nnbr; ++j) {
-                const int k = (int)(std::lower_bound(u.begin(), u.end(), idx[node * nnbr + j]) - u.begin());
-                local[((size_t)tile * T + t) * 32 + j] = (uint8_t)k;
+// Hilbert index of (x, y) on a 2^bits grid: the classic quadrant walk that
+// rotates / reflects the lower bits at every level.
+uint64_t hilbert_index(uint32_t x, uint32_t y, int bits) {
+    const uint32_t n = 1u << bits;
+    uint64_t d = 0;
+    for (uint32_t s = n >> 1; s > 0; s >>= 1) {
+        const uint32_t rx = (x & s) ? 1u : 0u, ry = (y & s) ? 1u : 0u;
+        d += (uint64_t)s * s * ((3u * rx) ^ ry);
+        if (ry == 0) {
+            if (rx == 1) {
+                x = n - 1 - x;
+                y = n - 1 - y;
             }
+            std::swap(x, y);
         }
     }
-    return true;
+    return d;
 }
+
+// mapping[new] = old: nodes sorted by (cube face, Hilbert index of the
+// equal-angle face coordinates, old index).
+std::vector<int> curve_order(int n, const double* x, const double* y, const double* z) {
+    constexpr int kBits = 16;
+    std::vector<uint64_t> key(n);
+    for (int i = 0; i < n; ++i) {
+        const double c[3] = {x[i], y[i], z[i]};
+        int ax = 0;
+        for (int d = 1; d < 3; ++d)
+            if (std::fabs(c[d]) > std::fabs(c[ax])) ax = d;
+        const int face = 2 * ax + (c[ax] > 0.0 ? 1 : 0);
+        const double m = std::fabs(c[ax]) > 0.0 ? std::fabs(c[ax]) : 1.0;
+        const int o0 = ax == 0 ? 1 : 0, o1 = ax == 2 ? 1 : 2;
+        uint32_t q[2];
+        const double uv[2] = {c[o0] / m, c[o1] / m};
+        for (int d = 0; d < 2; ++d) {
+            double a = std::atan(uv[d]) * (4.0 / 3.14159265358979323846);   // [-1, 1]
+            a = std::min(1.0, std::max(-1.0, a));
+            q[d] = (uint32_t)((a + 1.0) * 0.5 * (double)((1u << kBits) - 1) + 0.5);
+        }
+        key[i] = ((uint64_t)face << 40) | hilbert_index(q[0], q[1], kBits);
+    }
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+    return order;
+}
+
+// Per-tile tables (node indices in the curve order).
+struct TileTables {
+    int ntiles = 0, nchunks = 0, max_rows = 0;
+    std::vector<int> row_off, rows, ent_off, ent_tk, centre;
+    std::vector<float> ent_w;   // 4 per entry
+};
+
+TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std::vector<float>& w4,
+                       const std::vector<double>& X) {
+    TileTables tb;
+    tb.ntiles = (n + kEnsTileNodes - 1) / kEnsTileNodes;
+    tb.row_off.assign(tb.ntiles + 1, 0);
+    tb.centre.assign(tb.ntiles, 0);
+    tb.ent_off.push_back(0);
+    std::vector<int> u;
+    std::vector<std::vector<int>> bucket;
+    for (int tile = 0; tile < tb.ntiles; ++tile) {
+        const int n0 = tile * kEnsTileNodes, n1 = std::min(n, n0 + kEnsTileNodes);
+        u.clear();
+        for (int i = n0; i < n1; ++i)
+            for (int j = 0; j < nnbr; ++j) u.push_back(ridx[(size_t)i * nnbr + j]);
+        std::sort(u.begin(), u.end());
+        u.erase(std::unique(u.begin(), u.end()), u.end());
+        tb.max_rows = std::max(tb.max_rows, (int)u.size());
+        const int nch = ((int)u.size() + kEnsKc - 1) / kEnsKc;
+        for (int k = 0; k < nch * kEnsKc; ++k) tb.rows.push_back(k < (int)u.size() ? u[k] : -1);
+        tb.row_off[tile + 1] = (int)tb.rows.size();
+        // weight entries, grouped by chunk
+        bucket.assign(nch, {});
+        for (int i = n0; i < n1; ++i)
+            for (int j = 0; j < nnbr; ++j) {
+                const int k = (int)(std::lower_bound(u.begin(), u.end(), ridx[(size_t)i * nnbr + j]) - u.begin());
+                bucket[k / kEnsKc].push_back(((i - n0) | ((k % kEnsKc) << 8)) | (j << 16));
+            }
+        for (int c = 0; c < nch; ++c) {
+            for (int e : bucket[c]) {
+                const int t = e & 0xff, j = e >> 16;
+                tb.ent_tk.push_back(e & 0xffff);
+                const float* w = &w4[((size_t)(n0 + t) * nnbr + j) * 4];
+                tb.ent_w.insert(tb.ent_w.end(), w, w + 4);
+            }
+            tb.ent_off.push_back((int)tb.ent_tk.size());
+        }
+        // centre: the tile node nearest the tile's centroid
+        double cx = 0, cy = 0, cz = 0;
+        for (int i = n0; i < n1; ++i) { cx += X[3 * i]; cy += X[3 * i + 1]; cz += X[3 * i + 2]; }
+        cx /= (n1 - n0); cy /= (n1 - n0); cz /= (n1 - n0);
+        double best = 1e300;
+        for (int i = n0; i < n1; ++i) {
+            const double d = (X[3 * i] - cx) * (X[3 * i] - cx) + (X[3 * i + 1] - cy) * (X[3 * i + 1] - cy) +
+                             (X[3 * i + 2] - cz) * (X[3 * i + 2] - cz);
+            if (d < best) { best = d; tb.centre[tile] = i; }
+        }
+    }
+    tb.nchunks = (int)tb.rows.size() / kEnsKc;
+    return tb;
+}
+
+struct Variant {
+    int mpc = 32;
+    bool usable = false;
+};
 
 __global__ void ens_invariants_kernel(const float* __restrict__ H32, const double* __restrict__ Hh,
                                       const float4* __restrict__ PT, int n, int members, double gh0,
@@ -122,54 +184,60 @@ __global__ void ens_gather_state(const float* __restrict__ H32, const double* __
 
 struct Ensemble {
     bool ready = false;
-    int members = 0, n = 0, nnbr = 0, mf = 0, halves = 0;
+    int members = 0, n = 0, nnbr = 0, mf = 0, nsm = 148;
     double gh0 = 0, dt = 0;
     std::vector<int> perm_h;
     int* perm = nullptr;
-    float4* W = nullptr;
     float4* PT = nullptr;
+    float4* RS = nullptr;
     float *H32 = nullptr, *D32 = nullptr, *Ka = nullptr, *Kb = nullptr, *F = nullptr, *Kx = nullptr;
     double *Hh = nullptr, *Dh = nullptr, *io = nullptr, *inv = nullptr;
     float* bkH32 = nullptr;
     double* bkHh = nullptr;
     int* err = nullptr;
-    Tables tab[2];        // T = 4, T = 8
-    Variant var[4];       // (4,1) (4,2) (8,1) (8,2)
+    // tile tables
+    int ntiles = 0, max_rows = 0;
+    int *row_off = nullptr, *rows = nullptr, *ent_off = nullptr, *ent_tk = nullptr, *centre = nullptr;
+    float4* ent_w = nullptr;
+    Variant var[2];       // members per CTA: 32, 64
     int chosen = -1;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool timing = false;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     bool timed = false;
-    double tune_ms[4] = {0, 0, 0, 0};
+    double tune_ms[2] = {-1, -1};
 
     void release() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
-        void* ps[] = {perm, W, PT, H32, D32, Ka, Kb, F, Kx, Hh, Dh, io, inv, bkH32, bkHh, err};
+        void* ps[] = {perm, PT, RS, H32, D32, Ka, Kb, F, Kx, Hh, Dh, io, inv, bkH32, bkHh, err,
+                      row_off, rows, ent_off, ent_tk, centre, ent_w};
         for (void* p : ps) if (p) cudaFree(p);
-        perm = nullptr; W = nullptr; PT = nullptr; H32 = D32 = Ka = Kb = F = Kx = nullptr;
+        perm = nullptr; PT = nullptr; RS = nullptr; H32 = D32 = Ka = Kb = F = Kx = nullptr;
         Hh = Dh = io = inv = nullptr; bkH32 = nullptr; bkHh = nullptr; err = nullptr;
-        for (auto& t : tab) {
-            if (t.rows) cudaFree(t.rows);
-            if (t.kcount) cudaFree(t.kcount);
-            if (t.local) cudaFree(t.local);
-            t = Tables{};
-        }
+        row_off = rows = ent_off = ent_tk = centre = nullptr;
+        ent_w = nullptr;
         for (auto& v : var) v = Variant{};
         for (auto& e : ev) { if (e) cudaEventDestroy(e); e = nullptr; }
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
         chosen = -1;
+        tune_ms[0] = tune_ms[1] = -1;
         ready = false;
     }
 
-    EnsArgs args(int mode) const {
+    EnsArgs args(int mode, int mpc) const {
         EnsArgs a{};
         a.n = n;
+        a.ntiles = ntiles;
+        a.members = members;
+        a.units = ntiles * (members / mpc);
         a.mf = mf;
-        a.W = W;
+        a.row_off = row_off; a.rows = rows; a.ent_off = ent_off; a.ent_tk = ent_tk; a.ent_w = ent_w;
+        a.centre = centre;
         a.PT = PT;
+        a.RS = RS;
         a.H32 = H32; a.Hh = Hh; a.D32 = D32; a.Dh = Dh; a.F = F;
         a.gh0 = (float)gh0;
         a.dt6 = dt / 6.0;
@@ -184,47 +252,34 @@ struct Ensemble {
         return a;
     }
 
-    template <int T, int HPC>
-    static size_t smem_bytes() {
-        return (size_t)HPC * 2 * EnsTile<T>::kABytes + 2 * EnsTile<T>::kBBytes;
-    }
-
-    template <int T, int HPC>
-    void launch_tv(int mode) {
-        const Tables& tb = tab[T == 8];
-        EnsArgs a = args(mode);
-        a.rows = tb.rows;
-        a.kcount = tb.kcount;
-        a.local = tb.local;
-        a.ntiles = tb.ntiles;
-        const dim3 grid(tb.ntiles, halves / HPC);
-        const size_t sm = smem_bytes<T, HPC>();
+    template <int MPC>
+    void launch_v(int mode) {
+        using C = EnsCfg<MPC>;
+        const EnsArgs a = args(mode, MPC);
+        const int grid = std::min(a.units, nsm);
         switch (mode) {
-            case 0: ens_stage_kernel<T, HPC, kStage0><<<grid, 128 * HPC, sm, stream>>>(a); break;
-            case 1: ens_stage_kernel<T, HPC, kStage1><<<grid, 128 * HPC, sm, stream>>>(a); break;
-            case 2: ens_stage_kernel<T, HPC, kStage2><<<grid, 128 * HPC, sm, stream>>>(a); break;
-            case 3: ens_stage_kernel<T, HPC, kStage3><<<grid, 128 * HPC, sm, stream>>>(a); break;
-            default: ens_stage_kernel<T, HPC, kEvalOnly><<<grid, 128 * HPC, sm, stream>>>(a); break;
+            case 0: ens_stage_kernel<MPC, kStage0><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 1: ens_stage_kernel<MPC, kStage1><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 2: ens_stage_kernel<MPC, kStage2><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 3: ens_stage_kernel<MPC, kStage3><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            default: ens_stage_kernel<MPC, kEvalOnly><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
         }
     }
 
     void launch(int vi, int mode) {
-        const Variant& v = var[vi];
-        if (v.T == 4 && v.hpc == 1) launch_tv<4, 1>(mode);
-        else if (v.T == 4) launch_tv<4, 2>(mode);
-        else if (v.hpc == 1) launch_tv<8, 1>(mode);
-        else launch_tv<8, 2>(mode);
+        if (var[vi].mpc == 64) launch_v<64>(mode);
+        else launch_v<32>(mode);
         count_launch();
     }
 
-    template <int T, int HPC>
+    template <int MPC>
     static int set_attrs() {
-        const int sm = (int)smem_bytes<T, HPC>();
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, HPC, kStage0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, HPC, kStage1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, HPC, kStage2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, HPC, kStage3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, HPC, kEvalOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        const int sm = EnsCfg<MPC>::kSmem;
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kEvalOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
         return SWE_OK;
     }
 
@@ -250,7 +305,7 @@ struct Ensemble {
         SWE_CUDA_TRY(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
         SWE_CUDA_TRY(cudaStreamSynchronize(stream));
         if (h) {
-            set_error("ensemble kernel: a bounded mbarrier wait for tensor-core completion ran out");
+            set_error("ensemble kernel: a bounded mbarrier wait ran out (code %d)", h);
             return SWE_ERR_TIMEOUT;
         }
         return SWE_OK;
@@ -277,7 +332,7 @@ int tune(Ensemble& E) {
     SWE_CUDA_TRY(cudaEventCreate(&e1));
     float best = 1e30f;
     int best_i = -1;
-    for (int vi = 0; vi < 4; ++vi) {
+    for (int vi = 0; vi < 2; ++vi) {
         E.tune_ms[vi] = -1.0;
         if (!E.var[vi].usable) continue;
         for (int w = 0; w < 2; ++w)
@@ -325,31 +380,40 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
         set_error("swe_ens_init: null array");
         return SWE_ERR_ARG;
     }
+    for (long e = 0; e < (long)n * nnbr; ++e)
+        if (idx[e] < 0 || idx[e] >= n) { set_error("swe_ens_init: idx[%ld] = %d out of range", e, idx[e]); return SWE_ERR_INDEX; }
     Ensemble& E = g_ens;
     E.release();
     E.members = members;
     E.n = n;
     E.nnbr = nnbr;
     E.mf = 4 * members;
-    E.halves = members / 32;
     E.gh0 = gh0;
     E.dt = dt;
-    // RCM order (mapping[new] = old) and the renumbered stencils
-    E.perm_h.assign(n, 0);
-    SWE_TRY(swe_host_rcm_mapping(n, nnbr, idx, E.perm_h.data()));
+    {
+        int dev = 0;
+        SWE_CUDA_TRY(cudaGetDevice(&dev));
+        SWE_CUDA_TRY(cudaDeviceGetAttribute(&E.nsm, cudaDevAttrMultiProcessorCount, dev));
+    }
+    // curve order (mapping[new] = old) and the renumbered stencils
+    E.perm_h = curve_order(n, x, y, z);
     std::vector<int> inv(n), ridx((size_t)n * nnbr);
     for (int i = 0; i < n; ++i) inv[E.perm_h[i]] = i;
     for (long i = 0; i < n; ++i)
         for (int j = 0; j < nnbr; ++j) ridx[i * nnbr + j] = inv[idx[(long)E.perm_h[i] * nnbr + j]];
-    // static data in FP32, RCM order
-    std::vector<float> w((size_t)n * 32 * 4, 0.f), pt((size_t)n * kPointStride, 0.f);
+    // static data in FP32, curve order; operator row sums in FP64 of the FP32 weights
+    std::vector<float> w((size_t)n * nnbr * 4), pt((size_t)n * kPointStride, 0.f), rs((size_t)n * 4);
+    std::vector<double> X((size_t)n * 3);
     for (long i = 0; i < n; ++i) {
         const long o = E.perm_h[i];
+        double sum[4] = {0, 0, 0, 0};
         for (int j = 0; j < nnbr; ++j) {
-            float* q = &w[((size_t)i * 32 + j) * 4];
+            float* q = &w[((size_t)i * nnbr + j) * 4];
             q[0] = (float)Dx[o * nnbr + j]; q[1] = (float)Dy[o * nnbr + j];
             q[2] = (float)Dz[o * nnbr + j]; q[3] = (float)L[o * nnbr + j];
+            for (int op = 0; op < 4; ++op) sum[op] += (double)q[op];
         }
+        for (int op = 0; op < 4; ++op) rs[i * 4 + op] = (float)sum[op];
         float* r = &pt[(size_t)i * kPointStride];
         r[PT_X] = (float)x[o]; r[PT_Y] = (float)y[o]; r[PT_Z] = (float)z[o]; r[PT_F] = (float)f[o];
         r[PT_GHM] = (float)ghm[o];
@@ -357,12 +421,28 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
             r[PT_PU + c] = (float)p_u[o * 3 + c]; r[PT_PV + c] = (float)p_v[o * 3 + c];
             r[PT_PW + c] = (float)p_w[o * 3 + c]; r[PT_GG + c] = (float)gradghm[o * 3 + c];
         }
+        X[3 * i] = x[o]; X[3 * i + 1] = y[o]; X[3 * i + 2] = z[o];
     }
+    const TileTables tb = build_tiles(n, nnbr, ridx, w, X);
+    E.ntiles = tb.ntiles;
+    E.max_rows = tb.max_rows;
     SWE_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
     const size_t s32 = (size_t)n * E.mf * sizeof(float), s64 = (size_t)n * members * sizeof(double);
-    SWE_CUDA_TRY(cudaMalloc(&E.perm, n * sizeof(int)));
-    SWE_CUDA_TRY(cudaMalloc(&E.W, w.size() * sizeof(float)));
-    SWE_CUDA_TRY(cudaMalloc(&E.PT, pt.size() * sizeof(float)));
+    auto upload = [](auto** dst, const auto& vec) -> int {
+        const size_t bytes = vec.size() * sizeof(vec[0]);
+        SWE_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(dst), std::max<size_t>(bytes, 16)));
+        if (bytes) SWE_CUDA_TRY(cudaMemcpy(*dst, vec.data(), bytes, cudaMemcpyHostToDevice));
+        return SWE_OK;
+    };
+    SWE_TRY(upload(&E.perm, E.perm_h));
+    SWE_TRY(upload(reinterpret_cast<float**>(&E.PT), pt));
+    SWE_TRY(upload(reinterpret_cast<float**>(&E.RS), rs));
+    SWE_TRY(upload(&E.row_off, tb.row_off));
+    SWE_TRY(upload(&E.rows, tb.rows));
+    SWE_TRY(upload(&E.ent_off, tb.ent_off));
+    SWE_TRY(upload(&E.ent_tk, tb.ent_tk));
+    SWE_TRY(upload(&E.centre, tb.centre));
+    SWE_TRY(upload(reinterpret_cast<float**>(&E.ent_w), tb.ent_w));
     for (float** p : {&E.H32, &E.D32, &E.Ka, &E.Kb, &E.F, &E.Kx, &E.bkH32}) SWE_CUDA_TRY(cudaMalloc(p, s32));
     for (double** p : {&E.Hh, &E.Dh, &E.bkHh}) SWE_CUDA_TRY(cudaMalloc(p, s64));
     SWE_CUDA_TRY(cudaMalloc(&E.io, (size_t)n * members * 4 * sizeof(double)));
@@ -371,48 +451,15 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     SWE_CUDA_TRY(cudaMemset(E.err, 0, sizeof(int)));
     for (float* p : {E.H32, E.D32, E.Ka, E.Kb, E.F, E.Kx}) SWE_CUDA_TRY(cudaMemset(p, 0, s32));
     for (double* p : {E.Hh, E.Dh}) SWE_CUDA_TRY(cudaMemset(p, 0, s64));
-    SWE_CUDA_TRY(cudaMemcpy(E.perm, E.perm_h.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    SWE_CUDA_TRY(cudaMemcpy(E.W, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
-    SWE_CUDA_TRY(cudaMemcpy(E.PT, pt.data(), pt.size() * sizeof(float), cudaMemcpyHostToDevice));
-    // tile tables for the two tile sizes
-    {
-        std::vector<int> rows, kcount;
-        std::vector<uint8_t> local;
-        for (int ti = 0; ti < 2; ++ti) {
-            Tables& tb = E.tab[ti];
-            tb.ok = ti == 0 ? build_tiles<4>(n, nnbr, ridx, rows, kcount, local, tb.ntiles, tb.kmax_seen)
-                            : build_tiles<8>(n, nnbr, ridx, rows, kcount, local, tb.ntiles, tb.kmax_seen);
-            if (!tb.ok) continue;
-            SWE_CUDA_TRY(cudaMalloc(&tb.rows, rows.size() * sizeof(int)));
-            SWE_CUDA_TRY(cudaMalloc(&tb.kcount, kcount.size() * sizeof(int)));
-            SWE_CUDA_TRY(cudaMalloc(&tb.local, local.size()));
-            SWE_CUDA_TRY(cudaMemcpy(tb.rows, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice));
-            SWE_CUDA_TRY(cudaMemcpy(tb.kcount, kcount.data(), kcount.size() * sizeof(int), cudaMemcpyHostToDevice));
-            SWE_CUDA_TRY(cudaMemcpy(tb.local, local.data(), local.size(), cudaMemcpyHostToDevice));
-        }
-    }
-    if (!E.tab[0].ok && !E.tab[1].ok) {
-        const int k4 = E.tab[0].kmax_seen, k8 = E.tab[1].kmax_seen;
-        E.release();
-        set_error("swe_ens_init: a tile's neighbour set exceeds the kernel limit (T=4: %d rows > %d; T=8: %d > %d)",
-                  k4, EnsTile<4>::kKmax, k8, EnsTile<8>::kKmax);
-        return SWE_ERR_ARG;
-    }
-    {
-        const int Ts[4] = {4, 4, 8, 8}, hpcs[4] = {1, 2, 1, 2};
-        for (int vi = 0; vi < 4; ++vi) {
-            E.var[vi].T = Ts[vi];
-            E.var[vi].hpc = hpcs[vi];
-            E.var[vi].usable = E.tab[Ts[vi] == 8].ok && hpcs[vi] <= E.halves;
-        }
-    }
-    SWE_TRY((Ensemble::set_attrs<4, 1>()));
-    SWE_TRY((Ensemble::set_attrs<4, 2>()));
-    SWE_TRY((Ensemble::set_attrs<8, 1>()));
-    SWE_TRY((Ensemble::set_attrs<8, 2>()));
+    E.var[0].mpc = 32;
+    E.var[0].usable = true;
+    E.var[1].mpc = 64;
+    E.var[1].usable = members % 64 == 0;
+    SWE_TRY(Ensemble::set_attrs<32>());
+    SWE_TRY(Ensemble::set_attrs<64>());
     E.ready = true;
-    // default choice until tuned: T = 4, one half per CTA
-    E.chosen = E.var[0].usable ? 0 : 2;
+    // default choice until tuned: all members in one CTA
+    E.chosen = E.var[1].usable ? 1 : 0;
     return E.build_graph();
 }
 
@@ -484,36 +531,43 @@ int swe_ens_stage(int substep_id) {
 int swe_ens_tune(double* ms_per_step) {
     SWE_TRY(ens_ready());
     SWE_TRY(tune(g_ens));
-    if (ms_per_step)
-        for (int vi = 0; vi < 4; ++vi) ms_per_step[vi] = g_ens.tune_ms[vi];
+    if (ms_per_step) {
+        ms_per_step[0] = g_ens.tune_ms[0];
+        ms_per_step[1] = g_ens.tune_ms[1];
+        ms_per_step[2] = ms_per_step[3] = -1.0;
+    }
     return SWE_OK;
 }
 
 int swe_ens_use_variant(int tile_nodes, int members_per_cta) {
     SWE_TRY(ens_ready());
-    for (int vi = 0; vi < 4; ++vi) {
+    if (tile_nodes != kEnsTileNodes) {
+        set_error("swe_ens_use_variant: tiles have %d nodes, got %d", kEnsTileNodes, tile_nodes);
+        return SWE_ERR_ARG;
+    }
+    for (int vi = 0; vi < 2; ++vi) {
         const Variant& v = g_ens.var[vi];
-        if (v.T == tile_nodes && 32 * v.hpc == members_per_cta) {
+        if (v.mpc == members_per_cta) {
             if (!v.usable) {
-                set_error("swe_ens_use_variant: (%d, %d) not usable for this grid / member count", tile_nodes, members_per_cta);
+                set_error("swe_ens_use_variant: %d members per CTA does not divide %d members", members_per_cta,
+                          g_ens.members);
                 return SWE_ERR_ARG;
             }
             g_ens.chosen = vi;
             return g_ens.build_graph();
         }
     }
-    set_error("swe_ens_use_variant: no variant (%d nodes, %d members per CTA)", tile_nodes, members_per_cta);
+    set_error("swe_ens_use_variant: members per CTA must be 32 or 64, got %d", members_per_cta);
     return SWE_ERR_ARG;
 }
 
 int swe_ens_config(int* out) {
     SWE_TRY(ens_ready());
     if (!out) { set_error("swe_ens_config: null out"); return SWE_ERR_ARG; }
-    const Variant& v = g_ens.var[g_ens.chosen];
-    out[0] = v.T;
-    out[1] = 32 * v.hpc;
-    out[2] = g_ens.tab[0].kmax_seen;
-    out[3] = g_ens.tab[1].kmax_seen;
+    out[0] = kEnsTileNodes;
+    out[1] = g_ens.var[g_ens.chosen].mpc;
+    out[2] = g_ens.max_rows;
+    out[3] = g_ens.ntiles;
     return SWE_OK;
 }
 

@@ -278,7 +278,7 @@ class Ensemble:
         out = np.zeros(4, dtype=np.int32)
         check("swe_ens_config", self.lib.swe_ens_config(_p(out)))
         return {"tile_nodes": int(out[0]), "members_per_cta": int(out[1]),
-                "max_rows_tile4": int(out[2]), "max_rows_tile8": int(out[3])}
+                "max_rows_per_tile": int(out[2]), "tiles": int(out[3])}
 
     def invariants(self) -> np.ndarray:
         out = np.zeros((self.members, 2))

@@ -20,7 +20,7 @@ from swe_b200 import capi, gen, swe_input
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [(4, 32), (4, 64), (8, 32), (8, 64)]
+VARIANTS = [(32, 32), (32, 64)]
 
 
 @pytest.fixture(scope="module")
@@ -75,12 +75,12 @@ def test_members_are_independent(ens, model_l4):
     m = model_l4
     H64 = _members(m, 64)
     ens.init(m, 64)
-    ens.use_variant(4, 32)
+    ens.use_variant(32, 32)
     ens.set_state(H64)
     ens.step(5)
     a = ens.get_state()
     ens.init(m, 32)
-    ens.use_variant(4, 32)
+    ens.use_variant(32, 32)
     ens.set_state(H64[32:])
     ens.step(5)
     b = ens.get_state()
