@@ -3,9 +3,9 @@
 // B members (32 or 64) share one grid.  The library orders nodes along a
 // Hilbert curve on the six faces of the cube around the sphere, so that 32
 // consecutive nodes form a compact patch, and builds per-tile tables once:
-// the tile's unique neighbour rows (ascending, padded to 16-row chunks), its
-// stencil weights as entries sorted by chunk, the node that centres it, and
-// the operators' row sums.  All member states stay device-resident; each RK4
+// the tile's unique neighbour rows (ascending, padded to 16-row chunks), the
+// stencil slot (if any) of every (tile node, chunk row) pair, the node that
+// centres it, and the operators' row sums.  All member states stay device-resident; each RK4
 // stage is one persistent tcgen05 kernel (ensemble_kernel.cuh).  An autotuner
 // times each members-per-CTA variant on the live state and keeps the fastest;
 // whole steps replay a captured CUDA graph.
@@ -73,19 +73,17 @@ std::vector<int> curve_order(int n, const double* x, const double* y, const doub
 // Per-tile tables (node indices in the curve order).
 struct TileTables {
     int ntiles = 0, nchunks = 0, max_rows = 0;
-    std::vector<int> row_off, rows, ent_off, ent_tk, centre;
-    std::vector<float> ent_w;   // 4 per entry
+    std::vector<int> row_off, rows, centre;
+    std::vector<uint32_t> jmap;   // [chunk][row group][node t] 4 stencil slots (255 = none)
 };
 
-TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std::vector<float>& w4,
-                       const std::vector<double>& X) {
+TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std::vector<double>& X) {
     TileTables tb;
     tb.ntiles = (n + kEnsTileNodes - 1) / kEnsTileNodes;
     tb.row_off.assign(tb.ntiles + 1, 0);
     tb.centre.assign(tb.ntiles, 0);
-    tb.ent_off.push_back(0);
     std::vector<int> u;
-    std::vector<std::vector<int>> bucket;
+    std::vector<uint8_t> slot;   // [t][k] stencil slot of row k in node t's stencil
     for (int tile = 0; tile < tb.ntiles; ++tile) {
         const int n0 = tile * kEnsTileNodes, n1 = std::min(n, n0 + kEnsTileNodes);
         u.clear();
@@ -95,24 +93,22 @@ TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std:
         u.erase(std::unique(u.begin(), u.end()), u.end());
         tb.max_rows = std::max(tb.max_rows, (int)u.size());
         const int nch = ((int)u.size() + kEnsKc - 1) / kEnsKc;
-        for (int k = 0; k < nch * kEnsKc; ++k) tb.rows.push_back(k < (int)u.size() ? u[k] : -1);
+        const int kpad = nch * kEnsKc;
+        for (int k = 0; k < kpad; ++k) tb.rows.push_back(k < (int)u.size() ? u[k] : -1);
         tb.row_off[tile + 1] = (int)tb.rows.size();
-        // weight entries, grouped by chunk
-        bucket.assign(nch, {});
+        slot.assign((size_t)kEnsTileNodes * kpad, 0xff);
         for (int i = n0; i < n1; ++i)
             for (int j = 0; j < nnbr; ++j) {
                 const int k = (int)(std::lower_bound(u.begin(), u.end(), ridx[(size_t)i * nnbr + j]) - u.begin());
-                bucket[k / kEnsKc].push_back(((i - n0) | ((k % kEnsKc) << 8)) | (j << 16));
+                slot[(size_t)(i - n0) * kpad + k] = (uint8_t)j;
             }
-        for (int c = 0; c < nch; ++c) {
-            for (int e : bucket[c]) {
-                const int t = e & 0xff, j = e >> 16;
-                tb.ent_tk.push_back(e & 0xffff);
-                const float* w = &w4[((size_t)(n0 + t) * nnbr + j) * 4];
-                tb.ent_w.insert(tb.ent_w.end(), w, w + 4);
-            }
-            tb.ent_off.push_back((int)tb.ent_tk.size());
-        }
+        for (int c = 0; c < nch; ++c)
+            for (int g = 0; g < 4; ++g)
+                for (int t = 0; t < kEnsTileNodes; ++t) {
+                    uint32_t v = 0;
+                    for (int i = 0; i < 4; ++i) v |= (uint32_t)slot[(size_t)t * kpad + c * kEnsKc + 4 * g + i] << (8 * i);
+                    tb.jmap.push_back(v);
+                }
         // centre: the tile node nearest the tile's centroid
         double cx = 0, cy = 0, cz = 0;
         for (int i = n0; i < n1; ++i) { cx += X[3 * i]; cy += X[3 * i + 1]; cz += X[3 * i + 2]; }
@@ -197,8 +193,9 @@ struct Ensemble {
     int* err = nullptr;
     // tile tables
     int ntiles = 0, max_rows = 0;
-    int *row_off = nullptr, *rows = nullptr, *ent_off = nullptr, *ent_tk = nullptr, *centre = nullptr;
-    float4* ent_w = nullptr;
+    int *row_off = nullptr, *rows = nullptr, *centre = nullptr;
+    uint32_t* jmap = nullptr;
+    float4* W = nullptr;
     Variant var[2];       // members per CTA: 32, 64
     int chosen = -1;
     cudaStream_t stream = nullptr;
@@ -212,12 +209,13 @@ struct Ensemble {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
         void* ps[] = {perm, PT, RS, H32, D32, Ka, Kb, F, Kx, Hh, Dh, io, inv, bkH32, bkHh, err,
-                      row_off, rows, ent_off, ent_tk, centre, ent_w};
+                      row_off, rows, centre, jmap, W};
         for (void* p : ps) if (p) cudaFree(p);
         perm = nullptr; PT = nullptr; RS = nullptr; H32 = D32 = Ka = Kb = F = Kx = nullptr;
         Hh = Dh = io = inv = nullptr; bkH32 = nullptr; bkHh = nullptr; err = nullptr;
-        row_off = rows = ent_off = ent_tk = centre = nullptr;
-        ent_w = nullptr;
+        row_off = rows = centre = nullptr;
+        jmap = nullptr;
+        W = nullptr;
         for (auto& v : var) v = Variant{};
         for (auto& e : ev) { if (e) cudaEventDestroy(e); e = nullptr; }
         if (stream) cudaStreamDestroy(stream);
@@ -234,7 +232,7 @@ struct Ensemble {
         a.members = members;
         a.units = ntiles * (members / mpc);
         a.mf = mf;
-        a.row_off = row_off; a.rows = rows; a.ent_off = ent_off; a.ent_tk = ent_tk; a.ent_w = ent_w;
+        a.row_off = row_off; a.rows = rows; a.jmap = jmap; a.W = W;
         a.centre = centre;
         a.PT = PT;
         a.RS = RS;
@@ -402,13 +400,13 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     for (long i = 0; i < n; ++i)
         for (int j = 0; j < nnbr; ++j) ridx[i * nnbr + j] = inv[idx[(long)E.perm_h[i] * nnbr + j]];
     // static data in FP32, curve order; operator row sums in FP64 of the FP32 weights
-    std::vector<float> w((size_t)n * nnbr * 4), pt((size_t)n * kPointStride, 0.f), rs((size_t)n * 4);
+    std::vector<float> w((size_t)n * 32 * 4, 0.f), pt((size_t)n * kPointStride, 0.f), rs((size_t)n * 4);
     std::vector<double> X((size_t)n * 3);
     for (long i = 0; i < n; ++i) {
         const long o = E.perm_h[i];
         double sum[4] = {0, 0, 0, 0};
         for (int j = 0; j < nnbr; ++j) {
-            float* q = &w[((size_t)i * nnbr + j) * 4];
+            float* q = &w[((size_t)i * 32 + j) * 4];
             q[0] = (float)Dx[o * nnbr + j]; q[1] = (float)Dy[o * nnbr + j];
             q[2] = (float)Dz[o * nnbr + j]; q[3] = (float)L[o * nnbr + j];
             for (int op = 0; op < 4; ++op) sum[op] += (double)q[op];
@@ -423,7 +421,7 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
         }
         X[3 * i] = x[o]; X[3 * i + 1] = y[o]; X[3 * i + 2] = z[o];
     }
-    const TileTables tb = build_tiles(n, nnbr, ridx, w, X);
+    const TileTables tb = build_tiles(n, nnbr, ridx, X);
     E.ntiles = tb.ntiles;
     E.max_rows = tb.max_rows;
     SWE_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
@@ -439,10 +437,9 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     SWE_TRY(upload(reinterpret_cast<float**>(&E.RS), rs));
     SWE_TRY(upload(&E.row_off, tb.row_off));
     SWE_TRY(upload(&E.rows, tb.rows));
-    SWE_TRY(upload(&E.ent_off, tb.ent_off));
-    SWE_TRY(upload(&E.ent_tk, tb.ent_tk));
+    SWE_TRY(upload(&E.jmap, tb.jmap));
     SWE_TRY(upload(&E.centre, tb.centre));
-    SWE_TRY(upload(reinterpret_cast<float**>(&E.ent_w), tb.ent_w));
+    SWE_TRY(upload(reinterpret_cast<float**>(&E.W), w));
     for (float** p : {&E.H32, &E.D32, &E.Ka, &E.Kb, &E.F, &E.Kx, &E.bkH32}) SWE_CUDA_TRY(cudaMalloc(p, s32));
     for (double** p : {&E.Hh, &E.Dh, &E.bkHh}) SWE_CUDA_TRY(cudaMalloc(p, s64));
     SWE_CUDA_TRY(cudaMalloc(&E.io, (size_t)n * members * 4 * sizeof(double)));

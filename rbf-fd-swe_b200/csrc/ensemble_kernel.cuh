@@ -26,10 +26,11 @@
 //
 // Persistent, warp-specialised CTA (one per SM; it owns all of tensor memory):
 //   * converter warps (MPC/8): for each 16-row chunk of K they gather the rows
-//     (16-byte loads, one chunk ahead), centre and split them into the B
-//     operand, and build the matching A chunk from the tile's weight entries
-//     sorted by chunk (zero, then scatter hi/lo); a ring of kEnsStages slots
-//     hands chunks to
+//     (16-byte loads issued one chunk ahead into a ping-pong register set),
+//     centre and split them into the B operand, and write the matching A chunk
+//     densely, one 16-byte core row (4 chunk rows of one operator and node) per
+//     store, from a map of chunk rows to stencil slots; a ring of kEnsStages
+//     slots hands chunks to
 //   * the MMA warp: one thread issues 2 k-steps x 3 MMAs (128 x N x 8) per
 //     chunk into one of two TMEM accumulators and commits each chunk to the
 //     slot's "empty" barrier and each tile to the accumulator's "full" barrier;
@@ -52,7 +53,6 @@ constexpr int kEnsTileNodes = 32;   // nodes per tile (M = 4 * 32)
 constexpr int kEnsKc = 16;          // neighbour rows per pipeline chunk
 constexpr int kEnsStages = 3;       // ring slots
 constexpr int kEnsEpiWarps = 8;
-constexpr int kEnsMaxEntPerChunk = kEnsKc * kEnsTileNodes;   // every (row, node) pair once
 constexpr uint32_t kEnsWaitTries = 1u << 22;
 
 template <int MPC>
@@ -63,7 +63,7 @@ struct EnsCfg {
     static constexpr int kMmaWarp = kConvWarps;
     static constexpr int kEpiWarp0 = kConvWarps + 1;
     static constexpr int kThreads = 32 * (kConvWarps + 1 + kEnsEpiWarps);
-    static constexpr int kEntPerThread = kEnsMaxEntPerChunk / kConvThreads;
+    static constexpr int kOpp = 256 / kConvThreads;          // operator pairs per converter (A build)
     static constexpr int kSboA = (kEnsKc / 4) * 128;       // A: 8-row groups of 16-byte core rows
     static constexpr int kSboB = (kEnsKc / 4) * 128 + 16;  // B: odd 16-byte stride, conflict-free stores
     static constexpr int kAHalf = (128 / 8) * kSboA;       // one of hi / lo
@@ -73,7 +73,7 @@ struct EnsCfg {
     static constexpr int kXchGroupFloats = 4 * kEnsTileNodes * kXchStride;
     static constexpr int kSmem = kEnsStages * kStageBytes + 2 * kXchGroupFloats * 4;
     static constexpr int kTmemCols = (2 * kN <= 256) ? 256 : 512;
-    static_assert(kEnsMaxEntPerChunk % kConvThreads == 0, "entries per thread");
+    static_assert(kOpp == 1 || kOpp == 2, "A build covers 32 nodes x 4 row groups x 2 operator pairs");
     static_assert(kN % 64 == 0 || kN == 32, "epilogue column chunks");
 };
 
@@ -85,9 +85,8 @@ struct EnsArgs {
     int mf;                // 4 * members (row length of the state arrays)
     const int* row_off;    // [ntiles + 1] offsets into rows, multiples of kEnsKc
     const int* rows;       // unique neighbour rows of each tile, ascending; -1 pads
-    const int* ent_off;    // [rows / kEnsKc + 1] weight entries of each chunk
-    const int* ent_tk;     // entry: node t | (row within chunk) << 8
-    const float4* ent_w;   // entry: (Dx, Dy, Dz, L) weight
+    const uint32_t* jmap;  // [chunk][row group][node t]: stencil slot of each of the 4 rows, 255 = none
+    const float4* W;       // [n][32] (Dx, Dy, Dz, L) per stencil slot
     const int* centre;     // [ntiles] node whose state centres the tile
     const float4* PT;      // [n][5] pointwise record (20 floats)
     const float4* RS;      // [n] row sums of the four operators
@@ -136,36 +135,59 @@ __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, volatile int*
     return false;
 }
 
-// Position of a converter in its CTA's sequence of (work unit, chunk) steps.
-struct Pos {
+// Position of a converter in its CTA's sequence of (work unit, chunk) steps;
+// the chunk range of the following unit is fetched one unit ahead.
+struct Cursor {
     int u, gc, gc_end;     // unit, global chunk id, end of the unit's chunks
+    int nx_gc, nx_end;     // chunk range of unit u + gridDim.x
     bool valid;
 };
 
-__device__ __forceinline__ Pos first_pos(const EnsArgs& a, int halves) {
-    Pos p;
+__device__ __forceinline__ void unit_range(const EnsArgs& a, int u, int halves, int& g0, int& g1) {
+    if (u < a.units) {
+        const int tile = u / halves;
+        g0 = __ldg(a.row_off + tile) / kEnsKc;
+        g1 = __ldg(a.row_off + tile + 1) / kEnsKc;
+    } else {
+        g0 = g1 = 0;
+    }
+}
+
+__device__ __forceinline__ Cursor first_cursor(const EnsArgs& a, int halves) {
+    Cursor p;
     p.u = blockIdx.x;
     p.valid = p.u < a.units;
-    if (p.valid) {
-        const int tile = p.u / halves;
-        p.gc = __ldg(a.row_off + tile) / kEnsKc;
-        p.gc_end = __ldg(a.row_off + tile + 1) / kEnsKc;
-    }
+    unit_range(a, p.u, halves, p.gc, p.gc_end);
+    unit_range(a, p.u + gridDim.x, halves, p.nx_gc, p.nx_end);
     return p;
 }
 
-__device__ __forceinline__ Pos next_pos(Pos p, const EnsArgs& a, int halves) {
+__device__ __forceinline__ Cursor next_cursor(Cursor p, const EnsArgs& a, int halves) {
     if (!p.valid) return p;
     if (++p.gc < p.gc_end) return p;
     p.u += gridDim.x;
     p.valid = p.u < a.units;
-    if (p.valid) {
-        const int tile = p.u / halves;
-        p.gc = __ldg(a.row_off + tile) / kEnsKc;
-        p.gc_end = __ldg(a.row_off + tile + 1) / kEnsKc;
-    }
+    p.gc = p.nx_gc;
+    p.gc_end = p.nx_end;
+    unit_range(a, p.u + gridDim.x, halves, p.nx_gc, p.nx_end);
     return p;
 }
+
+// Indices of one step (row ids for the B operand, stencil slots for the A operand).
+struct Fetch {
+    int4 idx = make_int4(-1, -1, -1, -1);
+    uint32_t jj = 0xffffffffu;
+    int u = -1;
+};
+
+// Operands of one step held in registers.
+template <int OPP>
+struct ConvSet {
+    float4 x[4];           // 4 gathered rows x 4 member-fields
+    float4 cen;            // centre state of the same member-fields
+    int live;              // bit i: row i is a real row
+    float2 w[OPP][4];      // weights of the operator pairs for the 4 chunk rows
+};
 
 }  // namespace ens
 
@@ -206,113 +228,86 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
     if (warp < C::kConvWarps) {
         // =============================== converters ===============================
         const int ct = threadIdx.x;              // 0 .. 4*MPC-1
-        const int quad = ct % MPC;               // member within the CTA's block
-        const int kg = ct / MPC;                 // rows 4kg .. 4kg+3 of each chunk
-        ens::Pos p0 = ens::first_pos(a, halves);
-        ens::Pos p1 = ens::next_pos(p0, a, halves);
-        // stage "x" (current): rows loaded; stage "i" (next): row indices loaded
-        int4 idx0 = make_int4(-1, -1, -1, -1), idx1 = make_int4(-1, -1, -1, -1);
-        int e00 = 0, e01 = 0, e10 = 0, e11 = 0;
-        if (p0.valid) {
-            idx0 = __ldg(reinterpret_cast<const int4*>(a.rows + p0.gc * kEnsKc + 4 * kg));
-            e00 = __ldg(a.ent_off + p0.gc);
-            e01 = __ldg(a.ent_off + p0.gc + 1);
-        }
-        if (p1.valid) {
-            idx1 = __ldg(reinterpret_cast<const int4*>(a.rows + p1.gc * kEnsKc + 4 * kg));
-            e10 = __ldg(a.ent_off + p1.gc);
-            e11 = __ldg(a.ent_off + p1.gc + 1);
-        }
-        auto load_rows = [&](const ens::Pos& p, const int4& id, float4 (&x)[4]) {
-            const long col = (long)(p.u % halves) * C::kN + 4 * quad;
-            const int r[4] = {id.x, id.y, id.z, id.w};
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                x[i] = r[i] >= 0 ? ens::ldg_f4(a.Kin + (long)r[i] * a.mf + col) : make_float4(0.f, 0.f, 0.f, 0.f);
+        // B operand: rows 4kg..4kg+3 of each chunk x member-fields 4quad..4quad+3
+        const int quad = ct % MPC;
+        const int kg = ct / MPC;
+        // A operand: node t, rows 4akg..4akg+3 of each chunk, operator pairs opp0 .. opp0+kOpp-1
+        const int at = ct & 31;
+        const int akg = (ct >> 5) & 3;
+        const int opp0 = (ct >> 7) * C::kOpp;
+        ens::Cursor cur = ens::first_cursor(a, halves);
+        ens::Fetch fx;                 // indices of the step after the current one
+        ens::ConvSet<C::kOpp> sa, sb;  // operands of the current / next step (ping-pong)
+        auto fetch_idx = [&](const ens::Cursor& p, ens::Fetch& f) {
+            if (!p.valid) return;
+            f.idx = __ldg(reinterpret_cast<const int4*>(a.rows + p.gc * kEnsKc + 4 * kg));
+            f.jj = __ldg(a.jmap + (p.gc * 4 + akg) * 32 + at);
+            f.u = p.u;
         };
-        auto load_ent = [&](int e0, int e1, int (&tk)[C::kEntPerThread], float4 (&w)[C::kEntPerThread]) {
-#pragma unroll
-            for (int q = 0; q < C::kEntPerThread; ++q) {
-                const int e = e0 + ct + q * C::kConvThreads;
-                tk[q] = e < e1 ? __ldg(a.ent_tk + e) : -1;
-                w[q] = e < e1 ? __ldg(a.ent_w + e) : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-        };
-        auto load_centre = [&](const ens::Pos& p) {
+        auto fetch_ops = [&](const ens::Cursor& p, const ens::Fetch& f, ens::ConvSet<C::kOpp>& o, const float4& cen_prev,
+                             int u_prev) {
+            if (!p.valid) return;
             const int tile = p.u / halves;
             const long col = (long)(p.u % halves) * C::kN + 4 * quad;
-            return ens::ldg_f4(a.Kin + (long)__ldg(a.centre + tile) * a.mf + col);
+            const int r[4] = {f.idx.x, f.idx.y, f.idx.z, f.idx.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                o.x[i] = r[i] >= 0 ? ens::ldg_f4(a.Kin + (long)r[i] * a.mf + col) : make_float4(0.f, 0.f, 0.f, 0.f);
+            o.live = (r[0] >= 0 ? 1 : 0) | (r[1] >= 0 ? 2 : 0) | (r[2] >= 0 ? 4 : 0) | (r[3] >= 0 ? 8 : 0);
+            o.cen = (p.u != u_prev) ? ens::ldg_f4(a.Kin + (long)__ldg(a.centre + tile) * a.mf + col) : cen_prev;
+            const long node = (long)tile * kEnsTileNodes + at;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const uint32_t j = (f.jj >> (8 * i)) & 0xffu;
+#pragma unroll
+                for (int q = 0; q < C::kOpp; ++q)
+                    o.w[q][i] = j != 0xffu ? __ldg(reinterpret_cast<const float2*>(a.W + node * 32 + j) + opp0 + q)
+                                           : make_float2(0.f, 0.f);
+            }
         };
-        float4 x0[4], x1[4];
-        int tk0[C::kEntPerThread], tk1[C::kEntPerThread];
-        float4 w0[C::kEntPerThread], w1[C::kEntPerThread];
-        float4 cen0 = make_float4(0.f, 0.f, 0.f, 0.f), cen1 = cen0;
-        if (p0.valid) {
-            load_rows(p0, idx0, x0);
-            load_ent(e00, e01, tk0, w0);
-            cen0 = load_centre(p0);
-        }
         int g = 0;
-        while (p0.valid) {
-            // look ahead: rows and entries of p1, indices of p2
-            ens::Pos p2 = ens::next_pos(p1, a, halves);
-            int4 idx2 = make_int4(-1, -1, -1, -1);
-            int e20 = 0, e21 = 0;
-            if (p1.valid) {
-                load_rows(p1, idx1, x1);
-                load_ent(e10, e11, tk1, w1);
-                cen1 = (p1.u != p0.u) ? load_centre(p1) : cen0;
-            }
-            if (p2.valid) {
-                idx2 = __ldg(reinterpret_cast<const int4*>(a.rows + p2.gc * kEnsKc + 4 * kg));
-                e20 = __ldg(a.ent_off + p2.gc);
-                e21 = __ldg(a.ent_off + p2.gc + 1);
-            }
-            // ---- fill ring slot s with chunk p0 ----
+        auto step = [&](ens::ConvSet<C::kOpp>& o, ens::ConvSet<C::kOpp>& nx, int u_cur) -> bool {
+            // look ahead: operands of the next step, indices of the one after
+            ens::Cursor nxt = ens::next_cursor(cur, a, halves);
+            fetch_ops(nxt, fx, nx, o.cen, u_cur);
+            ens::Cursor nxt2 = ens::next_cursor(nxt, a, halves);
+            fetch_idx(nxt2, fx);
             const int s = g % kEnsStages;
-            const bool got = ens::wait(&empty_bar[s], ((g / kEnsStages) & 1) ^ 1, abort_v, a.err, 3);
+            if (!ens::wait(&empty_bar[s], ((g / kEnsStages) & 1) ^ 1, abort_v, a.err, 3)) return false;
             unsigned char* slot = smem + s * C::kStageBytes;
             unsigned char* A_hi = slot;
             unsigned char* A_lo = slot + C::kAHalf;
             unsigned char* B_hi = slot + 2 * C::kAHalf;
             unsigned char* B_lo = B_hi + C::kBHalf;
-            if (got) {
-                uint4* z = reinterpret_cast<uint4*>(A_hi);
-                for (int q = ct; q < 2 * C::kAHalf / 16; q += C::kConvThreads) z[q] = make_uint4(0, 0, 0, 0);
-            }
-            // zeroing done by every converter before any scatter; one verdict for all of them
-            if (!ens::named_and(1, C::kConvThreads, got && !*abort_v)) break;
+            // A: one 16-byte core row (4 chunk rows) of (operator, node) per operator handled
 #pragma unroll
-            for (int q = 0; q < C::kEntPerThread; ++q) {
-                if (tk0[q] < 0) continue;
-                const int t = tk0[q] & 0xff, kk = tk0[q] >> 8;
-                const float w[4] = {w0[q].x, w0[q].y, w0[q].z, w0[q].w};
+            for (int q = 0; q < C::kOpp; ++q)
 #pragma unroll
-                for (int op = 0; op < 4; ++op) {
-                    const int r = 32 * op + t;
-                    const uint32_t off = (r >> 3) * C::kSboA + (kk >> 2) * 128 + (r & 7) * 16 + (kk & 3) * 4;
-                    float hi, lo;
-                    tc::tf32_split(w[op], hi, lo);
-                    *reinterpret_cast<float*>(A_hi + off) = hi;
-                    *reinterpret_cast<float*>(A_lo + off) = lo;
+                for (int h = 0; h < 2; ++h) {
+                    const int r = 32 * (2 * (opp0 + q) + h) + at;
+                    float4 hi, lo;
+                    tc::tf32_split(h ? o.w[q][0].y : o.w[q][0].x, hi.x, lo.x);
+                    tc::tf32_split(h ? o.w[q][1].y : o.w[q][1].x, hi.y, lo.y);
+                    tc::tf32_split(h ? o.w[q][2].y : o.w[q][2].x, hi.z, lo.z);
+                    tc::tf32_split(h ? o.w[q][3].y : o.w[q][3].x, hi.w, lo.w);
+                    const uint32_t off = (r >> 3) * C::kSboA + akg * 128 + (r & 7) * 16;
+                    *reinterpret_cast<float4*>(A_hi + off) = hi;
+                    *reinterpret_cast<float4*>(A_lo + off) = lo;
                 }
-            }
+            // B: 4 rows x 4 member-fields; each member-field's 4 rows are one 16-byte core row
             {
-                // B: 4 rows x 4 member-fields; each member-field's 4 rows are one 16-byte core row
-                const float xv[4][4] = {{x0[0].x, x0[0].y, x0[0].z, x0[0].w},
-                                        {x0[1].x, x0[1].y, x0[1].z, x0[1].w},
-                                        {x0[2].x, x0[2].y, x0[2].z, x0[2].w},
-                                        {x0[3].x, x0[3].y, x0[3].z, x0[3].w}};
-                const int4 idr = idx0;
-                const bool live[4] = {idr.x >= 0, idr.y >= 0, idr.z >= 0, idr.w >= 0};
-                const float cv[4] = {cen0.x, cen0.y, cen0.z, cen0.w};
+                const float xv[4][4] = {{o.x[0].x, o.x[0].y, o.x[0].z, o.x[0].w},
+                                        {o.x[1].x, o.x[1].y, o.x[1].z, o.x[1].w},
+                                        {o.x[2].x, o.x[2].y, o.x[2].z, o.x[2].w},
+                                        {o.x[3].x, o.x[3].y, o.x[3].z, o.x[3].w}};
+                const float cv[4] = {o.cen.x, o.cen.y, o.cen.z, o.cen.w};
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int nrow = 4 * quad + j;
                     float4 hi, lo;
                     float y[4];
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) y[i] = live[i] ? xv[i][j] - cv[j] : 0.f;
+                    for (int i = 0; i < 4; ++i) y[i] = ((o.live >> i) & 1) ? xv[i][j] - cv[j] : 0.f;
                     tc::tf32_split(y[0], hi.x, lo.x);
                     tc::tf32_split(y[1], hi.y, lo.y);
                     tc::tf32_split(y[2], hi.z, lo.z);
@@ -326,15 +321,22 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&full_bar[s]);
             ++g;
-            // rotate
-            p0 = p1; p1 = p2;
-            idx0 = idx1; idx1 = idx2;
-            e10 = e20; e11 = e21;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) x0[i] = x1[i];
-#pragma unroll
-            for (int q = 0; q < C::kEntPerThread; ++q) { tk0[q] = tk1[q]; w0[q] = w1[q]; }
-            cen0 = cen1;
+            cur = nxt;
+            return true;
+        };
+        if (cur.valid) {
+            ens::Fetch f0;
+            fetch_idx(cur, f0);
+            fetch_ops(cur, f0, sa, sa.cen, -1);
+            fetch_idx(ens::next_cursor(cur, a, halves), fx);
+        }
+        // two steps per trip so that the ping-pong sets never need copying
+        while (cur.valid) {
+            int u = cur.u;
+            if (!step(sa, sb, u)) break;
+            if (!cur.valid) break;
+            u = cur.u;
+            if (!step(sb, sa, u)) break;
         }
     } else if (warp == C::kMmaWarp) {
         // =============================== MMA issuer ===============================
