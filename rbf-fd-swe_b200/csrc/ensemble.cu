@@ -422,6 +422,7 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
         X[3 * i] = x[o]; X[3 * i + 1] = y[o]; X[3 * i + 2] = z[o];
     }
     const TileTables tb = build_tiles(n, nnbr, ridx, X);
+
     E.ntiles = tb.ntiles;
     E.max_rows = tb.max_rows;
     SWE_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));

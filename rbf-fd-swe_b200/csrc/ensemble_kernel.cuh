@@ -38,8 +38,8 @@
 //     32 columns at a time, transpose (op, node) rows to (node, member) sets
 //     through shared memory, add the centre back, evaluate the pointwise part
 //     of eval_RHS_swe (rk4_rbffd_swe.c:320-353) and apply the RK_substep
-//     combine (:30-72) for one (node, member) per thread, while the MMA warp
-//     already fills the other accumulator.
+//     combine (:30-72) for one (node, member) per thread, while the tensor
+//     cores already fill the other accumulator.
 // Every mbarrier wait is bounded; a timeout sets an error word and a shared
 // abort flag that makes every role leave its loop.
 #pragma once
@@ -71,7 +71,10 @@ struct EnsCfg {
     static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
     static constexpr int kXchStride = 36;                  // floats per (op, node) row; 9 x 16 B
     static constexpr int kXchGroupFloats = 4 * kEnsTileNodes * kXchStride;
-    static constexpr int kSmem = kEnsStages * kStageBytes + 2 * kXchGroupFloats * 4;
+    static constexpr int kTbRs = kEnsTileNodes * kPointStride * 4;   // per-tile buffer: PT, row sums, centre
+    static constexpr int kTbCen = kTbRs + kEnsTileNodes * 16;
+    static constexpr int kTileBuf = (kTbCen + kN * 4 + 127) / 128 * 128;
+    static constexpr int kSmem = kEnsStages * kStageBytes + 2 * kXchGroupFloats * 4 + 2 * kTileBuf;
     static constexpr int kTmemCols = (2 * kN <= 256) ? 256 : 512;
     static_assert(kOpp == 1 || kOpp == 2, "A build covers 32 nodes x 4 row groups x 2 operator pairs");
     static_assert(kN % 64 == 0 || kN == 32, "epilogue column chunks");
@@ -119,9 +122,7 @@ __device__ __forceinline__ bool named_and(int id, int nthreads, bool v) {
         : "memory");
     return r != 0;
 }
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(b)) : "memory");
-}
+using tc::mbar_arrive;
 __device__ __forceinline__ float4 ldg_f4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
 // Bounded wait that also gives up as soon as another role has aborted.
@@ -138,7 +139,8 @@ __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, volatile int*
 // Position of a converter in its CTA's sequence of (work unit, chunk) steps;
 // the chunk range of the following unit is fetched one unit ahead.
 struct Cursor {
-    int u, gc, gc_end;     // unit, global chunk id, end of the unit's chunks
+    int u, ti;               // unit, and its position in this CTA's sequence of units
+    int gc, gc0, gc_end;     // global chunk id, first and end chunk of the unit
     int nx_gc, nx_end;     // chunk range of unit u + gridDim.x
     bool valid;
 };
@@ -156,8 +158,10 @@ __device__ __forceinline__ void unit_range(const EnsArgs& a, int u, int halves, 
 __device__ __forceinline__ Cursor first_cursor(const EnsArgs& a, int halves) {
     Cursor p;
     p.u = blockIdx.x;
+    p.ti = 0;
     p.valid = p.u < a.units;
     unit_range(a, p.u, halves, p.gc, p.gc_end);
+    p.gc0 = p.gc;
     unit_range(a, p.u + gridDim.x, halves, p.nx_gc, p.nx_end);
     return p;
 }
@@ -166,8 +170,9 @@ __device__ __forceinline__ Cursor next_cursor(Cursor p, const EnsArgs& a, int ha
     if (!p.valid) return p;
     if (++p.gc < p.gc_end) return p;
     p.u += gridDim.x;
+    ++p.ti;
     p.valid = p.u < a.units;
-    p.gc = p.nx_gc;
+    p.gc = p.gc0 = p.nx_gc;
     p.gc_end = p.nx_end;
     unit_range(a, p.u + gridDim.x, halves, p.nx_gc, p.nx_end);
     return p;
@@ -178,6 +183,12 @@ struct Fetch {
     int4 idx = make_int4(-1, -1, -1, -1);
     uint32_t jj = 0xffffffffu;
     int u = -1;
+};
+
+// Streamed operands of one epilogue chunk (two (node, member) pairs per thread).
+struct EpiSet {
+    float4 own[2], h32[2], d32[2];
+    double hh[2], dh[2];
 };
 
 // Operands of one step held in registers.
@@ -196,7 +207,7 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
     using C = EnsCfg<MPC>;
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t full_bar[kEnsStages], empty_bar[kEnsStages];
-    __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], fin_bar;
+    __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], tile_bar[2], fin_bar;
     __shared__ uint32_t tmem_s;
     __shared__ int abort_s;
     volatile int* abort_v = &abort_s;
@@ -211,6 +222,7 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
         for (int b = 0; b < 2; ++b) {
             tc::mbar_init(&accf_bar[b], 1);
             tc::mbar_init(&acce_bar[b], kEnsEpiWarps);
+            tc::mbar_init(&tile_bar[b], 1);
         }
         tc::mbar_init(&fin_bar, 1);
         abort_s = 0;
@@ -355,8 +367,7 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
                     const int s = g % kEnsStages;
                     if (!ens::wait(&full_bar[s], (g / kEnsStages) & 1, abort_v, a.err, 5)) { ok = false; break; }
                     tc::fence_after_sync();
-                    unsigned char* slot = smem + s * C::kStageBytes;
-                    const uint32_t a_hi = tc::smem_u32(slot), a_lo = a_hi + C::kAHalf;
+                    const uint32_t a_hi = tc::smem_u32(smem + s * C::kStageBytes), a_lo = a_hi + C::kAHalf;
                     const uint32_t b_hi = a_hi + 2 * C::kAHalf, b_lo = b_hi + C::kBHalf;
 #pragma unroll
                     for (int ks = 0; ks < kEnsKc / 8; ++ks) {
@@ -385,108 +396,151 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
     } else {
         // =============================== epilogue ===============================
         const int e = warp - C::kEpiWarp0;       // 0..7
+        const int et = threadIdx.x - 32 * C::kEpiWarp0;   // 0..255
         const int grp = e >> 2;                  // column chunks alternate between the two groups
         const int op = warp & 3;                 // TMEM lane quarter = operator
-        const int gt = threadIdx.x - 32 * (C::kEpiWarp0 + 4 * grp);   // 0..127 within the group
+        const int gt = et & 127;                 // thread within the group
         float* xch = reinterpret_cast<float*>(smem + kEnsStages * C::kStageBytes) + grp * C::kXchGroupFloats;
+        unsigned char* tbuf = smem + kEnsStages * C::kStageBytes + 2 * C::kXchGroupFloats * 4;
         const int members = a.members;
         const float c32 = (float)a.c;
+        constexpr bool kHD = MODE == kStage1 || MODE == kStage2 || MODE == kStage3;
+        // per-tile pointwise records, row sums and centre row: bulk copies into tbuf[it & 1]
+        auto issue_tile = [&](int u, int b) {
+            const int tile = u / halves;
+            const int nn = min(kEnsTileNodes, a.n - tile * kEnsTileNodes);
+            unsigned char* tb = tbuf + b * C::kTileBuf;
+            tc::mbar_arrive_expect_tx(&tile_bar[b], nn * (kPointStride * 4 + 16) + C::kN * 4);
+            tc::bulk_g2s(tb, a.PT + (long)tile * kEnsTileNodes * 5, nn * kPointStride * 4, &tile_bar[b]);
+            tc::bulk_g2s(tb + C::kTbRs, a.RS + (long)tile * kEnsTileNodes, nn * 16, &tile_bar[b]);
+            tc::bulk_g2s(tb + C::kTbCen, a.Kin + (long)__ldg(a.centre + tile) * a.mf + (u % halves) * C::kN,
+                         C::kN * 4, &tile_bar[b]);
+        };
+        // streamed per-(node, member) operands of one chunk for this thread's two pairs
+        auto fetch = [&](int u, int ch, ens::EpiSet& o) {
+            if (u >= a.units) return;
+            const int tile = u / halves;
+            const int col0 = (u % halves) * C::kN;
+#pragma unroll
+            for (int pi = 0; pi < 2; ++pi) {
+                const int pr = gt + 128 * pi;
+                const long node = (long)tile * kEnsTileNodes + (pr >> 3);
+                if (node >= a.n) continue;
+                const int mfb = col0 + ch * 32 + 4 * (pr & 7);
+                const long e4 = node * a.mf + mfb;
+                const long eh = node * members + (mfb >> 2);
+                o.own[pi] = ens::ldg_f4(a.Kin + e4);
+                if (MODE != kEvalOnly) o.hh[pi] = __ldg(a.Hh + eh);
+                if (kHD) {
+                    o.h32[pi] = ens::ldg_f4(a.H32 + e4);
+                    o.d32[pi] = ens::ldg_f4(a.D32 + e4);
+                    o.dh[pi] = __ldg(a.Dh + eh);
+                }
+            }
+        };
+        // one 32-column chunk: accumulator -> exchange -> (node, member) epilogue
+        auto chunk = [&](int u, int it, int ch, const ens::EpiSet& o) {
+            const int ab = it & 1;
+            const int tile = u / halves;
+            const int col0 = (u % halves) * C::kN;
+            const float* tb = reinterpret_cast<const float*>(tbuf + (it & 1) * C::kTileBuf);
+            {
+                const uint32_t taddr = tmem + ((uint32_t)(32 * op) << 16) + ab * C::kN + ch * 32;
+                float v0[16], v1[16];
+                tc::tmem_ld16(taddr, v0);
+                tc::tmem_ld16(taddr + 16, v1);
+                tc::tmem_wait_ld();
+                float* row = xch + (op * 32 + lane) * C::kXchStride;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    *reinterpret_cast<float4*>(row + 4 * q) = make_float4(v0[4 * q], v0[4 * q + 1], v0[4 * q + 2], v0[4 * q + 3]);
+                    *reinterpret_cast<float4*>(row + 16 + 4 * q) =
+                        make_float4(v1[4 * q], v1[4 * q + 1], v1[4 * q + 2], v1[4 * q + 3]);
+                }
+            }
+            ens::named_sync(2 + grp, 128);
+#pragma unroll
+            for (int pi = 0; pi < 2; ++pi) {
+                const int pr = gt + 128 * pi;
+                const int t = pr >> 3, bm = pr & 7;
+                const long node = (long)tile * kEnsTileNodes + t;
+                if (node >= a.n) continue;
+                const int mfb = col0 + ch * 32 + 4 * bm;      // first mf of this member
+                const int member = mfb >> 2;
+                float S[16];
+#pragma unroll
+                for (int o2 = 0; o2 < 4; ++o2) {
+                    const float4 sv = *reinterpret_cast<const float4*>(xch + (o2 * 32 + t) * C::kXchStride + 4 * bm);
+                    S[4 * o2] = sv.x; S[4 * o2 + 1] = sv.y; S[4 * o2 + 2] = sv.z; S[4 * o2 + 3] = sv.w;
+                }
+                const float4 cen = *reinterpret_cast<const float4*>(tb + C::kTbCen / 4 + (mfb - col0));
+                const float4 rs4 = *reinterpret_cast<const float4*>(tb + C::kTbRs / 4 + 4 * t);
+                const float cf[4] = {cen.x, cen.y, cen.z, cen.w};
+                const float rs[4] = {rs4.x, rs4.y, rs4.z, rs4.w};
+#pragma unroll
+                for (int o2 = 0; o2 < 4; ++o2)
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) S[4 * o2 + f] = fmaf(cf[f], rs[o2], S[4 * o2 + f]);
+                const float q[4] = {o.own[pi].x, o.own[pi].y, o.own[pi].z, o.own[pi].w};
+                float F[4];
+                pointwise_rhs<float>(S, q, tb + t * kPointStride, a.gh0, F);
+                const long e4 = node * a.mf + mfb;
+                const long eh = node * members + member;
+                if (MODE == kEvalOnly) {
+                    *reinterpret_cast<float4*>(a.F + e4) = make_float4(F[0], F[1], F[2], F[3]);
+                } else if (MODE == kStage0) {
+                    // K = H + c F (q is the base state here); D = F
+                    const double fh = (double)F[3];
+                    *reinterpret_cast<float4*>(a.D32 + e4) = make_float4(F[0], F[1], F[2], 0.f);
+                    a.Dh[eh] = fh;
+                    *reinterpret_cast<float4*>(a.Kout + e4) =
+                        make_float4(__fadd_rn(q[0], __fmul_rn(c32, F[0])), __fadd_rn(q[1], __fmul_rn(c32, F[1])),
+                                    __fadd_rn(q[2], __fmul_rn(c32, F[2])), __double2float_rn(o.hh[pi] + a.c * fh));
+                } else if (MODE == kStage1 || MODE == kStage2) {
+                    const double fh = (double)F[3];
+                    const float4 h4 = o.h32[pi], d4 = o.d32[pi];
+                    *reinterpret_cast<float4*>(a.D32 + e4) =
+                        make_float4(__fadd_rn(d4.x, __fmul_rn(2.f, F[0])), __fadd_rn(d4.y, __fmul_rn(2.f, F[1])),
+                                    __fadd_rn(d4.z, __fmul_rn(2.f, F[2])), 0.f);
+                    a.Dh[eh] = o.dh[pi] + 2.0 * fh;
+                    *reinterpret_cast<float4*>(a.Kout + e4) =
+                        make_float4(__fadd_rn(h4.x, __fmul_rn(c32, F[0])), __fadd_rn(h4.y, __fmul_rn(c32, F[1])),
+                                    __fadd_rn(h4.z, __fmul_rn(c32, F[2])), __double2float_rn(o.hh[pi] + a.c * fh));
+                } else {
+                    const float4 h4 = o.h32[pi], d4 = o.d32[pi];
+                    const float du = __fadd_rn(d4.x, F[0]), dv = __fadd_rn(d4.y, F[1]), dw = __fadd_rn(d4.z, F[2]);
+                    const double dh = o.dh[pi] + (double)F[3];
+                    const double h = o.hh[pi] + a.dt6 * dh;
+                    a.Hh[eh] = h;
+                    *reinterpret_cast<float4*>(a.H32 + e4) =
+                        make_float4(__double2float_rn((double)h4.x + a.dt6 * (double)du),
+                                    __double2float_rn((double)h4.y + a.dt6 * (double)dv),
+                                    __double2float_rn((double)h4.z + a.dt6 * (double)dw), __double2float_rn(h));
+                }
+            }
+            ens::named_sync(2 + grp, 128);
+        };
+        constexpr int kCh = C::kN / 64;          // chunks per group per tile
+        ens::EpiSet sa;
+        if (et == 0 && blockIdx.x < a.units) issue_tile(blockIdx.x, 0);
         int it = 0;
         for (int u = blockIdx.x; u < a.units; u += gridDim.x, ++it) {
             const int ab = it & 1;
-            const bool got = ens::wait(&accf_bar[ab], (it >> 1) & 1, abort_v, a.err, 7);
-            if (!ens::named_and(2 + grp, 128, got && !*abort_v)) break;
+            const bool got = ens::wait(&accf_bar[ab], (it >> 1) & 1, abort_v, a.err, 7) &&
+                             ens::wait(&tile_bar[it & 1], (it >> 1) & 1, abort_v, a.err, 8);
+            // every epilogue thread is done with the previous tile (and its tile buffer)
+            if (!ens::named_and(4, 32 * kEnsEpiWarps, got && !*abort_v)) break;
             tc::fence_after_sync();
-            const int tile = u / halves;
-            const int col0 = (u % halves) * C::kN;
-            const long cnode = __ldg(a.centre + tile);
-            for (int ch = grp; ch < C::kN / 32; ch += 2) {
-                float v[32];
-                {
-                    const uint32_t taddr = tmem + ((uint32_t)(32 * op) << 16) + ab * C::kN + ch * 32;
-                    float v0[16], v1[16];
-                    tc::tmem_ld16(taddr, v0);
-                    tc::tmem_ld16(taddr + 16, v1);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int q = 0; q < 16; ++q) { v[q] = v0[q]; v[16 + q] = v1[q]; }
-                }
-                float* row = xch + (op * 32 + lane) * C::kXchStride;
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    *reinterpret_cast<float4*>(row + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-                ens::named_sync(2 + grp, 128);
-#pragma unroll
-                for (int pi = 0; pi < 2; ++pi) {
-                    const int pr = gt + 128 * pi;
-                    const int t = pr >> 3, bm = pr & 7;
-                    const long node = (long)tile * kEnsTileNodes + t;
-                    if (node >= a.n) continue;
-                    const int mfb = col0 + ch * 32 + 4 * bm;      // first mf of this member
-                    const int member = mfb >> 2;
-                    float S[16];
-#pragma unroll
-                    for (int o = 0; o < 4; ++o) {
-                        const float4 sv = *reinterpret_cast<const float4*>(xch + (o * 32 + t) * C::kXchStride + 4 * bm);
-                        S[4 * o] = sv.x; S[4 * o + 1] = sv.y; S[4 * o + 2] = sv.z; S[4 * o + 3] = sv.w;
-                    }
-                    const float4 cen = ens::ldg_f4(a.Kin + cnode * a.mf + mfb);
-                    const float4 rs4 = __ldg(a.RS + node);
-                    const float cf[4] = {cen.x, cen.y, cen.z, cen.w};
-                    const float rs[4] = {rs4.x, rs4.y, rs4.z, rs4.w};
-#pragma unroll
-                    for (int o = 0; o < 4; ++o)
-#pragma unroll
-                        for (int f = 0; f < 4; ++f) S[4 * o + f] = fmaf(cf[f], rs[o], S[4 * o + f]);
-                    const float4 q4 = ens::ldg_f4(a.Kin + node * a.mf + mfb);
-                    const float q[4] = {q4.x, q4.y, q4.z, q4.w};
-                    float pt[kPointStride];
-#pragma unroll
-                    for (int pp = 0; pp < 5; ++pp) {
-                        const float4 pv = __ldg(a.PT + node * 5 + pp);
-                        pt[4 * pp] = pv.x; pt[4 * pp + 1] = pv.y; pt[4 * pp + 2] = pv.z; pt[4 * pp + 3] = pv.w;
-                    }
-                    float F[4];
-                    pointwise_rhs<float>(S, q, pt, a.gh0, F);
-                    const long e4 = node * a.mf + mfb;
-                    const long eh = node * members + member;
-                    if (MODE == kEvalOnly) {
-                        *reinterpret_cast<float4*>(a.F + e4) = make_float4(F[0], F[1], F[2], F[3]);
-                    } else if (MODE == kStage0) {
-                        // K = H + c F (q is the base state here); D = F
-                        const double fh = (double)F[3];
-                        const double hb = a.Hh[eh];
-                        *reinterpret_cast<float4*>(a.D32 + e4) = make_float4(F[0], F[1], F[2], 0.f);
-                        a.Dh[eh] = fh;
-                        *reinterpret_cast<float4*>(a.Kout + e4) =
-                            make_float4(__fadd_rn(q[0], __fmul_rn(c32, F[0])), __fadd_rn(q[1], __fmul_rn(c32, F[1])),
-                                        __fadd_rn(q[2], __fmul_rn(c32, F[2])), __double2float_rn(hb + a.c * fh));
-                    } else if (MODE == kStage1 || MODE == kStage2) {
-                        const double fh = (double)F[3];
-                        const double hb = a.Hh[eh];
-                        const float4 h4 = *reinterpret_cast<const float4*>(a.H32 + e4);
-                        const float4 d4 = *reinterpret_cast<const float4*>(a.D32 + e4);
-                        *reinterpret_cast<float4*>(a.D32 + e4) =
-                            make_float4(__fadd_rn(d4.x, __fmul_rn(2.f, F[0])), __fadd_rn(d4.y, __fmul_rn(2.f, F[1])),
-                                        __fadd_rn(d4.z, __fmul_rn(2.f, F[2])), 0.f);
-                        a.Dh[eh] = a.Dh[eh] + 2.0 * fh;
-                        *reinterpret_cast<float4*>(a.Kout + e4) =
-                            make_float4(__fadd_rn(h4.x, __fmul_rn(c32, F[0])), __fadd_rn(h4.y, __fmul_rn(c32, F[1])),
-                                        __fadd_rn(h4.z, __fmul_rn(c32, F[2])), __double2float_rn(hb + a.c * fh));
-                    } else {
-                        const float4 h4 = *reinterpret_cast<const float4*>(a.H32 + e4);
-                        const float4 d4 = *reinterpret_cast<const float4*>(a.D32 + e4);
-                        const float du = __fadd_rn(d4.x, F[0]), dv = __fadd_rn(d4.y, F[1]), dw = __fadd_rn(d4.z, F[2]);
-                        const double dh = a.Dh[eh] + (double)F[3];
-                        const double h = a.Hh[eh] + a.dt6 * dh;
-                        a.Hh[eh] = h;
-                        *reinterpret_cast<float4*>(a.H32 + e4) =
-                            make_float4(__double2float_rn((double)h4.x + a.dt6 * (double)du),
-                                        __double2float_rn((double)h4.y + a.dt6 * (double)dv),
-                                        __double2float_rn((double)h4.z + a.dt6 * (double)dw), __double2float_rn(h));
-                    }
-                }
-                ens::named_sync(2 + grp, 128);
+            if (et == 0 && u + (int)gridDim.x < a.units) {
+                tc::fence_async_smem();   // the buffer's earlier reads come before the copy's writes
+                issue_tile(u + gridDim.x, (it + 1) & 1);
+            }
+#pragma unroll 1
+            for (int c = 0; c < kCh; ++c) {
+                // streamed operands first: their latency overlaps the accumulator read and exchange
+                const int ch = grp + 2 * c;
+                fetch(u, ch, sa);
+                chunk(u, it, ch, sa);
             }
             tc::fence_before_sync();
             __syncwarp();

@@ -27,20 +27,9 @@ constexpr int kTmaThreads = 32 * (kTmaConsumerWarps + 1);
 constexpr uint32_t kTmaWaitTries = 1u << 24;
 
 namespace tma {
-__device__ __forceinline__ void arrive_expect_tx(uint64_t* b, uint32_t tx) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(b)), "r"(tx)
-                 : "memory");
-}
-__device__ __forceinline__ void arrive(uint64_t* b) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            tc::smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(tc::smem_u32(mbar))
-        : "memory");
-}
+using tc::bulk_g2s;
+__device__ __forceinline__ void arrive_expect_tx(uint64_t* b, uint32_t tx) { tc::mbar_arrive_expect_tx(b, tx); }
+__device__ __forceinline__ void arrive(uint64_t* b) { tc::mbar_arrive(b); }
 }  // namespace tma
 
 template <typename T>

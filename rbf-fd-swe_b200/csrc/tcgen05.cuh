@@ -105,6 +105,22 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, 
     return false;
 }
 
+// ---- bulk copies (global -> shared, completion counted in bytes on an mbarrier) ------
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* b, uint32_t tx) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(tx) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+// Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+        : "memory");
+}
+
 // Round an FP32 value to the nearest TF32 (10 explicit mantissa bits), ties
 // away from zero; the result is exactly representable, so the tensor core's
 // own FP32 -> TF32 conversion leaves it unchanged.
