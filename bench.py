@@ -45,6 +45,8 @@ WORKLOADS = {
     "plain_fp32_n655362": (8, "fp32", "plain FP32, N=655362 (level 8), CFDL, RCM, dt=60 s"),
     "ens_tf32_n163842_b64": (7, "tf32x3", "batched ensemble, N=163842 (level 7), 64 members, 3xTF32 on tcgen05, dt=120 s"),
     "ens_tf32_n40962_b64": (6, "tf32x3", "batched ensemble, N=40962 (level 6), 64 members, 3xTF32 on tcgen05, dt=225 s"),
+    "ens_bf16_n163842_b64": (7, "bf16x3", "batched ensemble, N=163842 (level 7), 64 members, split BF16 on tcgen05, "
+                                          "dt=120 s"),
     "serve_mix": (0, "serve", "serving: Poisson arrivals over N in {2562, 10242, 40962, 163842}, 1-32 members, "
                               "10-500 steps, 80 GB budget, FP64"),
 }
@@ -210,9 +212,9 @@ def run_reference(args, level, prec, wl):
     print(json.dumps(line), flush=True)
 
 
-def run_ensemble(args, level, desc, members=64):
-    """member-steps/s of the batched 3xTF32 form, next to the plain FP64 form on the
-    same grid, with the h error of a few members against the plain FP64 run."""
+def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
+    """member-steps/s of the batched form (3xTF32 or split BF16), next to the plain FP64
+    form on the same grid, with the h error of a few members against the plain FP64 run."""
     import torch
 
     from swe_b200 import capi, gen
@@ -230,6 +232,7 @@ def run_ensemble(args, level, desc, members=64):
     ens = capi.Ensemble()
     capi.check("swe_cuda_select_device", ens.lib.swe_cuda_select_device(local))
     ens.init(m, members)
+    ens.set_precision(precision)
     ens.set_state(H0)
     tune_ms = ens.tune().tolist()
     cfg = ens.config()
@@ -314,10 +317,11 @@ def run_ensemble(args, level, desc, members=64):
     ens.finalize()
     if rank == 0:
         line = {
-            "metric": "member-steps/s (batched ensemble, 3xTF32 tcgen05) and ratio to plain FP64",
+            "metric": f"member-steps/s (batched ensemble, {'3xTF32' if precision == 'tf32x3' else 'split BF16'} "
+                      "tcgen05) and ratio to plain FP64",
             "value": member_steps, "unit": "member-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "tf32x3 (fp32 state, fp64 h accumulation)",
+            "scaling": "weak", "vs_baseline": None, "dtype": f"{precision} (fp32 state, fp64 h accumulation)",
             "data": "synthetic (seeded icosahedral grid, PHS RBF-FD weights, TC5 ICs, per-member 1e-3 h noise)",
             "config": {"workload": args.workload, "description": desc, "nodes": N, "members": members,
                        "dt": d.dt, "kernel_variant": cfg, "tune_ms_per_step": tune_ms,
@@ -428,10 +432,10 @@ def main():
     args.warmup = max(args.warmup, 3)
     level, prec, desc = WORKLOADS[args.workload]
     if args.impl == "reference":
-        return run_reference(args, level if level else 6, "fp64" if prec in ("tf32x3", "serve") else prec,
+        return run_reference(args, level if level else 6, "fp64" if prec in ("tf32x3", "bf16x3", "serve") else prec,
                              args.workload)
-    if prec == "tf32x3":
-        return run_ensemble(args, level, desc)
+    if prec in ("tf32x3", "bf16x3"):
+        return run_ensemble(args, level, desc, precision=prec)
     if prec == "serve":
         return run_serving(args, desc)
 

@@ -132,10 +132,11 @@ int swe_cuda_finalize(void);
  * states of the same grid together.  Static arrays are the canonical FP64
  * ones in natural node order -- idx [n][nnbr] 0-based, Dx, Dy, Dz, L [n][nnbr]
  * already scaled as input.c:314-319 scales them, x, y, z, f, ghm [n],
- * p_u, p_v, p_w, gradghm [n][3].  The library reorders nodes by the
- * reference's RCM permutation internally; states are exchanged as
- * [members][n][4] FP64 in natural order.
- * Precision: stencil products in 3xTF32 on tcgen05 with FP32 accumulation;
+ * p_u, p_v, p_w, gradghm [n][3].  The library reorders nodes along a
+ * space-filling curve internally; states are exchanged as [members][n][4]
+ * FP64 in natural order.
+ * Precision: stencil products in 3xTF32 (or split BF16, see
+ * swe_ens_set_precision) on tcgen05 with FP32 accumulation;
  * u, v, w and the stage states K in FP32; the RK4 accumulation of h (base
  * state and D register) in FP64; invariants in FP64. */
 int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int* idx,
@@ -152,15 +153,20 @@ int swe_ens_eval_rhs(const double* K, double* F);
  * kernels); swe_ens_stage runs one stage, same semantics as RK_substep. */
 int swe_ens_step(int nsteps);
 int swe_ens_stage(int substep_id);
-/* Autotuner: times one RK4 step of every kernel variant (tile of 4 or 8 nodes x
- * 32 or 64 members per CTA) on the live state, restores the state and keeps
- * the fastest.  ms_per_step[4] (may be NULL) receives the timings, -1 where a
- * variant does not apply.  config[4] = {tile nodes, members per CTA, largest
- * neighbour set of a 4-node tile, of an 8-node tile}. */
+/* Autotuner: times one RK4 step of every kernel variant (32 or 64 members per
+ * CTA; tiles are 32 nodes) in the current precision on the live state,
+ * restores the state and keeps the fastest.  ms_per_step[4] (may be NULL)
+ * receives the timings ({32, 64} members per CTA, then two unused slots), -1
+ * where a variant does not apply.  config[5] = {tile nodes, members per CTA,
+ * largest neighbour set of a tile, tiles, precision}. */
 int swe_ens_tune(double* ms_per_step);
 int swe_ens_config(int* config);
-/* Forces one variant (tile_nodes 4 or 8, members_per_cta 32 or 64). */
+/* Forces one variant (tile_nodes 32, members_per_cta 32 or 64). */
 int swe_ens_use_variant(int tile_nodes, int members_per_cta);
+/* Precision of the stencil products: 0 = 3xTF32 (default; hi and lo parts both
+ * exact TF32, |x - hi - lo| <= 2^-22 |x|), 1 = split BF16 (2^-17), both with
+ * FP32 accumulation and the same FP64 h accumulation. */
+int swe_ens_set_precision(int precision);
 /* FP64 (mass, energy) per member, [members][2], definitions as swe_cuda_invariants. */
 int swe_ens_invariants(double* mass_energy);
 int swe_ens_sync(void);

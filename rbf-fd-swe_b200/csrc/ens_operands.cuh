@@ -1,0 +1,286 @@
+// Operand policies of the batched-ensemble kernel: how the converter threads
+// gather one 16-row chunk of a tile's neighbour rows and weights, split them
+// into hi / lo parts in the tensor core's shared-memory layout, and how the
+// MMA thread issues the chunk's three products.
+//
+//   Tf32x3: kind::tf32, hi / lo both exact TF32 (|x - hi - lo| <= 2^-22 |x|),
+//           2 k-steps of K = 8 per chunk.
+//   Bf16x3: kind::f16 with BF16 operands, hi = bf16(x), lo = bf16(x - hi)
+//           (|x - hi - lo| <= 2^-17 |x|), one k-step of K = 16 per chunk;
+//           half the shared-memory bytes of Tf32x3 and twice the tensor rate.
+//
+// Both are K-major without swizzle: 8-row x 16-byte core matrices, LBO = 128
+// (the next core matrix along K), SBO = the stride between 8-row groups.  The
+// B (state) operand's SBO is padded by 16 bytes so that the converters'
+// 16-byte stores of consecutive member-fields fall in distinct bank groups.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <type_traits>
+
+#include "tcgen05.cuh"
+
+namespace swe {
+
+constexpr int kEnsTileNodes = 32;   // nodes per tile (M = 4 operators x 32 nodes)
+constexpr int kEnsKc = 16;          // neighbour rows per pipeline chunk
+
+enum EnsPrecision { kTf32x3 = 0, kBf16x3 = 1 };
+
+struct EnsArgs;
+
+namespace ens {
+
+__device__ __forceinline__ float4 ldg_f4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ float2 ldg_f2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+
+// hi = bf16(a, b) (round to nearest even), lo = bf16 of the remainders; packed pairs, a in the low half.
+__device__ __forceinline__ uint32_t bf16x2_split(float a, float b, uint32_t& lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    const float2 hf = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+template <int MPC, int PREC>
+struct Operands;
+
+// --------------------------------------------------------------------------------------
+// 3xTF32.  B thread: member-fields 4q..4q+3 of rows 4kg..4kg+3; A thread: node t, rows
+// 4akg..4akg+3, operator pairs opp0 .. opp0 + kOpp - 1.
+// --------------------------------------------------------------------------------------
+template <int MPC>
+struct Operands<MPC, kTf32x3> {
+    static constexpr int kN = 4 * MPC;
+    static constexpr int kConvThreads = 4 * MPC;
+    static constexpr int kOpp = 256 / kConvThreads;
+    static constexpr int kSboA = (kEnsKc / 4) * 128;
+    static constexpr int kSboB = (kEnsKc / 4) * 128 + 16;
+    static constexpr int kAHalf = (128 / 8) * kSboA;
+    static constexpr int kBHalf = (kN / 8) * kSboB;
+    static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
+    static constexpr int kStages = 3;
+    static_assert(kOpp == 1 || kOpp == 2, "A build covers 32 nodes x 4 row groups x 2 operator pairs");
+
+    struct Thread {
+        int quad, kg, at, akg, opp0;
+        __device__ explicit Thread(int ct)
+            : quad(ct % MPC), kg(ct / MPC), at(ct & 31), akg((ct >> 5) & 3), opp0((ct >> 7) * kOpp) {}
+        __device__ int col() const { return 4 * quad; }
+    };
+    struct Fetch {
+        int4 idx = make_int4(-1, -1, -1, -1);
+        uint32_t jj = 0xffffffffu;
+    };
+    struct Set {
+        float4 x[4];          // 4 gathered rows x 4 member-fields
+        float4 cen;           // centre state of the same member-fields
+        int live;             // bit i: row i is a real row
+        float2 w[kOpp][4];    // weights of the operator pairs for the 4 chunk rows
+    };
+
+    __device__ static void fetch_idx(const int* rows, const uint32_t* jmap, int gc, const Thread& th, Fetch& f) {
+        f.idx = __ldg(reinterpret_cast<const int4*>(rows + gc * kEnsKc + 4 * th.kg));
+        f.jj = __ldg(jmap + (gc * 4 + th.akg) * 32 + th.at);
+    }
+    __device__ static void fetch_ops(const float* Kin, int mf, long col, const float4* W, long node, const float* cen_row,
+                                     const Thread& th, const Fetch& f, Set& o, const Set& prev) {
+        const int r[4] = {f.idx.x, f.idx.y, f.idx.z, f.idx.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            o.x[i] = r[i] >= 0 ? ldg_f4(Kin + (long)r[i] * mf + col) : make_float4(0.f, 0.f, 0.f, 0.f);
+        o.live = (r[0] >= 0 ? 1 : 0) | (r[1] >= 0 ? 2 : 0) | (r[2] >= 0 ? 4 : 0) | (r[3] >= 0 ? 8 : 0);
+        o.cen = cen_row ? ldg_f4(cen_row + col) : prev.cen;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t j = (f.jj >> (8 * i)) & 0xffu;
+#pragma unroll
+            for (int q = 0; q < kOpp; ++q)
+                o.w[q][i] = j != 0xffu ? __ldg(reinterpret_cast<const float2*>(W + node * 32 + j) + th.opp0 + q)
+                                       : make_float2(0.f, 0.f);
+        }
+    }
+    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o) {
+        unsigned char* A_hi = slot;
+        unsigned char* A_lo = slot + kAHalf;
+        unsigned char* B_hi = slot + 2 * kAHalf;
+        unsigned char* B_lo = B_hi + kBHalf;
+        // A: one 16-byte core row (4 chunk rows) of (operator, node) per operator handled
+#pragma unroll
+        for (int q = 0; q < kOpp; ++q)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = 32 * (2 * (th.opp0 + q) + h) + th.at;
+                float4 hi, lo;
+                tc::tf32_split(h ? o.w[q][0].y : o.w[q][0].x, hi.x, lo.x);
+                tc::tf32_split(h ? o.w[q][1].y : o.w[q][1].x, hi.y, lo.y);
+                tc::tf32_split(h ? o.w[q][2].y : o.w[q][2].x, hi.z, lo.z);
+                tc::tf32_split(h ? o.w[q][3].y : o.w[q][3].x, hi.w, lo.w);
+                const uint32_t off = (r >> 3) * kSboA + th.akg * 128 + (r & 7) * 16;
+                *reinterpret_cast<float4*>(A_hi + off) = hi;
+                *reinterpret_cast<float4*>(A_lo + off) = lo;
+            }
+        // B: each member-field's 4 rows are one 16-byte core row
+        const float xv[4][4] = {{o.x[0].x, o.x[0].y, o.x[0].z, o.x[0].w},
+                                {o.x[1].x, o.x[1].y, o.x[1].z, o.x[1].w},
+                                {o.x[2].x, o.x[2].y, o.x[2].z, o.x[2].w},
+                                {o.x[3].x, o.x[3].y, o.x[3].z, o.x[3].w}};
+        const float cv[4] = {o.cen.x, o.cen.y, o.cen.z, o.cen.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int nrow = 4 * th.quad + j;
+            float4 hi, lo;
+            float y[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) y[i] = ((o.live >> i) & 1) ? xv[i][j] - cv[j] : 0.f;
+            tc::tf32_split(y[0], hi.x, lo.x);
+            tc::tf32_split(y[1], hi.y, lo.y);
+            tc::tf32_split(y[2], hi.z, lo.z);
+            tc::tf32_split(y[3], hi.w, lo.w);
+            const uint32_t off = (nrow >> 3) * kSboB + th.kg * 128 + (nrow & 7) * 16;
+            *reinterpret_cast<float4*>(B_hi + off) = hi;
+            *reinterpret_cast<float4*>(B_lo + off) = lo;
+        }
+    }
+    // The chunk's products A_hi B_hi + A_hi B_lo + A_lo B_hi into accumulator d.
+    __device__ static void issue(uint32_t slot, uint32_t d, bool first) {
+        constexpr uint32_t idesc = tc::idesc_tf32(128, kN);
+        const uint32_t a_hi = slot, a_lo = slot + kAHalf, b_hi = slot + 2 * kAHalf, b_lo = b_hi + kBHalf;
+#pragma unroll
+        for (int ks = 0; ks < kEnsKc / 8; ++ks) {
+            const uint64_t dah = tc::smem_desc(a_hi + ks * 256, 128, kSboA);
+            const uint64_t dal = tc::smem_desc(a_lo + ks * 256, 128, kSboA);
+            const uint64_t dbh = tc::smem_desc(b_hi + ks * 256, 128, kSboB);
+            const uint64_t dbl = tc::smem_desc(b_lo + ks * 256, 128, kSboB);
+            tc::mma_tf32(d, dah, dbh, idesc, (!first || ks > 0) ? 1u : 0u);
+            tc::mma_tf32(d, dah, dbl, idesc, 1u);
+            tc::mma_tf32(d, dal, dbh, idesc, 1u);
+        }
+    }
+};
+
+// --------------------------------------------------------------------------------------
+// split BF16.  B thread: member-fields 2p, 2p+1 of rows 8kh..8kh+7; A thread: node t,
+// rows 8akh..8akh+7, operators op0 .. op0 + kOps - 1.
+// --------------------------------------------------------------------------------------
+template <int MPC>
+struct Operands<MPC, kBf16x3> {
+    static constexpr int kN = 4 * MPC;
+    static constexpr int kConvThreads = 4 * MPC;
+    static constexpr int kOps = 256 / kConvThreads;
+    static constexpr int kSboA = (kEnsKc / 8) * 128;
+    static constexpr int kSboB = (kEnsKc / 8) * 128 + 16;
+    static constexpr int kAHalf = (128 / 8) * kSboA;
+    static constexpr int kBHalf = (kN / 8) * kSboB;
+    static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
+    static constexpr int kStages = 5;
+    static_assert(kOps == 1 || kOps == 2, "A build covers 32 nodes x 2 row halves x 4 operators");
+
+    struct Thread {
+        int p, kh, at, akh, op0;
+        __device__ explicit Thread(int ct)
+            : p(ct % (kN / 2)), kh(ct / (kN / 2)), at(ct & 31), akh((ct >> 5) & 1), op0((ct >> 6) * kOps) {}
+        __device__ int col() const { return 2 * p; }
+    };
+    struct Fetch {
+        int4 idx[2] = {make_int4(-1, -1, -1, -1), make_int4(-1, -1, -1, -1)};
+        uint32_t jj[2] = {0xffffffffu, 0xffffffffu};
+    };
+    // weights of the thread's operators for the 8 chunk rows: one operator, or the pair op0, op0 + 1
+    using WT = typename std::conditional<kOps == 1, float, float2>::type;
+    struct Set {
+        float2 x[8];          // 8 gathered rows x 2 member-fields
+        float2 cen;
+        int live;             // bit i: row i is a real row
+        WT w[8];
+    };
+
+    __device__ static void fetch_idx(const int* rows, const uint32_t* jmap, int gc, const Thread& th, Fetch& f) {
+        const int4* r = reinterpret_cast<const int4*>(rows + gc * kEnsKc + 8 * th.kh);
+        f.idx[0] = __ldg(r);
+        f.idx[1] = __ldg(r + 1);
+        f.jj[0] = __ldg(jmap + (gc * 4 + 2 * th.akh) * 32 + th.at);
+        f.jj[1] = __ldg(jmap + (gc * 4 + 2 * th.akh + 1) * 32 + th.at);
+    }
+    __device__ static void fetch_ops(const float* Kin, int mf, long col, const float4* W, long node, const float* cen_row,
+                                     const Thread& th, const Fetch& f, Set& o, const Set& prev) {
+        const int r[8] = {f.idx[0].x, f.idx[0].y, f.idx[0].z, f.idx[0].w,
+                          f.idx[1].x, f.idx[1].y, f.idx[1].z, f.idx[1].w};
+        int live = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            o.x[i] = r[i] >= 0 ? ldg_f2(Kin + (long)r[i] * mf + col) : make_float2(0.f, 0.f);
+            live |= (r[i] >= 0 ? 1 : 0) << i;
+        }
+        o.live = live;
+        o.cen = cen_row ? ldg_f2(cen_row + col) : prev.cen;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t j = (f.jj[i >> 2] >> (8 * (i & 3))) & 0xffu;
+            if constexpr (kOps == 1)
+                o.w[i] = j != 0xffu ? __ldg(reinterpret_cast<const float*>(W + node * 32 + j) + th.op0) : 0.f;
+            else
+                o.w[i] = j != 0xffu ? __ldg(reinterpret_cast<const float2*>(W + node * 32 + j) + (th.op0 >> 1))
+                                    : make_float2(0.f, 0.f);
+        }
+    }
+    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o) {
+        unsigned char* A_hi = slot;
+        unsigned char* A_lo = slot + kAHalf;
+        unsigned char* B_hi = slot + 2 * kAHalf;
+        unsigned char* B_lo = B_hi + kBHalf;
+        // A: one 16-byte core row (8 chunk rows) of (operator, node) per operator handled
+#pragma unroll
+        for (int q = 0; q < kOps; ++q) {
+            const int op = th.op0 + q;
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if constexpr (kOps == 1) v[i] = o.w[i];
+                else v[i] = (op & 1) ? o.w[i].y : o.w[i].x;
+            }
+            uint4 hi, lo;
+            hi.x = bf16x2_split(v[0], v[1], lo.x);
+            hi.y = bf16x2_split(v[2], v[3], lo.y);
+            hi.z = bf16x2_split(v[4], v[5], lo.z);
+            hi.w = bf16x2_split(v[6], v[7], lo.w);
+            const int r = 32 * op + th.at;
+            const uint32_t off = (r >> 3) * kSboA + th.akh * 128 + (r & 7) * 16;
+            *reinterpret_cast<uint4*>(A_hi + off) = hi;
+            *reinterpret_cast<uint4*>(A_lo + off) = lo;
+        }
+        // B: each member-field's 8 rows are one 16-byte core row
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const float c = j ? o.cen.y : o.cen.x;
+            float y[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) y[i] = ((o.live >> i) & 1) ? (j ? o.x[i].y : o.x[i].x) - c : 0.f;
+            uint4 hi, lo;
+            hi.x = bf16x2_split(y[0], y[1], lo.x);
+            hi.y = bf16x2_split(y[2], y[3], lo.y);
+            hi.z = bf16x2_split(y[4], y[5], lo.z);
+            hi.w = bf16x2_split(y[6], y[7], lo.w);
+            const int nrow = 2 * th.p + j;
+            const uint32_t off = (nrow >> 3) * kSboB + th.kh * 128 + (nrow & 7) * 16;
+            *reinterpret_cast<uint4*>(B_hi + off) = hi;
+            *reinterpret_cast<uint4*>(B_lo + off) = lo;
+        }
+    }
+    __device__ static void issue(uint32_t slot, uint32_t d, bool first) {
+        constexpr uint32_t idesc = tc::idesc_bf16(128, kN);
+        const uint32_t a_hi = slot, a_lo = slot + kAHalf, b_hi = slot + 2 * kAHalf, b_lo = b_hi + kBHalf;
+        const uint64_t dah = tc::smem_desc(a_hi, 128, kSboA);
+        const uint64_t dal = tc::smem_desc(a_lo, 128, kSboA);
+        const uint64_t dbh = tc::smem_desc(b_hi, 128, kSboB);
+        const uint64_t dbl = tc::smem_desc(b_lo, 128, kSboB);
+        tc::mma_f16(d, dah, dbh, idesc, first ? 0u : 1u);
+        tc::mma_f16(d, dah, dbl, idesc, 1u);
+        tc::mma_f16(d, dal, dbh, idesc, 1u);
+    }
+};
+
+}  // namespace ens
+}  // namespace swe

@@ -198,6 +198,7 @@ struct Ensemble {
     float4* W = nullptr;
     Variant var[2];       // members per CTA: 32, 64
     int chosen = -1;
+    int prec = kTf32x3;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool timing = false;
@@ -250,34 +251,39 @@ struct Ensemble {
         return a;
     }
 
-    template <int MPC>
+    template <int MPC, int PREC>
     void launch_v(int mode) {
-        using C = EnsCfg<MPC>;
+        using C = EnsCfg<MPC, PREC>;
         const EnsArgs a = args(mode, MPC);
         const int grid = std::min(a.units, nsm);
         switch (mode) {
-            case 0: ens_stage_kernel<MPC, kStage0><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
-            case 1: ens_stage_kernel<MPC, kStage1><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
-            case 2: ens_stage_kernel<MPC, kStage2><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
-            case 3: ens_stage_kernel<MPC, kStage3><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
-            default: ens_stage_kernel<MPC, kEvalOnly><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 0: ens_stage_kernel<MPC, kStage0, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 1: ens_stage_kernel<MPC, kStage1, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 2: ens_stage_kernel<MPC, kStage2, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 3: ens_stage_kernel<MPC, kStage3, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            default: ens_stage_kernel<MPC, kEvalOnly, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
         }
     }
 
     void launch(int vi, int mode) {
-        if (var[vi].mpc == 64) launch_v<64>(mode);
-        else launch_v<32>(mode);
+        if (prec == kBf16x3) {
+            if (var[vi].mpc == 64) launch_v<64, kBf16x3>(mode);
+            else launch_v<32, kBf16x3>(mode);
+        } else {
+            if (var[vi].mpc == 64) launch_v<64, kTf32x3>(mode);
+            else launch_v<32, kTf32x3>(mode);
+        }
         count_launch();
     }
 
-    template <int MPC>
+    template <int MPC, int PREC>
     static int set_attrs() {
-        const int sm = EnsCfg<MPC>::kSmem;
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kEvalOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        const int sm = EnsCfg<MPC, PREC>::kSmem;
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage0, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage1, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage2, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage3, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kEvalOnly, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
         return SWE_OK;
     }
 
@@ -453,8 +459,11 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     E.var[0].usable = true;
     E.var[1].mpc = 64;
     E.var[1].usable = members % 64 == 0;
-    SWE_TRY(Ensemble::set_attrs<32>());
-    SWE_TRY(Ensemble::set_attrs<64>());
+    SWE_TRY((Ensemble::set_attrs<32, kTf32x3>()));
+    SWE_TRY((Ensemble::set_attrs<64, kTf32x3>()));
+    SWE_TRY((Ensemble::set_attrs<32, kBf16x3>()));
+    SWE_TRY((Ensemble::set_attrs<64, kBf16x3>()));
+    E.prec = kTf32x3;
     E.ready = true;
     // default choice until tuned: all members in one CTA
     E.chosen = E.var[1].usable ? 1 : 0;
@@ -566,7 +575,20 @@ int swe_ens_config(int* out) {
     out[1] = g_ens.var[g_ens.chosen].mpc;
     out[2] = g_ens.max_rows;
     out[3] = g_ens.ntiles;
+    out[4] = g_ens.prec;
     return SWE_OK;
+}
+
+int swe_ens_set_precision(int precision) {
+    SWE_TRY(ens_ready());
+    if (precision != kTf32x3 && precision != kBf16x3) {
+        set_error("swe_ens_set_precision: %d is neither 0 (3xTF32) nor 1 (split BF16)", precision);
+        return SWE_ERR_ARG;
+    }
+    SWE_CUDA_TRY(cudaStreamSynchronize(g_ens.stream));
+    g_ens.prec = precision;
+    g_ens.tune_ms[0] = g_ens.tune_ms[1] = -1.0;
+    return g_ens.build_graph();
 }
 
 int swe_ens_invariants(double* out) {

@@ -1,4 +1,4 @@
-// Batched-ensemble RK4 stage kernel on tcgen05 tensor cores (3xTF32).
+// Batched-ensemble RK4 stage kernel on tcgen05 tensor cores (3xTF32 or split BF16).
 //
 // B ensemble members share one grid.  The state is stored member-innermost,
 // [node][mf] with mf = 4*member + field, so a neighbour's state for all members
@@ -14,9 +14,10 @@
 // t's stencil).  Each unique row is gathered once per tile instead of once per
 // stencil slot.
 //
-// Precision (3xTF32): both operands are split x ~ hi + lo, each rounded to
-// nearest TF32 (|x - hi - lo| <= 2^-22 |x|), and D = A_hi B_hi + A_hi B_lo +
-// A_lo B_hi accumulates in FP32 in tensor memory.  The gathered states are
+// Precision: both operands are split x ~ hi + lo, and D = A_hi B_hi + A_hi B_lo
+// + A_lo B_hi accumulates in FP32 in tensor memory; the split is 3xTF32 (both
+// parts exact TF32, |x - hi - lo| <= 2^-22 |x|) or split BF16 (2^-17), see
+// ens_operands.cuh.  The gathered states are
 // centred on the state of one node of the tile (c[mf]) before the split;
 // c * sum_k W (row sums of the FP32 weights, summed in FP64) is added back in
 // the epilogue.  Derivative and hyperviscosity weights annihilate constants,
@@ -29,10 +30,10 @@
 //     (16-byte loads issued one chunk ahead into a ping-pong register set),
 //     centre and split them into the B operand, and write the matching A chunk
 //     densely, one 16-byte core row (4 chunk rows of one operator and node) per
-//     store, from a map of chunk rows to stencil slots; a ring of kEnsStages
-//     slots hands chunks to
-//   * the MMA warp: one thread issues 2 k-steps x 3 MMAs (128 x N x 8) per
-//     chunk into one of two TMEM accumulators and commits each chunk to the
+//     store, from a map of chunk rows to stencil slots; a ring of slots hands
+//     chunks to
+//   * the MMA warp: one thread issues the chunk's 3 products (128 x N x 16)
+//     into one of two TMEM accumulators and commits each chunk to the
 //     slot's "empty" barrier and each tile to the accumulator's "full" barrier;
 //   * 8 epilogue warps (two per TMEM lane quarter): tcgen05.ld the accumulator
 //     32 columns at a time, transpose (op, node) rows to (node, member) sets
@@ -44,40 +45,35 @@
 // abort flag that makes every role leave its loop.
 #pragma once
 
+#include "ens_operands.cuh"
 #include "stage_kernel.cuh"
 #include "tcgen05.cuh"
 
 namespace swe {
 
-constexpr int kEnsTileNodes = 32;   // nodes per tile (M = 4 * 32)
-constexpr int kEnsKc = 16;          // neighbour rows per pipeline chunk
-constexpr int kEnsStages = 3;       // ring slots
 constexpr int kEnsEpiWarps = 8;
 constexpr uint32_t kEnsWaitTries = 1u << 22;
 
-template <int MPC>
+template <int MPC, int PREC>
 struct EnsCfg {
+    using Op = ens::Operands<MPC, PREC>;
     static constexpr int kN = 4 * MPC;                     // MMA N: member-fields per CTA
-    static constexpr int kConvWarps = MPC / 8;             // (kEnsKc / 4) * MPC converter threads
+    static constexpr int kConvWarps = MPC / 8;             // 4 * MPC converter threads
     static constexpr int kConvThreads = 32 * kConvWarps;
     static constexpr int kMmaWarp = kConvWarps;
     static constexpr int kEpiWarp0 = kConvWarps + 1;
     static constexpr int kThreads = 32 * (kConvWarps + 1 + kEnsEpiWarps);
-    static constexpr int kOpp = 256 / kConvThreads;          // operator pairs per converter (A build)
-    static constexpr int kSboA = (kEnsKc / 4) * 128;       // A: 8-row groups of 16-byte core rows
-    static constexpr int kSboB = (kEnsKc / 4) * 128 + 16;  // B: odd 16-byte stride, conflict-free stores
-    static constexpr int kAHalf = (128 / 8) * kSboA;       // one of hi / lo
-    static constexpr int kBHalf = (kN / 8) * kSboB;
-    static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
+    static constexpr int kStages = Op::kStages;            // ring slots
+    static constexpr int kStageBytes = Op::kStageBytes;
     static constexpr int kXchStride = 36;                  // floats per (op, node) row; 9 x 16 B
     static constexpr int kXchGroupFloats = 4 * kEnsTileNodes * kXchStride;
     static constexpr int kTbRs = kEnsTileNodes * kPointStride * 4;   // per-tile buffer: PT, row sums, centre
     static constexpr int kTbCen = kTbRs + kEnsTileNodes * 16;
     static constexpr int kTileBuf = (kTbCen + kN * 4 + 127) / 128 * 128;
-    static constexpr int kSmem = kEnsStages * kStageBytes + 2 * kXchGroupFloats * 4 + 2 * kTileBuf;
+    static constexpr int kSmem = kStages * kStageBytes + 2 * kXchGroupFloats * 4 + 2 * kTileBuf;
     static constexpr int kTmemCols = (2 * kN <= 256) ? 256 : 512;
-    static_assert(kOpp == 1 || kOpp == 2, "A build covers 32 nodes x 4 row groups x 2 operator pairs");
-    static_assert(kN % 64 == 0 || kN == 32, "epilogue column chunks");
+    static_assert(kConvThreads == Op::kConvThreads, "converter thread count");
+    static_assert(kN % 64 == 0, "epilogue column chunks");
 };
 
 struct EnsArgs {
@@ -123,7 +119,6 @@ __device__ __forceinline__ bool named_and(int id, int nthreads, bool v) {
     return r != 0;
 }
 using tc::mbar_arrive;
-__device__ __forceinline__ float4 ldg_f4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
 // Bounded wait that also gives up as soon as another role has aborted.
 __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, volatile int* abort_s, int* err, int code) {
@@ -178,35 +173,20 @@ __device__ __forceinline__ Cursor next_cursor(Cursor p, const EnsArgs& a, int ha
     return p;
 }
 
-// Indices of one step (row ids for the B operand, stencil slots for the A operand).
-struct Fetch {
-    int4 idx = make_int4(-1, -1, -1, -1);
-    uint32_t jj = 0xffffffffu;
-    int u = -1;
-};
-
 // Streamed operands of one epilogue chunk (two (node, member) pairs per thread).
 struct EpiSet {
     float4 own[2], h32[2], d32[2];
     double hh[2], dh[2];
 };
 
-// Operands of one step held in registers.
-template <int OPP>
-struct ConvSet {
-    float4 x[4];           // 4 gathered rows x 4 member-fields
-    float4 cen;            // centre state of the same member-fields
-    int live;              // bit i: row i is a real row
-    float2 w[OPP][4];      // weights of the operator pairs for the 4 chunk rows
-};
-
 }  // namespace ens
 
-template <int MPC, int MODE>
-__global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(const EnsArgs a) {
-    using C = EnsCfg<MPC>;
+template <int MPC, int MODE, int PREC>
+__global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kernel(const EnsArgs a) {
+    using C = EnsCfg<MPC, PREC>;
+    using Op = typename C::Op;
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full_bar[kEnsStages], empty_bar[kEnsStages];
+    __shared__ __align__(8) uint64_t full_bar[C::kStages], empty_bar[C::kStages];
     __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], tile_bar[2], fin_bar;
     __shared__ uint32_t tmem_s;
     __shared__ int abort_s;
@@ -215,7 +195,7 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int halves = a.members / MPC;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kEnsStages; ++s) {
+        for (int s = 0; s < C::kStages; ++s) {
             tc::mbar_init(&full_bar[s], C::kConvWarps);
             tc::mbar_init(&empty_bar[s], 1);
         }
@@ -239,96 +219,28 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
 
     if (warp < C::kConvWarps) {
         // =============================== converters ===============================
-        const int ct = threadIdx.x;              // 0 .. 4*MPC-1
-        // B operand: rows 4kg..4kg+3 of each chunk x member-fields 4quad..4quad+3
-        const int quad = ct % MPC;
-        const int kg = ct / MPC;
-        // A operand: node t, rows 4akg..4akg+3 of each chunk, operator pairs opp0 .. opp0+kOpp-1
-        const int at = ct & 31;
-        const int akg = (ct >> 5) & 3;
-        const int opp0 = (ct >> 7) * C::kOpp;
+        const typename Op::Thread th(threadIdx.x);
         ens::Cursor cur = ens::first_cursor(a, halves);
-        ens::Fetch fx;                 // indices of the step after the current one
-        ens::ConvSet<C::kOpp> sa, sb;  // operands of the current / next step (ping-pong)
-        auto fetch_idx = [&](const ens::Cursor& p, ens::Fetch& f) {
-            if (!p.valid) return;
-            f.idx = __ldg(reinterpret_cast<const int4*>(a.rows + p.gc * kEnsKc + 4 * kg));
-            f.jj = __ldg(a.jmap + (p.gc * 4 + akg) * 32 + at);
-            f.u = p.u;
-        };
-        auto fetch_ops = [&](const ens::Cursor& p, const ens::Fetch& f, ens::ConvSet<C::kOpp>& o, const float4& cen_prev,
-                             int u_prev) {
+        typename Op::Fetch fx;         // indices of the step after the current one
+        typename Op::Set sa, sb;       // operands of the current / next step (ping-pong)
+        auto fetch_ops = [&](const ens::Cursor& p, const typename Op::Fetch& f, typename Op::Set& o,
+                             const typename Op::Set& prev, int u_prev) {
             if (!p.valid) return;
             const int tile = p.u / halves;
-            const long col = (long)(p.u % halves) * C::kN + 4 * quad;
-            const int r[4] = {f.idx.x, f.idx.y, f.idx.z, f.idx.w};
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                o.x[i] = r[i] >= 0 ? ens::ldg_f4(a.Kin + (long)r[i] * a.mf + col) : make_float4(0.f, 0.f, 0.f, 0.f);
-            o.live = (r[0] >= 0 ? 1 : 0) | (r[1] >= 0 ? 2 : 0) | (r[2] >= 0 ? 4 : 0) | (r[3] >= 0 ? 8 : 0);
-            o.cen = (p.u != u_prev) ? ens::ldg_f4(a.Kin + (long)__ldg(a.centre + tile) * a.mf + col) : cen_prev;
-            const long node = (long)tile * kEnsTileNodes + at;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const uint32_t j = (f.jj >> (8 * i)) & 0xffu;
-#pragma unroll
-                for (int q = 0; q < C::kOpp; ++q)
-                    o.w[q][i] = j != 0xffu ? __ldg(reinterpret_cast<const float2*>(a.W + node * 32 + j) + opp0 + q)
-                                           : make_float2(0.f, 0.f);
-            }
+            const long col = (long)(p.u % halves) * C::kN + th.col();
+            const float* cen_row = p.u != u_prev ? a.Kin + (long)__ldg(a.centre + tile) * a.mf : nullptr;
+            Op::fetch_ops(a.Kin, a.mf, col, a.W, (long)tile * kEnsTileNodes + th.at, cen_row, th, f, o, prev);
         };
         int g = 0;
-        auto step = [&](ens::ConvSet<C::kOpp>& o, ens::ConvSet<C::kOpp>& nx, int u_cur) -> bool {
+        auto step = [&](typename Op::Set& o, typename Op::Set& nx, int u_cur) -> bool {
             // look ahead: operands of the next step, indices of the one after
             ens::Cursor nxt = ens::next_cursor(cur, a, halves);
-            fetch_ops(nxt, fx, nx, o.cen, u_cur);
+            fetch_ops(nxt, fx, nx, o, u_cur);
             ens::Cursor nxt2 = ens::next_cursor(nxt, a, halves);
-            fetch_idx(nxt2, fx);
-            const int s = g % kEnsStages;
-            if (!ens::wait(&empty_bar[s], ((g / kEnsStages) & 1) ^ 1, abort_v, a.err, 3)) return false;
-            unsigned char* slot = smem + s * C::kStageBytes;
-            unsigned char* A_hi = slot;
-            unsigned char* A_lo = slot + C::kAHalf;
-            unsigned char* B_hi = slot + 2 * C::kAHalf;
-            unsigned char* B_lo = B_hi + C::kBHalf;
-            // A: one 16-byte core row (4 chunk rows) of (operator, node) per operator handled
-#pragma unroll
-            for (int q = 0; q < C::kOpp; ++q)
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int r = 32 * (2 * (opp0 + q) + h) + at;
-                    float4 hi, lo;
-                    tc::tf32_split(h ? o.w[q][0].y : o.w[q][0].x, hi.x, lo.x);
-                    tc::tf32_split(h ? o.w[q][1].y : o.w[q][1].x, hi.y, lo.y);
-                    tc::tf32_split(h ? o.w[q][2].y : o.w[q][2].x, hi.z, lo.z);
-                    tc::tf32_split(h ? o.w[q][3].y : o.w[q][3].x, hi.w, lo.w);
-                    const uint32_t off = (r >> 3) * C::kSboA + akg * 128 + (r & 7) * 16;
-                    *reinterpret_cast<float4*>(A_hi + off) = hi;
-                    *reinterpret_cast<float4*>(A_lo + off) = lo;
-                }
-            // B: 4 rows x 4 member-fields; each member-field's 4 rows are one 16-byte core row
-            {
-                const float xv[4][4] = {{o.x[0].x, o.x[0].y, o.x[0].z, o.x[0].w},
-                                        {o.x[1].x, o.x[1].y, o.x[1].z, o.x[1].w},
-                                        {o.x[2].x, o.x[2].y, o.x[2].z, o.x[2].w},
-                                        {o.x[3].x, o.x[3].y, o.x[3].z, o.x[3].w}};
-                const float cv[4] = {o.cen.x, o.cen.y, o.cen.z, o.cen.w};
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int nrow = 4 * quad + j;
-                    float4 hi, lo;
-                    float y[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) y[i] = ((o.live >> i) & 1) ? xv[i][j] - cv[j] : 0.f;
-                    tc::tf32_split(y[0], hi.x, lo.x);
-                    tc::tf32_split(y[1], hi.y, lo.y);
-                    tc::tf32_split(y[2], hi.z, lo.z);
-                    tc::tf32_split(y[3], hi.w, lo.w);
-                    const uint32_t off = (nrow >> 3) * C::kSboB + kg * 128 + (nrow & 7) * 16;
-                    *reinterpret_cast<float4*>(B_hi + off) = hi;
-                    *reinterpret_cast<float4*>(B_lo + off) = lo;
-                }
-            }
+            if (nxt2.valid) Op::fetch_idx(a.rows, a.jmap, nxt2.gc, th, fx);
+            const int s = g % C::kStages;
+            if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) return false;
+            Op::build(smem + s * C::kStageBytes, th, o);
             tc::fence_async_smem();
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&full_bar[s]);
@@ -337,10 +249,11 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
             return true;
         };
         if (cur.valid) {
-            ens::Fetch f0;
-            fetch_idx(cur, f0);
-            fetch_ops(cur, f0, sa, sa.cen, -1);
-            fetch_idx(ens::next_cursor(cur, a, halves), fx);
+            typename Op::Fetch f0;
+            Op::fetch_idx(a.rows, a.jmap, cur.gc, th, f0);
+            fetch_ops(cur, f0, sa, sa, -1);
+            const ens::Cursor n1 = ens::next_cursor(cur, a, halves);
+            if (n1.valid) Op::fetch_idx(a.rows, a.jmap, n1.gc, th, fx);
         }
         // two steps per trip so that the ping-pong sets never need copying
         while (cur.valid) {
@@ -353,7 +266,6 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
     } else if (warp == C::kMmaWarp) {
         // =============================== MMA issuer ===============================
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_tf32(128, C::kN);
             int g = 0, it = 0;
             bool ok = true;
             for (int u = blockIdx.x; u < a.units && ok; u += gridDim.x, ++it) {
@@ -364,21 +276,10 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
                 const int gc0 = __ldg(a.row_off + tile) / kEnsKc, gc1 = __ldg(a.row_off + tile + 1) / kEnsKc;
                 const uint32_t d = tmem + ab * C::kN;
                 for (int gc = gc0; gc < gc1; ++gc, ++g) {
-                    const int s = g % kEnsStages;
-                    if (!ens::wait(&full_bar[s], (g / kEnsStages) & 1, abort_v, a.err, 5)) { ok = false; break; }
+                    const int s = g % C::kStages;
+                    if (!ens::wait(&full_bar[s], (g / C::kStages) & 1, abort_v, a.err, 5)) { ok = false; break; }
                     tc::fence_after_sync();
-                    const uint32_t a_hi = tc::smem_u32(smem + s * C::kStageBytes), a_lo = a_hi + C::kAHalf;
-                    const uint32_t b_hi = a_hi + 2 * C::kAHalf, b_lo = b_hi + C::kBHalf;
-#pragma unroll
-                    for (int ks = 0; ks < kEnsKc / 8; ++ks) {
-                        const uint64_t dah = tc::smem_desc(a_hi + ks * 256, 128, C::kSboA);
-                        const uint64_t dal = tc::smem_desc(a_lo + ks * 256, 128, C::kSboA);
-                        const uint64_t dbh = tc::smem_desc(b_hi + ks * 256, 128, C::kSboB);
-                        const uint64_t dbl = tc::smem_desc(b_lo + ks * 256, 128, C::kSboB);
-                        tc::mma_tf32(d, dah, dbh, idesc, (gc > gc0 || ks > 0) ? 1u : 0u);
-                        tc::mma_tf32(d, dah, dbl, idesc, 1u);
-                        tc::mma_tf32(d, dal, dbh, idesc, 1u);
-                    }
+                    Op::issue(tc::smem_u32(smem + s * C::kStageBytes), d, gc == gc0);
                     tc::mma_commit(&empty_bar[s]);
                 }
                 if (!ok) break;
@@ -400,8 +301,8 @@ __global__ void __launch_bounds__(EnsCfg<MPC>::kThreads, 1) ens_stage_kernel(con
         const int grp = e >> 2;                  // column chunks alternate between the two groups
         const int op = warp & 3;                 // TMEM lane quarter = operator
         const int gt = et & 127;                 // thread within the group
-        float* xch = reinterpret_cast<float*>(smem + kEnsStages * C::kStageBytes) + grp * C::kXchGroupFloats;
-        unsigned char* tbuf = smem + kEnsStages * C::kStageBytes + 2 * C::kXchGroupFloats * 4;
+        float* xch = reinterpret_cast<float*>(smem + C::kStages * C::kStageBytes) + grp * C::kXchGroupFloats;
+        unsigned char* tbuf = smem + C::kStages * C::kStageBytes + 2 * C::kXchGroupFloats * 4;
         const int members = a.members;
         const float c32 = (float)a.c;
         constexpr bool kHD = MODE == kStage1 || MODE == kStage2 || MODE == kStage3;

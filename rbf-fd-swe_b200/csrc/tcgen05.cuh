@@ -1,6 +1,6 @@
 // Thin inline-PTX wrappers for the sm_100a pieces the ensemble kernel uses:
-// tensor memory (TMEM) allocation, tcgen05.mma kind::tf32 with shared-memory
-// operands, tcgen05.commit to an mbarrier, tcgen05.ld of the accumulator, and
+// tensor memory (TMEM) allocation, tcgen05.mma kind::tf32 and kind::f16 (BF16)
+// with shared-memory operands, tcgen05.commit to an mbarrier, tcgen05.ld of the accumulator, and
 // bounded mbarrier waits.  Descriptor formats follow the PTX ISA's tcgen05
 // "shared memory descriptor" and "instruction descriptor" tables.
 #pragma once
@@ -51,6 +51,25 @@ __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
            | (2u << 7)               // A format TF32
            | (2u << 10)              // B format TF32
            | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Instruction descriptor for kind::f16 with BF16 A and B (the same type, as kind::f16
+// requires), FP32 accumulator, both operands K-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4)                 // D format F32
+           | (1u << 7)               // A format BF16
+           | (1u << 10)              // B format BF16
+           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[smem] * B[smem], BF16 operands, K = 16
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
 }
 
 // D[tmem] (+)= A[smem] * B[smem]

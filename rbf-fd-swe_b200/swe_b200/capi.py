@@ -62,6 +62,7 @@ def load() -> ctypes.CDLL:
     lib.swe_cuda_select_kernel.argtypes = [i]
     lib.swe_cuda_kernel_info.argtypes = [vp]
     lib.swe_ens_init.argtypes = [i, i, i, d, d] + [vp] * 14
+    lib.swe_ens_set_precision.argtypes = [i]
     for name in ("swe_ens_set_state", "swe_ens_get_state", "swe_ens_tune", "swe_ens_config",
                  "swe_ens_invariants", "swe_ens_last_timings"):
         getattr(lib, name).argtypes = [vp]
@@ -274,11 +275,20 @@ class Ensemble:
     def use_variant(self, tile_nodes: int, members_per_cta: int) -> None:
         check("swe_ens_use_variant", self.lib.swe_ens_use_variant(tile_nodes, members_per_cta))
 
+    PRECISIONS = ("tf32x3", "bf16x3")
+
+    def set_precision(self, name: str) -> None:
+        """Stencil products in 3xTF32 ("tf32x3", the default) or split BF16 ("bf16x3")."""
+        if name not in self.PRECISIONS:
+            raise ValueError(f"precision must be one of {self.PRECISIONS}, got {name!r}")
+        check("swe_ens_set_precision", self.lib.swe_ens_set_precision(self.PRECISIONS.index(name)))
+
     def config(self) -> dict:
-        out = np.zeros(4, dtype=np.int32)
+        out = np.zeros(5, dtype=np.int32)
         check("swe_ens_config", self.lib.swe_ens_config(_p(out)))
         return {"tile_nodes": int(out[0]), "members_per_cta": int(out[1]),
-                "max_rows_per_tile": int(out[2]), "tiles": int(out[3])}
+                "max_rows_per_tile": int(out[2]), "tiles": int(out[3]),
+                "precision": self.PRECISIONS[int(out[4])]}
 
     def invariants(self) -> np.ndarray:
         out = np.zeros((self.members, 2))

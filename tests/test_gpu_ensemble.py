@@ -1,12 +1,13 @@
-"""Batched-ensemble form on the GPU (tcgen05 3xTF32), through the C ABI.
+"""Batched-ensemble form on the GPU (tcgen05, 3xTF32 or split BF16), through the C ABI.
 
-Bars (FP32-level arithmetic checked against the FP64 oracle):
-* eval_rhs of every member: condition-normalised error <= 4e-6 (a few FP32
-  ulps of the term scale, conftest.cond_err) in every kernel variant;
+Bars (checked against the FP64 oracle):
+* eval_rhs of every member: condition-normalised error (conftest.cond_err, the
+  error over the term scale) <= 4e-6 for 3xTF32 (a few FP32 ulps) and <= 5e-5
+  for split BF16 (three products each within 2^-17 of |w| |x - c|, |x - c| <=
+  2 max|x|: 6 * 2^-17 = 4.6e-5), in every kernel variant;
 * 20 RK4 steps of every member against the FP64 oracle: per-field max-norm
-  relative error within 5x of what the plain FP32 restatement of the
-  reference reaches on the same member (FP32-class accuracy; measured 1.7-4.3x,
-  the tensor core's FP32 accumulation being the difference);
+  relative error within 5x (3xTF32, FP32-class) or 120x (split BF16) of what
+  the plain FP32 restatement of the reference reaches on the same member;
 * a member's result does not depend on the other members (32- and 64-member
   runs agree bitwise for the members they share);
 * FP64 invariants of the device state equal the oracle's sums of the same state.
@@ -40,23 +41,37 @@ def _members(m, members, seed0=100):
     return np.stack([gen.perturb_h(m.H_init, seed0 + b) for b in range(members)])
 
 
+COND_BOUND = {"tf32x3": 4e-6, "bf16x3": 5e-5}
+
+
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3"])
 @pytest.mark.parametrize("tile,mpc", VARIANTS)
-def test_eval_rhs_every_variant(ens, model_l4, tile, mpc):
+def test_eval_rhs_every_variant(ens, model_l4, tile, mpc, prec):
     m = model_l4
     ens.init(m, 64)
+    ens.set_precision(prec)
     ens.use_variant(tile, mpc)
+    assert ens.config()["precision"] == prec
     K = _members(m, 64)
     F = ens.eval_rhs(K)
     port = oracle.Port(m, "fp64")
     worst = 0.0
     for b in (0, 1, 31, 32, 63):
         worst = max(worst, cond_err(F[b], port.eval_rhs(K[b]), m, K[b]))
-    assert worst <= 4e-6, worst
+    print(f"eval_rhs cond_err {prec} mpc={mpc}: {worst:.3e}")
+    assert worst <= COND_BOUND[prec], worst
 
 
-def test_steps_match_fp64_oracle(ens, model_l4):
+# 3xTF32 is FP32-class (measured 1.3-2.9x the FP32 restatement's error after 20 steps);
+# split BF16 carries 2^-17 operand splits (measured 17-57x); the bars keep ~2x margin.
+STEP_FACTOR = {"tf32x3": 5.0, "bf16x3": 120.0}
+
+
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3"])
+def test_steps_match_fp64_oracle(ens, model_l4, prec):
     m = model_l4
     ens.init(m, 64)
+    ens.set_precision(prec)
     ens.tune()
     H0 = _members(m, 64)
     ens.set_state(H0)
@@ -68,7 +83,16 @@ def test_steps_match_fp64_oracle(ens, model_l4):
         want = port.run(H0[b], 20)
         fp32_err = rel_err(port32.run(H0[b], 20), want)
         err = rel_err(H[b], want)
-        assert (err <= 5 * fp32_err).all(), (b, err, fp32_err)
+        print(f"20 steps {prec} member {b}: err {err} fp32 {fp32_err} ratio {err / fp32_err}")
+        assert (err <= STEP_FACTOR[prec] * fp32_err).all(), (b, err, fp32_err)
+
+
+def test_rejects_bad_precision(ens, model_l4):
+    ens.init(model_l4, 32)
+    with pytest.raises(capi.SweError):
+        capi.check("swe_ens_set_precision", ens.lib.swe_ens_set_precision(2))
+    with pytest.raises(ValueError):
+        ens.set_precision("fp16")
 
 
 def test_members_are_independent(ens, model_l4):
