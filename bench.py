@@ -62,6 +62,55 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+# ---- replicas (one process per GPU, no data-path collective) --------------------------------
+
+def world_info():
+    """(rank, local_rank, world_size) from the torchrun environment (1 process if unset)."""
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def init_replicas(backend: str = "nccl", timeout_s: float = 120.0) -> None:
+    """Process group for the timing reductions only; a short timeout ends a rank that waits
+    for a peer which died, instead of hanging."""
+    import datetime
+
+    import torch.distributed as dist
+    if world_info()[2] > 1 and not dist.is_initialized():
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+
+def sync_ranks() -> None:
+    """Barrier across replicas (no-op for one process)."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.barrier()
+
+
+def max_over_ranks(x: float, device="cpu") -> float:
+    """The job's time is the slowest replica's: max over ranks of a per-rank time."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: float, t_per_rank: float, device="cpu") -> float:
+    """Whole-job throughput of N replicas: all ranks' units over the slowest rank's time."""
+    import torch.distributed as dist
+    world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
+    return units_per_rank * world / max_over_ranks(t_per_rank, device)
+
+
+def finish_replicas() -> None:
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.destroy_process_group()
+
+
 def measured_peak_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -219,13 +268,9 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
 
     from swe_b200 import capi, gen
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    rank, local, world = world_info()
     torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    init_replicas()
     d, m, pm = build_workload(level, "fp64", device=f"cuda:{local}")
     N = d.N
     H0 = np.stack([gen.perturb_h(m.H_init, 1000 + b) for b in range(members)])
@@ -247,6 +292,8 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
     with ClockSampler(local) as clocks:
         clocks.wait_for(1, 5.0)
         first = clocks.count()
+        sync_ranks()
+        torch.cuda.synchronize()
         with torch.cuda.stream(stream):
             for s in range(args.steps):
                 flush.zero_()
@@ -254,6 +301,7 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
                 ens.step(1)
                 stops[s].record(stream)
         torch.cuda.synchronize()
+        sync_ranks()
         launches = capi.kernel_launches() - launches0
         t_total = sum(a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops))
 
@@ -263,6 +311,7 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
             ens.sync()
         clocks.wait_for(first + 3, 5.0, keep_busy=busy)
     ens.sync()
+    t_total = max_over_ranks(t_total, f"cuda:{local}")
     member_steps = members * args.steps * world / t_total
     t_stage = t_total / (4 * args.steps)
     ens_bytes = ENS_SHARED_BYTES + members * ENS_MEMBER_BYTES
@@ -341,19 +390,17 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
             "state_finite": bool(np.isfinite(Hout).all()),
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    finish_replicas()
 
 
 def run_serving(args, desc):
     """Seeded Poisson stream of forecast requests through the serving form."""
     from swe_b200 import capi, gen, swe_input
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
+    rank, local, world = world_info()
     import torch
     torch.cuda.set_device(local)
+    init_replicas()
     rng = np.random.default_rng(args.seed)
     levels = [4, 5, 6, 7]
     models = {}
@@ -393,11 +440,12 @@ def run_serving(args, desc):
     lat = np.array([res[r][2] for r in ids])
     wait_admit = np.array([res[r][1] for r in ids])
     member_steps = sum(mb * st for lv, mb, st, seed in reqs)
+    wall = max_over_ranks(wall, f"cuda:{local}")      # each replica serves its own stream
     node_stages = sum(4.0 * models[lv].N * mb * st for lv, mb, st, seed in reqs)
     if rank == 0:
         line = {
             "metric": "serving: aggregate member-steps/s with p50/p99 request latency",
-            "value": member_steps / wall, "unit": "member-steps/s", "n_gpus": 1, "steps": None,
+            "value": member_steps * world / wall, "unit": "member-steps/s", "n_gpus": world, "steps": None,
             "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded request stream",
             "config": {"workload": args.workload, "description": desc, "requests": nreq,
@@ -406,12 +454,13 @@ def run_serving(args, desc):
                           "max": float(lat.max())},
             "admission_wait_s": {"p50": float(np.percentile(wait_admit, 50)),
                                  "p99": float(np.percentile(wait_admit, 99))},
-            "node_stage_updates_per_s": node_stages / wall,
+            "node_stage_updates_per_s": node_stages * world / wall,
             "wall_s": wall, "server": stats,
             "gpu_launches": int(capi.kernel_launches() - launches0),
             "state_finite": bool(all(np.isfinite(o).all() for o in outs)),
         }
         print(json.dumps(line), flush=True)
+    finish_replicas()
 
 
 def main():
@@ -440,16 +489,12 @@ def main():
         return run_serving(args, desc)
 
     import torch
-    import torch.distributed as dist
 
     from swe_b200 import capi
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, local, world = world_info()
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    init_replicas()
 
     d, m, pm = build_workload(level, prec, device=f"cuda:{local}")
     N = d.N
@@ -469,8 +514,7 @@ def main():
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     launches0 = capi.kernel_launches()
-    if world > 1:
-        dist.barrier()
+    sync_ranks()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         clocks.wait_for(1, 5.0)
@@ -482,6 +526,7 @@ def main():
                 plain.step(1)
                 stops[s].record(stream)
         torch.cuda.synchronize()
+        sync_ranks()
         launches = capi.kernel_launches() - launches0
         t_steps = [a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops)]
         t_total = float(sum(t_steps))
@@ -502,10 +547,7 @@ def main():
                     plain.rk_substep(st)
         k_time, k_launches, _ = plain.timings()
         plain.set_timing(False)
-    if world > 1:
-        t = torch.tensor([t_total], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total = float(t.item())
+    t_total = max_over_ranks(t_total, f"cuda:{local}")
     value = 4.0 * N * args.steps * world / t_total
 
     # ---- end to end through the C ABI with pinned host buffers --------------------------
@@ -517,18 +559,14 @@ def main():
         plain.set_state_ptr(H_host.data_ptr())
         plain.step(1)
         plain.get_state_ptr(H_out.data_ptr())
-    if world > 1:
-        dist.barrier()
+    sync_ranks()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         plain.set_state_ptr(H_host.data_ptr())
         plain.step(1)
         plain.get_state_ptr(H_out.data_ptr())     # synchronises
     t_e2e = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([t_e2e], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = max_over_ranks(t_e2e, f"cuda:{local}")
     e2e = 4.0 * N * e2e_steps * world / t_e2e
     finite = bool(np.isfinite(H_out.numpy()).all())
 
@@ -570,8 +608,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     plain.finalize()
-    if world > 1:
-        dist.destroy_process_group()
+    finish_replicas()
 
 
 if __name__ == "__main__":
