@@ -56,6 +56,17 @@ ALG_BYTES = {"fp64": 1396, "fp32": 760}      # per node-stage (FP64: 4*31*8+31*4
 ENS_SHARED_BYTES = 4 * 31 * 4 + 31 * 4 + 17 * 4
 ENS_MEMBER_BYTES = 4 * 4 + 14 * 4 + 4
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) per launch of the dominant kernel, from ncu captures of the same
+# command (dram__bytes_read.sum + dram__bytes_write.sum, averaged over the captured launches);
+# the profile summaries under profiles/ give the commands.
+TRAFFIC_BYTES = {
+    "plain_fp64_n40962": 57.09e6,       # swe::stage_kernel (register form), 8 launches, stages 0-3
+    "plain_fp64_n163842": 233.53e6,     # swe::stage_tma_kernel, 12 launches of the timed region
+    "plain_fp64_n655362": 945.25e6,     # swe::stage_tma_kernel, 12 launches
+    "plain_fp32_n655362": 512.92e6,     # swe::stage_tma_kernel, 12 launches
+    "ens_tf32_n163842_b64": 1041.20e6,  # swe::ens_stage_kernel<64, stage, 3xTF32>, 12 launches
+    "ens_bf16_n163842_b64": 1041.46e6,  # swe::ens_stage_kernel<64, stage, BF16>, 12 launches
+}
 
 
 def log(*a):
@@ -294,6 +305,7 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
         first = clocks.count()
         sync_ranks()
         torch.cuda.synchronize()
+        torch.cuda.profiler.start()
         with torch.cuda.stream(stream):
             for s in range(args.steps):
                 flush.zero_()
@@ -301,6 +313,7 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
                 ens.step(1)
                 stops[s].record(stream)
         torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
         sync_ranks()
         launches = capi.kernel_launches() - launches0
         t_total = sum(a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops))
@@ -326,7 +339,7 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
         ens.set_state(H0)
         ens.step(1)
         Hout = ens.get_state()
-    t_e2e = time.perf_counter() - t0
+    t_e2e = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
     nbytes = H0.nbytes
 
     # plain FP64 on the same grid: member-steps/s = steps/s of one state
@@ -379,11 +392,11 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
             "ratio_vs_plain_fp64": member_steps / plain_steps,
             "h_err_vs_fp64": {"steps": args.err_steps, "members": err_members,
                               "max_norm_rel_per_field_max": errs.max(0).tolist()},
-            "e2e": {"value": members * e2e_steps / t_e2e, "unit": "member-steps/s",
+            "e2e": {"value": members * e2e_steps * world / t_e2e, "unit": "member-steps/s",
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                         "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(args.workload), "peak_source": peak_kind,
                          "kernel": "swe::ens_stage_kernel", "kernel_us": round(t_stage * 1e6, 2),
                          "alg_bytes_per_node_stage": ens_bytes},
             "clocks": clocks.summary(first),
@@ -519,6 +532,7 @@ def main():
     with ClockSampler(local) as clocks:
         clocks.wait_for(1, 5.0)
         first_sample = clocks.count()
+        torch.cuda.profiler.start()                 # a profiler run with --profile-from-start off sees this loop only
         with torch.cuda.stream(stream):
             for s in range(args.steps):
                 flush.zero_()                       # L2 flush between timed steps (not timed)
@@ -526,19 +540,14 @@ def main():
                 plain.step(1)
                 stops[s].record(stream)
         torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
         sync_ranks()
         launches = capi.kernel_launches() - launches0
         t_steps = [a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops)]
         t_total = float(sum(t_steps))
 
-        # The timed region is far shorter than nvidia-smi's 200 ms period: keep
-        # the same step loop running (untimed) until 3 samples cover it.
-        def busy():
-            for _ in range(200):
-                plain.step(1)
-            plain.sync()
-        clocks.wait_for(first_sample + 3, 5.0, keep_busy=busy)
-        # ---- per-stage kernel durations for the roofline (same stream, events) -------
+        # ---- per-stage kernel durations for the roofline (same stream, events), right
+        # after the timed steps and at the same clocks --------------------------------------
         plain.set_timing(True)
         with torch.cuda.stream(stream):
             for s in range(max(3, args.steps // 4)):
@@ -547,6 +556,14 @@ def main():
                     plain.rk_substep(st)
         k_time, k_launches, _ = plain.timings()
         plain.set_timing(False)
+
+        # The timed region is far shorter than nvidia-smi's 200 ms period: keep
+        # the same step loop running (untimed) until 3 samples cover it.
+        def busy():
+            for _ in range(200):
+                plain.step(1)
+            plain.sync()
+        clocks.wait_for(first_sample + 3, 5.0, keep_busy=busy)
     t_total = max_over_ranks(t_total, f"cuda:{local}")
     value = 4.0 * N * args.steps * world / t_total
 
@@ -576,7 +593,7 @@ def main():
     achieved = ALG_BYTES[prec] * N / t_kernel / 1e9
     kinfo = plain.kernel_info()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(args.workload), "peak_source": peak_kind,
                 "kernel": "swe::stage_tma_kernel" if kinfo["in_use"] == "pipelined" else "swe::stage_kernel",
                 "kernel_us": round(t_kernel * 1e6, 2), "alg_bytes_per_node_stage": ALG_BYTES[prec],
                 "kernel_choice": kinfo}

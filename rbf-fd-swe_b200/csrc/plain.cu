@@ -154,8 +154,9 @@ struct Plain {
     int* err = nullptr;             // pipelined kernel: bounded-wait error word
     bool tma_ok = false;            // pipelined kernel set up
     int kernel_choice = 0;          // 0 = bulk-copy pipelined kernel, 1 = register-streaming kernel
-    float tune_us[2] = {0.f, 0.f};  // eval-mode launch time of each kernel at init
-    int ntiles = 0, grid_tma = 0;
+    float tune_us[2] = {0.f, 0.f};  // eval-mode launch time of each kernel at init (pipelined: best tile)
+    int tma_tile = 64;              // pipelined kernel: nodes per tile (64: 1 CTA/SM, 32: 2 CTAs/SM)
+    int sms = 0;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int grid = 0;
@@ -181,6 +182,7 @@ struct Plain {
         err = nullptr;
         tma_ok = false;
         kernel_choice = 0;
+        tma_tile = 64;
         for (auto e : ev) cudaEventDestroy(e);
         ev.clear();
         ev_used = 0;
@@ -232,19 +234,28 @@ struct Plain {
 
     bool use_tma() const { return tma_ok && kernel_choice == 0; }
 
+    template <typename T, int TILE>
+    void launch_tma(const StageArgs<T>& a, int mode) {
+        using Sh = TmaShape<TILE>;
+        const int ntiles = (n + TILE - 1) / TILE;
+        const TmaArgs<T> ta{a, ntiles, err};
+        const int g = std::max(1, std::min(ntiles, sms * Sh::kCtasPerSm));
+        const int sm = TmaLayout<T, TILE>::kSmem;
+        switch (mode) {
+            case 0: stage_tma_kernel<T, kStage0, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
+            case 1: stage_tma_kernel<T, kStage1, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
+            case 2: stage_tma_kernel<T, kStage2, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
+            case 3: stage_tma_kernel<T, kStage3, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
+            default: stage_tma_kernel<T, kEvalOnly, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
+        }
+    }
+
     template <typename T>
     void launch_t(int mode) {
         const StageArgs<T> a = args<T>(mode);
         if (use_tma()) {
-            TmaArgs<T> ta{a, ntiles, err};
-            const int sm = TmaLayout<T>::kSmem;
-            switch (mode) {
-                case 0: stage_tma_kernel<T, kStage0><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
-                case 1: stage_tma_kernel<T, kStage1><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
-                case 2: stage_tma_kernel<T, kStage2><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
-                case 3: stage_tma_kernel<T, kStage3><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
-                default: stage_tma_kernel<T, kEvalOnly><<<grid_tma, kTmaThreads, sm, stream>>>(ta); break;
-            }
+            if (tma_tile == 32) launch_tma<T, 32>(a, mode);
+            else launch_tma<T, 64>(a, mode);
             return;
         }
         switch (mode) {
@@ -291,6 +302,17 @@ struct Plain {
 
 static Plain g_plain;
 
+template <typename T, int TILE>
+static int set_tma_attrs() {
+    const int sm = TmaLayout<T, TILE>::kSmem;
+    SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage0, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage1, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage2, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage3, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kEvalOnly, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    return SWE_OK;
+}
+
 template <typename T>
 static int upload_static(Plain& P, const void* x, const void* y, const void* z, const void* f, const void* ghm,
                          const void* pu, const void* pv, const void* pw, const void* gg, const int* idx,
@@ -309,15 +331,10 @@ static int upload_static(Plain& P, const void* x, const void* y, const void* z, 
     SWE_CUDA_TRY(cudaMemcpy(P.PT, pbuf.data(), pbuf.size() * sizeof(T), cudaMemcpyHostToDevice));
     P.tma_ok = true;
     {
-        P.ntiles = (P.n + kTmaTile - 1) / kTmaTile;
         SWE_CUDA_TRY(cudaMalloc(&P.err, sizeof(int)));
         SWE_CUDA_TRY(cudaMemset(P.err, 0, sizeof(int)));
-        const int sm = TmaLayout<T>::kSmem;
-        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kStage3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(stage_tma_kernel<T, kEvalOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_TRY((set_tma_attrs<T, 64>()));
+        SWE_TRY((set_tma_attrs<T, 32>()));
     }
     return SWE_OK;
 }
@@ -435,19 +452,21 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
         SWE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel<float, kStage1>, kStageThreads, 0));
     const int want = ceil_div(P.n, 4 * kStageWarps);
     P.grid = std::max(1, std::min(want, sms * std::max(per_sm, 1)));
-    P.grid_tma = std::max(1, std::min(P.ntiles, sms));
+    P.sms = sms;
     P.ready = true;
-    // The two stage kernels do identical arithmetic; keep the faster one for
-    // this patch (the pipelined kernel wins once every SM has many tiles).
+    // The stage kernels do identical arithmetic; keep the fastest for this patch:
+    // the register kernel, or the pipelined kernel with 64- or 32-node tiles (the
+    // pipelined kernel wins once every SM has many tiles).
     {
         cudaEvent_t e0, e1;
         SWE_CUDA_TRY(cudaEventCreate(&e0));
         SWE_CUDA_TRY(cudaEventCreate(&e1));
         SWE_CUDA_TRY(cudaMemsetAsync(P.Kx, 0, srow, P.stream));
-        float best = 1e30f;
-        int best_k = 0;
-        for (int kc = 0; kc < 2; ++kc) {
-            P.kernel_choice = kc;
+        const int cand_kernel[3] = {0, 0, 1}, cand_tile[3] = {64, 32, 64};
+        float us_c[3] = {0.f, 0.f, 0.f};
+        for (int c = 0; c < 3; ++c) {
+            P.kernel_choice = cand_kernel[c];
+            P.tma_tile = cand_tile[c];
             for (int w = 0; w < 2; ++w) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
             SWE_CUDA_TRY(cudaEventRecord(e0, P.stream));
             for (int r = 0; r < 5; ++r) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
@@ -456,13 +475,16 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
             SWE_CUDA_TRY(cudaGetLastError());
             float ms = 0.f;
             SWE_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-            P.tune_us[kc] = ms * 1e3f / 5.f;
-            if (ms < best) { best = ms; best_k = kc; }
+            us_c[c] = ms * 1e3f / 5.f;
         }
-        count_launch(14);
+        count_launch(21);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        P.kernel_choice = best_k;
+        // the pipelined kernel keeps its faster tile, also when the register kernel wins
+        P.tma_tile = us_c[1] < us_c[0] ? 32 : 64;
+        P.tune_us[0] = std::min(us_c[0], us_c[1]);
+        P.tune_us[1] = us_c[2];
+        P.kernel_choice = P.tune_us[1] < P.tune_us[0] ? 1 : 0;
         SWE_TRY(check_tma_err());
     }
     if ((st = P.build_graph()) != SWE_OK) return st;
@@ -553,10 +575,17 @@ int swe_cuda_sync(void) {
 
 int swe_cuda_select_kernel(int which) {
     SWE_TRY(require_ready());
-    if (which != 0 && which != 1) { set_error("swe_cuda_select_kernel: 0 (bulk-copy pipeline) or 1"); return SWE_ERR_ARG; }
+    if (which < 0 || which > 3) {
+        set_error("swe_cuda_select_kernel: 0 (pipelined), 1 (register), 2 / 3 (pipelined, 64 / 32-node tiles), got %d",
+                  which);
+        return SWE_ERR_ARG;
+    }
     Plain& P = g_plain;
+    if (which != 1 && !P.tma_ok) { set_error("swe_cuda_select_kernel: the pipelined kernel is not set up"); return SWE_ERR_STATE; }
     SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
-    P.kernel_choice = which;
+    P.kernel_choice = which == 1 ? 1 : 0;
+    if (which == 2) P.tma_tile = 64;
+    if (which == 3) P.tma_tile = 32;
     if (P.graph) cudaGraphExecDestroy(P.graph);
     P.graph = nullptr;
     return P.build_graph();
@@ -566,7 +595,7 @@ int swe_cuda_kernel_info(int* out) {
     SWE_TRY(require_ready());
     if (!out) { set_error("null out"); return SWE_ERR_ARG; }
     out[0] = g_plain.use_tma() ? 0 : 1;
-    out[1] = g_plain.tma_ok ? 1 : 0;
+    out[1] = g_plain.tma_ok ? g_plain.tma_tile : 0;
     out[2] = (int)(g_plain.tune_us[0] * 1000.f);   // nanoseconds per eval launch, pipelined
     out[3] = (int)(g_plain.tune_us[1] * 1000.f);   // register-streaming
     return SWE_OK;

@@ -1,19 +1,20 @@
 // Fused RK4 stage kernel, bulk-copy pipelined (plain form, FP64 / FP32).
 //
 // Same math and lane split as stage_kernel.cuh, restructured around B200's
-// bulk copy engine.  A persistent CTA per SM runs one producer warp and 16
-// consumer warps over tiles of 64 consecutive nodes.  For every tile the
-// producer issues six cp.async.bulk copies (global -> shared, completing on an
-// mbarrier) into one of kStages ring slots: the tile's packed weights
-// (64 x 1 KB in FP64), packed stencil indices, pointwise records, own state
-// rows, and the H / D rows for stages 1-3 -- every contiguous per-node stream
-// of the stage.  Consumers wait on the slot's mbarrier, gather the neighbour
-// states through L1/L2 (the state arrays are L2-resident; a tile's neighbours
-// are scattered rows, which suits plain loads better than many small bulk
-// copies), run the stencil sums, reduction and pointwise/RK combine with
-// every other operand in shared memory, store their outputs and release the
-// slot.  Every wait is bounded; a timeout sets an error word and the kernel
-// drains its outstanding copies and returns.
+// bulk copy engine.  Persistent CTAs run one producer warp and TILE/4 consumer
+// warps over tiles of TILE consecutive nodes: 64-node tiles with one CTA per SM,
+// or 32-node tiles with two CTAs per SM (two producers in flight per SM; the
+// library times both at init).  For every tile the producer issues six
+// cp.async.bulk copies (global -> shared, completing on an mbarrier) into one
+// of kStages ring slots: the tile's packed weights (TILE x 1 KB in FP64),
+// packed stencil indices, pointwise records, own state rows, and the H / D rows
+// for stages 1-3 -- every contiguous per-node stream of the stage.  Consumers
+// wait on the slot's mbarrier, gather the neighbour states through L1/L2 (the
+// state arrays are L2-resident; a tile's neighbours are scattered rows, which
+// suits plain loads better than many small bulk copies), run the stencil sums,
+// reduction and pointwise/RK combine with every other operand in shared memory,
+// store their outputs and release the slot.  Every wait is bounded; a timeout
+// sets an error word and the kernel drains its outstanding copies and returns.
 #pragma once
 
 #include "stage_kernel.cuh"
@@ -21,9 +22,13 @@
 
 namespace swe {
 
-constexpr int kTmaTile = 64;           // nodes per tile
-constexpr int kTmaConsumerWarps = kTmaTile / 4;
-constexpr int kTmaThreads = 32 * (kTmaConsumerWarps + 1);
+template <int TILE>
+struct TmaShape {
+    static constexpr int kTile = TILE;                     // nodes per tile
+    static constexpr int kConsumerWarps = TILE / 4;        // 4 nodes per warp
+    static constexpr int kThreads = 32 * (kConsumerWarps + 1);
+    static constexpr int kCtasPerSm = 64 / TILE;
+};
 constexpr uint32_t kTmaWaitTries = 1u << 24;
 
 namespace tma {
@@ -32,8 +37,9 @@ __device__ __forceinline__ void arrive_expect_tx(uint64_t* b, uint32_t tx) { tc:
 __device__ __forceinline__ void arrive(uint64_t* b) { tc::mbar_arrive(b); }
 }  // namespace tma
 
-template <typename T>
+template <typename T, int TILE>
 struct TmaLayout {
+    static constexpr int kTmaTile = TILE;
     static constexpr int kWn = kSlots * 4 * (int)sizeof(T);     // weight bytes per node
     static constexpr int kIdxn = kSlots * 4;                      // index bytes per node
     static constexpr int kPtn = kPointStride * (int)sizeof(T);   // pointwise bytes per node
@@ -41,7 +47,7 @@ struct TmaLayout {
     static constexpr int oW = 0, oIdx = oW + kTmaTile * kWn, oPt = oIdx + kTmaTile * kIdxn,
                          oOwn = oPt + kTmaTile * kPtn, oH = oOwn + kTmaTile * kRow, oD = oH + kTmaTile * kRow;
     static constexpr int kSlotBytes = ((oD + kTmaTile * kRow) + 127) / 128 * 128;
-    static constexpr int kStages = (sizeof(T) == 8) ? 2 : 4;
+    static constexpr int kStages = (sizeof(T) == 8) ? 2 : 4;   // 180 KB (FP64) / 196 KB (FP32) per SM
     static constexpr int kSmem = kStages * kSlotBytes;
 };
 
@@ -52,9 +58,12 @@ struct TmaArgs {
     int* err;
 };
 
-template <typename T, int MODE>
-__global__ void __launch_bounds__(kTmaThreads, 1) stage_tma_kernel(const TmaArgs<T> ta) {
-    using Lay = TmaLayout<T>;
+template <typename T, int MODE, int TILE>
+__global__ void __launch_bounds__(TmaShape<TILE>::kThreads, TmaShape<TILE>::kCtasPerSm)
+    stage_tma_kernel(const TmaArgs<T> ta) {
+    using Lay = TmaLayout<T, TILE>;
+    constexpr int kTmaTile = TILE;
+    constexpr int kTmaConsumerWarps = TmaShape<TILE>::kConsumerWarps;
     const StageArgs<T>& a = ta.s;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[Lay::kStages], empty[Lay::kStages];

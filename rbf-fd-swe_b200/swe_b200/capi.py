@@ -213,7 +213,7 @@ class Plain:
         out = np.zeros(4, dtype=np.int32)
         check("swe_cuda_kernel_info", self.lib.swe_cuda_kernel_info(_p(out)))
         return {"in_use": "pipelined" if out[0] == 0 else "register", "pipelined_available": bool(out[1]),
-                "tune_us": {"pipelined": out[2] / 1e3, "register": out[3] / 1e3}}
+                "pipelined_tile": int(out[1]), "tune_us": {"pipelined": out[2] / 1e3, "register": out[3] / 1e3}}
 
     def invariants(self) -> np.ndarray:
         out = np.zeros(2)

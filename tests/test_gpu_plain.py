@@ -179,21 +179,23 @@ def test_pipelined_and_register_kernels_agree_bitwise(plain, prec):
     _, d = generated_input(6)
     m, _ = layout.prepare(swe_input.to_model(d), use_rcm=True, simd_length=32)
     plain.init_model(m, prec)
-    plain.select_kernel(0)
-    assert plain.kernel_info()["in_use"] == "pipelined"
     dt = np.float64 if prec == "fp64" else np.float32
     K = _perturbed(m.H_init).astype(dt)
-    F0 = plain.eval_rhs(K)
-    plain.set_state(m.H_init.astype(dt))
-    plain.step(7)
-    H0 = plain.get_state()
-    plain.select_kernel(1)
-    assert plain.kernel_info()["in_use"] == "register"
-    F1 = plain.eval_rhs(K)
-    plain.set_state(m.H_init.astype(dt))
-    plain.step(7)
-    H1 = plain.get_state()
-    assert np.array_equal(F0, F1) and np.array_equal(H0, H1)
+    results = {}
+    # 2 / 3: pipelined kernel with 64- / 32-node tiles (two CTAs per SM); 1: register kernel
+    for which, kind, tile in ((2, "pipelined", 64), (3, "pipelined", 32), (1, "register", None)):
+        plain.select_kernel(which)
+        info = plain.kernel_info()
+        assert info["in_use"] == kind
+        if tile:
+            assert info["pipelined_tile"] == tile
+        F = plain.eval_rhs(K)
+        plain.set_state(m.H_init.astype(dt))
+        plain.step(7)
+        results[which] = (F, plain.get_state())
+    F0, H0 = results[1]
+    for which in (2, 3):
+        assert np.array_equal(results[which][0], F0) and np.array_equal(results[which][1], H0), which
     if prec == "fp64":
         assert rel_err(F0, oracle.Port(m, "fp64").eval_rhs(K)).max() <= 1e-12
 
