@@ -98,14 +98,15 @@ int swe_cuda_sync(void);
 
 /* Kernel choice.  0 = the bulk-copy pipelined stage kernel (a producer warp
  * streams each tile's weights, indices, pointwise data and state rows into
- * shared memory with cp.async.bulk; tiles of 64 nodes, one CTA per SM, or of
- * 32 nodes, two CTAs per SM); 1 = the register-streaming kernel.  All do the
- * same arithmetic in the same order; swe_cuda_init times the pipelined kernel
- * with both tiles and the register kernel on the patch, keeps the pipelined
- * kernel's faster tile, and uses the fastest.  info[4] = {kernel in use (0/1),
- * pipelined tile in nodes (0 if unavailable), ns per eval launch of kernel 0
- * (its faster tile), of kernel 1}.  swe_cuda_select_kernel also takes 2 / 3:
- * the pipelined kernel with 64- / 32-node tiles. */
+ * shared memory with cp.async.bulk; tiles of 64 nodes, one CTA per SM, of 32
+ * nodes, two CTAs per SM, or of 16 nodes, four CTAs per SM); 1 = the
+ * register-streaming kernel.  All do the same arithmetic in the same order;
+ * swe_cuda_init times the pipelined kernel with each tile and the register
+ * kernel on the patch, keeps the pipelined kernel's fastest tile, and uses the
+ * fastest kernel.  info[4] = {kernel in use (0/1), pipelined tile in nodes (0
+ * if unavailable), ns per eval launch of kernel 0 (its fastest tile), of
+ * kernel 1}.  swe_cuda_select_kernel also takes 2 / 3 / 4: the pipelined
+ * kernel with 64- / 32- / 16-node tiles. */
 int swe_cuda_select_kernel(int which);
 int swe_cuda_kernel_info(int* info);
 

@@ -255,6 +255,7 @@ struct Plain {
         const StageArgs<T> a = args<T>(mode);
         if (use_tma()) {
             if (tma_tile == 32) launch_tma<T, 32>(a, mode);
+            else if (tma_tile == 16) launch_tma<T, 16>(a, mode);
             else launch_tma<T, 64>(a, mode);
             return;
         }
@@ -335,6 +336,7 @@ static int upload_static(Plain& P, const void* x, const void* y, const void* z, 
         SWE_CUDA_TRY(cudaMemset(P.err, 0, sizeof(int)));
         SWE_TRY((set_tma_attrs<T, 64>()));
         SWE_TRY((set_tma_attrs<T, 32>()));
+        SWE_TRY((set_tma_attrs<T, 16>()));
     }
     return SWE_OK;
 }
@@ -462,9 +464,10 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
         SWE_CUDA_TRY(cudaEventCreate(&e0));
         SWE_CUDA_TRY(cudaEventCreate(&e1));
         SWE_CUDA_TRY(cudaMemsetAsync(P.Kx, 0, srow, P.stream));
-        const int cand_kernel[3] = {0, 0, 1}, cand_tile[3] = {64, 32, 64};
-        float us_c[3] = {0.f, 0.f, 0.f};
-        for (int c = 0; c < 3; ++c) {
+        constexpr int kCand = 4;
+        const int cand_kernel[kCand] = {0, 0, 0, 1}, cand_tile[kCand] = {64, 32, 16, 64};
+        float us_c[kCand] = {0.f, 0.f, 0.f, 0.f};
+        for (int c = 0; c < kCand; ++c) {
             P.kernel_choice = cand_kernel[c];
             P.tma_tile = cand_tile[c];
             for (int w = 0; w < 2; ++w) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
@@ -477,13 +480,16 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
             SWE_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
             us_c[c] = ms * 1e3f / 5.f;
         }
-        count_launch(21);
+        count_launch(7 * kCand);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        // the pipelined kernel keeps its faster tile, also when the register kernel wins
-        P.tma_tile = us_c[1] < us_c[0] ? 32 : 64;
-        P.tune_us[0] = std::min(us_c[0], us_c[1]);
-        P.tune_us[1] = us_c[2];
+        // the pipelined kernel keeps its fastest tile, also when the register kernel wins
+        int bt = 0;
+        for (int c = 1; c < kCand - 1; ++c)
+            if (us_c[c] < us_c[bt]) bt = c;
+        P.tma_tile = cand_tile[bt];
+        P.tune_us[0] = us_c[bt];
+        P.tune_us[1] = us_c[kCand - 1];
         P.kernel_choice = P.tune_us[1] < P.tune_us[0] ? 1 : 0;
         SWE_TRY(check_tma_err());
     }
@@ -575,9 +581,9 @@ int swe_cuda_sync(void) {
 
 int swe_cuda_select_kernel(int which) {
     SWE_TRY(require_ready());
-    if (which < 0 || which > 3) {
-        set_error("swe_cuda_select_kernel: 0 (pipelined), 1 (register), 2 / 3 (pipelined, 64 / 32-node tiles), got %d",
-                  which);
+    if (which < 0 || which > 4) {
+        set_error("swe_cuda_select_kernel: 0 (pipelined), 1 (register), 2 / 3 / 4 (pipelined, 64 / 32 / 16-node tiles), "
+                  "got %d", which);
         return SWE_ERR_ARG;
     }
     Plain& P = g_plain;
@@ -586,6 +592,7 @@ int swe_cuda_select_kernel(int which) {
     P.kernel_choice = which == 1 ? 1 : 0;
     if (which == 2) P.tma_tile = 64;
     if (which == 3) P.tma_tile = 32;
+    if (which == 4) P.tma_tile = 16;
     if (P.graph) cudaGraphExecDestroy(P.graph);
     P.graph = nullptr;
     return P.build_graph();

@@ -3,8 +3,8 @@
 // Same math and lane split as stage_kernel.cuh, restructured around B200's
 // bulk copy engine.  Persistent CTAs run one producer warp and TILE/4 consumer
 // warps over tiles of TILE consecutive nodes: 64-node tiles with one CTA per SM,
-// or 32-node tiles with two CTAs per SM (two producers in flight per SM; the
-// library times both at init).  For every tile the producer issues six
+// 32-node tiles with two or 16-node tiles with four CTAs per SM (more producers
+// in flight per SM; the library times the three at init).  For every tile the producer issues six
 // cp.async.bulk copies (global -> shared, completing on an mbarrier) into one
 // of kStages ring slots: the tile's packed weights (TILE x 1 KB in FP64),
 // packed stencil indices, pointwise records, own state rows, and the H / D rows

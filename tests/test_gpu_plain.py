@@ -182,8 +182,8 @@ def test_pipelined_and_register_kernels_agree_bitwise(plain, prec):
     dt = np.float64 if prec == "fp64" else np.float32
     K = _perturbed(m.H_init).astype(dt)
     results = {}
-    # 2 / 3: pipelined kernel with 64- / 32-node tiles (two CTAs per SM); 1: register kernel
-    for which, kind, tile in ((2, "pipelined", 64), (3, "pipelined", 32), (1, "register", None)):
+    # 2 / 3 / 4: pipelined kernel with 64- / 32- / 16-node tiles (1 / 2 / 4 CTAs per SM); 1: register
+    for which, kind, tile in ((2, "pipelined", 64), (3, "pipelined", 32), (4, "pipelined", 16), (1, "register", None)):
         plain.select_kernel(which)
         info = plain.kernel_info()
         assert info["in_use"] == kind
@@ -194,7 +194,7 @@ def test_pipelined_and_register_kernels_agree_bitwise(plain, prec):
         plain.step(7)
         results[which] = (F, plain.get_state())
     F0, H0 = results[1]
-    for which in (2, 3):
+    for which in (2, 3, 4):
         assert np.array_equal(results[which][0], F0) and np.array_equal(results[which][1], H0), which
     if prec == "fp64":
         assert rel_err(F0, oracle.Port(m, "fp64").eval_rhs(K)).max() <= 1e-12
