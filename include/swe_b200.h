@@ -129,6 +129,28 @@ int swe_cuda_invariants(double* mass_energy);
 int swe_cuda_finalize(void);
 
 /* ---------------------------------------------------------------------------
+ * History output of the plain form
+ * ------------------------------------------------------------------------- */
+
+/* The writer the reference declares but never implements (USE_HIST:
+ * runtime_params.c:24-27 reads SWE_OUTPUT_FILE and SWE_HIST_INT,
+ * swe_config.h:112-115 holds them; nothing writes).  After swe_hist_open,
+ * every `interval` completed RK4 steps (swe_cuda_step, or swe_cuda_rk_substep
+ * with substep 3; counted from the last swe_cuda_set_state) the state is
+ * appended to `path` -- the same values swe_cuda_get_state returns, in the
+ * caller's layout -- without stopping the time loop: the copy runs on its own
+ * stream and a writer thread does the file I/O (at most 4 snapshots in
+ * flight).  Format: a 64-byte header {char "SWEHIST1"[8]; int32 value bytes;
+ * int32 interval; int64 values per record; double dt; int32 layout flags;
+ * int32 SIMD length; 24 zero bytes}, then per record {int64 step; double
+ * step * dt; values}.  swe_hist_close writes what is queued and closes the
+ * file (swe_cuda_init and swe_cuda_finalize also close it).  stats[4] =
+ * {open (0/1), records written, bytes written, steps since set_state}. */
+int swe_hist_open(const char* path, int interval);
+int swe_hist_close(void);
+int swe_hist_stats(long long* stats);
+
+/* ---------------------------------------------------------------------------
  * Batched-ensemble form (members share one grid; tcgen05 tensor cores)
  * ------------------------------------------------------------------------- */
 

@@ -15,6 +15,7 @@
 
 #include "common.cuh"
 #include "stage_kernel.cuh"
+#include "history.cuh"
 #include "stage_tma.cuh"
 
 namespace swe {
@@ -169,7 +170,12 @@ struct Plain {
 
     size_t fbytes(long count) const { return (size_t)count * fsize; }
 
+    HistoryWriter hist;             // history output (swe_hist_open)
+    long long steps_done = 0;       // completed RK4 steps since the last swe_cuda_set_state
+
     void release() {
+        hist.close();
+        steps_done = 0;
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
         for (void* p : {W, PT, H, Ka, Kb, D, F, Kx, raw}) if (p) cudaFree(p);
@@ -362,6 +368,15 @@ static int require_ready() {
     return SWE_OK;
 }
 
+static int permute_state(const void* src, void* dst, int dir);
+
+// One RK4 step has been enqueued: count it and snapshot the state if the history is due.
+static int after_step() {
+    Plain& P = g_plain;
+    ++P.steps_done;
+    return P.hist.after_step(P.steps_done, P.stream, [&](void* dbuf) { return permute_state(P.H, dbuf, 1); });
+}
+
 static int permute_state(const void* src, void* dst, int dir) {
     Plain& P = g_plain;
     const long total = (long)P.rows * 4;
@@ -506,6 +521,7 @@ int swe_cuda_set_state(const void* Hh) {
     SWE_TRY(permute_state(P.raw, P.H, 0));
     SWE_CUDA_TRY(cudaMemcpyAsync(P.Ka, P.H, bytes, cudaMemcpyDeviceToDevice, P.stream));
     SWE_CUDA_TRY(cudaMemcpyAsync(P.Kb, P.H, bytes, cudaMemcpyDeviceToDevice, P.stream));
+    P.steps_done = 0;
     return SWE_OK;
 }
 
@@ -549,7 +565,8 @@ int swe_cuda_rk_substep(int substep_id) {
         set_error("time stepping needs compute_pid_s == 0 and patch_size == compute_size (no halos)");
         return SWE_ERR_ARG;
     }
-    return P.launch(substep_id);
+    SWE_TRY(P.launch(substep_id));
+    return substep_id == 3 ? after_step() : SWE_OK;
 }
 
 int swe_cuda_step(int nsteps) {
@@ -564,7 +581,10 @@ int swe_cuda_step(int nsteps) {
         for (auto& e : P.step_ev) if (!e) SWE_CUDA_TRY(cudaEventCreate(&e));
         SWE_CUDA_TRY(cudaEventRecord(P.step_ev[0], P.stream));
     }
-    for (int s = 0; s < nsteps; ++s) SWE_CUDA_TRY(cudaGraphLaunch(P.graph, P.stream));
+    for (int s = 0; s < nsteps; ++s) {
+        SWE_CUDA_TRY(cudaGraphLaunch(P.graph, P.stream));
+        SWE_TRY(after_step());
+    }
     count_launch(4LL * nsteps);
     if (P.timing) {
         SWE_CUDA_TRY(cudaEventRecord(P.step_ev[1], P.stream));
@@ -660,6 +680,30 @@ int swe_cuda_invariants(double* me) {
     const double area = 4.0 * 3.14159265358979323846 / (double)P.n;
     me[0] *= area;
     me[1] *= area;
+    return SWE_OK;
+}
+
+int swe_hist_open(const char* path, int interval) {
+    SWE_TRY(require_ready());
+    Plain& P = g_plain;
+    int dev = 0;
+    SWE_CUDA_TRY(cudaGetDevice(&dev));
+    return P.hist.open(path, interval, 4LL * P.rows, P.fsize, P.dt, P.cl.layout, P.cl.S, dev);
+}
+
+int swe_hist_close(void) {
+    SWE_TRY(require_ready());
+    SWE_CUDA_TRY(cudaStreamSynchronize(g_plain.stream));
+    return g_plain.hist.close();
+}
+
+int swe_hist_stats(long long* out) {
+    SWE_TRY(require_ready());
+    if (!out) { set_error("swe_hist_stats: null out"); return SWE_ERR_ARG; }
+    out[0] = g_plain.hist.active() ? 1 : 0;
+    out[1] = g_plain.hist.records();
+    out[2] = g_plain.hist.bytes();
+    out[3] = g_plain.steps_done;
     return SWE_OK;
 }
 

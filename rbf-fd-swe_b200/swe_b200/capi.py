@@ -61,6 +61,8 @@ def load() -> ctypes.CDLL:
     lib.swe_cuda_stream.restype = vp
     lib.swe_cuda_select_kernel.argtypes = [i]
     lib.swe_cuda_kernel_info.argtypes = [vp]
+    lib.swe_hist_open.argtypes = [ctypes.c_char_p, i]
+    lib.swe_hist_stats.argtypes = [vp]
     lib.swe_ens_init.argtypes = [i, i, i, d, d] + [vp] * 14
     lib.swe_ens_set_precision.argtypes = [i]
     for name in ("swe_ens_set_state", "swe_ens_get_state", "swe_ens_tune", "swe_ens_config",
@@ -219,6 +221,18 @@ class Plain:
         out = np.zeros(2)
         check("swe_cuda_invariants", self.lib.swe_cuda_invariants(_p(out)))
         return out
+
+    def hist_open(self, path: str, interval: int) -> None:
+        """Append the state to `path` every `interval` RK4 steps (see swe_b200.history)."""
+        check("swe_hist_open", self.lib.swe_hist_open(os.fsencode(path), int(interval)))
+
+    def hist_close(self) -> None:
+        check("swe_hist_close", self.lib.swe_hist_close())
+
+    def hist_stats(self) -> dict:
+        out = np.zeros(4, dtype=np.int64)
+        check("swe_hist_stats", self.lib.swe_hist_stats(_p(out)))
+        return {"open": bool(out[0]), "records": int(out[1]), "bytes": int(out[2]), "steps": int(out[3])}
 
     def finalize(self) -> None:
         check("swe_cuda_finalize", self.lib.swe_cuda_finalize())
