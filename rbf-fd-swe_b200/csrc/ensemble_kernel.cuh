@@ -52,7 +52,9 @@
 namespace swe {
 
 constexpr int kEnsEpiWarps = 8;
-constexpr uint32_t kEnsWaitTries = 1u << 22;
+constexpr uint32_t kEnsWaitTries = 1u << 22;              // final MMA drain: polls
+constexpr uint32_t kEnsWaitHintNs = 20000;                 // one sleeping try: up to 20 us
+constexpr uint64_t kEnsWaitLimitNs = 2000000000ull;        // a wait gives up after 2 s
 
 template <int MPC, int PREC>
 struct EnsCfg {
@@ -120,11 +122,16 @@ __device__ __forceinline__ bool named_and(int id, int nthreads, bool v) {
 }
 using tc::mbar_arrive;
 
-// Bounded wait that also gives up as soon as another role has aborted.
+// Bounded wait that also gives up as soon as another role has aborted.  Each try
+// sleeps in hardware (suspend-time hint) rather than spinning, so waiting warps
+// leave the issue slots to the working ones; the bound is wall time.
 __device__ __forceinline__ bool wait(uint64_t* b, uint32_t parity, volatile int* abort_s, int* err, int code) {
-    for (uint32_t t = 0; t < kEnsWaitTries; ++t) {
-        if (tc::mbar_try_wait(b, parity)) return true;
+    if (tc::mbar_try_wait(b, parity)) return true;
+    const uint64_t t0 = tc::globaltimer_ns();
+    for (;;) {
+        if (tc::mbar_try_wait_hint(b, parity, kEnsWaitHintNs)) return true;
         if (*abort_s) return false;
+        if (tc::globaltimer_ns() - t0 > kEnsWaitLimitNs) break;
     }
     *abort_s = 1;
     atomicExch(err, code);

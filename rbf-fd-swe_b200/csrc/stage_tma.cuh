@@ -29,7 +29,7 @@ struct TmaShape {
     static constexpr int kThreads = 32 * (kConsumerWarps + 1);
     static constexpr int kCtasPerSm = 64 / TILE;
 };
-constexpr uint32_t kTmaWaitTries = 1u << 24;
+constexpr uint64_t kTmaWaitLimitNs = 2000000000ull;   // a slot wait gives up after 2 s
 
 namespace tma {
 using tc::bulk_g2s;
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(TmaShape<TILE>::kThreads, TmaShape<TILE>::kCta
             const int s = it % Lay::kStages;
             int wait_ok = 1;
             if (lane == 0 && it >= Lay::kStages)
-                wait_ok = tc::mbar_wait_bounded(&empty[s], ((it / Lay::kStages) - 1) & 1, kTmaWaitTries);
+                wait_ok = tc::mbar_wait_timed(&empty[s], ((it / Lay::kStages) - 1) & 1, kTmaWaitLimitNs);
             wait_ok = __shfl_sync(0xffffffffu, wait_ok, 0);
             if (!wait_ok || *(volatile int*)&s_abort) {
                 if (lane == 0) { atomicExch(ta.err, 1); s_abort = 1; }
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(TmaShape<TILE>::kThreads, TmaShape<TILE>::kCta
         // drain: every issued slot must have landed before the CTA exits
         if (lane == 0)
             for (int j = max(0, issued - Lay::kStages); j < issued; ++j)
-                tc::mbar_wait_bounded(&full[j % Lay::kStages], (j / Lay::kStages) & 1, kTmaWaitTries);
+                tc::mbar_wait_timed(&full[j % Lay::kStages], (j / Lay::kStages) & 1, kTmaWaitLimitNs);
         return;
     }
 
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(TmaShape<TILE>::kThreads, TmaShape<TILE>::kCta
     int it = 0;
     for (int tile = blockIdx.x; tile < ta.ntiles; tile += gridDim.x, ++it) {
         const int s = it % Lay::kStages;
-        const bool ok = tc::mbar_wait_bounded(&full[s], (it / Lay::kStages) & 1, kTmaWaitTries);
+        const bool ok = tc::mbar_wait_timed(&full[s], (it / Lay::kStages) & 1, kTmaWaitLimitNs);
         if (!ok || *(volatile int*)&s_abort) {
             if (lane == 0) { atomicExch(ta.err, 2); s_abort = 1; }
             break;

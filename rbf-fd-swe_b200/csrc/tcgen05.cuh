@@ -116,6 +116,36 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// try_wait with a suspend-time hint: a thread whose phase is not complete sleeps in
+// hardware until it completes or about `hint_ns` pass, instead of re-polling.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* b, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Time-bounded wait that sleeps between tries (see mbar_try_wait_hint); false once
+// limit_ns of wall time have passed without the phase completing.
+__device__ __forceinline__ bool mbar_wait_timed(uint64_t* b, uint32_t parity, uint64_t limit_ns,
+                                                uint32_t hint_ns = 20000) {
+    if (mbar_try_wait(b, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
+        if (mbar_try_wait_hint(b, parity, hint_ns)) return true;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    }
+}
+
 // Bounded wait: gives up after max_tries polls (each try_wait already
 // suspends for a hardware-defined interval); returns false on timeout.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, uint32_t max_tries) {
