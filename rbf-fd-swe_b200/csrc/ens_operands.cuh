@@ -3,11 +3,15 @@
 // into hi / lo parts in the tensor core's shared-memory layout, and how the
 // MMA thread issues the chunk's three products.
 //
-//   Tf32x3: kind::tf32, hi / lo both exact TF32 (|x - hi - lo| <= 2^-22 |x|),
-//           2 k-steps of K = 8 per chunk.
+//   Tf32x3: kind::tf32, hi = tf32(x) rounded to nearest, lo = x - hi kept in
+//           FP32 and read by the tensor core at TF32 precision
+//           (|x - hi - lo| <= 2^-21 |x|), 2 k-steps of K = 8 per chunk.
 //   Bf16x3: kind::f16 with BF16 operands, hi = bf16(x), lo = bf16(x - hi)
 //           (|x - hi - lo| <= 2^-17 |x|), one k-step of K = 16 per chunk;
 //           half the shared-memory bytes of Tf32x3 and twice the tensor rate.
+//
+// Padding rows of a tile's neighbour list name the tile's centring node, so their
+// centred values are exactly zero (their weights are zero as well).
 //
 // Both are K-major without swizzle: 8-row x 16-byte core matrices, LBO = 128
 // (the next core matrix along K), SBO = the stride between 8-row groups.  The
@@ -77,7 +81,6 @@ struct Operands<MPC, kTf32x3> {
     struct Set {
         float4 x[4];          // 4 gathered rows x 4 member-fields
         float4 cen;           // centre state of the same member-fields
-        int live;             // bit i: row i is a real row
         float2 w[kOpp][4];    // weights of the operator pairs for the 4 chunk rows
     };
 
@@ -89,9 +92,7 @@ struct Operands<MPC, kTf32x3> {
                                      const Thread& th, const Fetch& f, Set& o, const Set& prev) {
         const int r[4] = {f.idx.x, f.idx.y, f.idx.z, f.idx.w};
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-            o.x[i] = r[i] >= 0 ? ldg_f4(Kin + (long)r[i] * mf + col) : make_float4(0.f, 0.f, 0.f, 0.f);
-        o.live = (r[0] >= 0 ? 1 : 0) | (r[1] >= 0 ? 2 : 0) | (r[2] >= 0 ? 4 : 0) | (r[3] >= 0 ? 8 : 0);
+        for (int i = 0; i < 4; ++i) o.x[i] = ldg_f4(Kin + (long)r[i] * mf + col);
         o.cen = cen_row ? ldg_f4(cen_row + col) : prev.cen;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -114,10 +115,10 @@ struct Operands<MPC, kTf32x3> {
             for (int h = 0; h < 2; ++h) {
                 const int r = 32 * (2 * (th.opp0 + q) + h) + th.at;
                 float4 hi, lo;
-                tc::tf32_split(h ? o.w[q][0].y : o.w[q][0].x, hi.x, lo.x);
-                tc::tf32_split(h ? o.w[q][1].y : o.w[q][1].x, hi.y, lo.y);
-                tc::tf32_split(h ? o.w[q][2].y : o.w[q][2].x, hi.z, lo.z);
-                tc::tf32_split(h ? o.w[q][3].y : o.w[q][3].x, hi.w, lo.w);
+                tc::tf32_split_lo_fp32(h ? o.w[q][0].y : o.w[q][0].x, hi.x, lo.x);
+                tc::tf32_split_lo_fp32(h ? o.w[q][1].y : o.w[q][1].x, hi.y, lo.y);
+                tc::tf32_split_lo_fp32(h ? o.w[q][2].y : o.w[q][2].x, hi.z, lo.z);
+                tc::tf32_split_lo_fp32(h ? o.w[q][3].y : o.w[q][3].x, hi.w, lo.w);
                 const uint32_t off = (r >> 3) * kSboA + th.akg * 128 + (r & 7) * 16;
                 *reinterpret_cast<float4*>(A_hi + off) = hi;
                 *reinterpret_cast<float4*>(A_lo + off) = lo;
@@ -134,11 +135,11 @@ struct Operands<MPC, kTf32x3> {
             float4 hi, lo;
             float y[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) y[i] = ((o.live >> i) & 1) ? xv[i][j] - cv[j] : 0.f;
-            tc::tf32_split(y[0], hi.x, lo.x);
-            tc::tf32_split(y[1], hi.y, lo.y);
-            tc::tf32_split(y[2], hi.z, lo.z);
-            tc::tf32_split(y[3], hi.w, lo.w);
+            for (int i = 0; i < 4; ++i) y[i] = xv[i][j] - cv[j];
+            tc::tf32_split_lo_fp32(y[0], hi.x, lo.x);
+            tc::tf32_split_lo_fp32(y[1], hi.y, lo.y);
+            tc::tf32_split_lo_fp32(y[2], hi.z, lo.z);
+            tc::tf32_split_lo_fp32(y[3], hi.w, lo.w);
             const uint32_t off = (nrow >> 3) * kSboB + th.kg * 128 + (nrow & 7) * 16;
             *reinterpret_cast<float4*>(B_hi + off) = hi;
             *reinterpret_cast<float4*>(B_lo + off) = lo;
@@ -193,7 +194,6 @@ struct Operands<MPC, kBf16x3> {
     struct Set {
         float2 x[8];          // 8 gathered rows x 2 member-fields
         float2 cen;
-        int live;             // bit i: row i is a real row
         WT w[8];
     };
 
@@ -208,13 +208,8 @@ struct Operands<MPC, kBf16x3> {
                                      const Thread& th, const Fetch& f, Set& o, const Set& prev) {
         const int r[8] = {f.idx[0].x, f.idx[0].y, f.idx[0].z, f.idx[0].w,
                           f.idx[1].x, f.idx[1].y, f.idx[1].z, f.idx[1].w};
-        int live = 0;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            o.x[i] = r[i] >= 0 ? ldg_f2(Kin + (long)r[i] * mf + col) : make_float2(0.f, 0.f);
-            live |= (r[i] >= 0 ? 1 : 0) << i;
-        }
-        o.live = live;
+        for (int i = 0; i < 8; ++i) o.x[i] = ldg_f2(Kin + (long)r[i] * mf + col);
         o.cen = cen_row ? ldg_f2(cen_row + col) : prev.cen;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -257,7 +252,7 @@ struct Operands<MPC, kBf16x3> {
             const float c = j ? o.cen.y : o.cen.x;
             float y[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) y[i] = ((o.live >> i) & 1) ? (j ? o.x[i].y : o.x[i].x) - c : 0.f;
+            for (int i = 0; i < 8; ++i) y[i] = (j ? o.x[i].y : o.x[i].x) - c;
             uint4 hi, lo;
             hi.x = bf16x2_split(y[0], y[1], lo.x);
             hi.y = bf16x2_split(y[2], y[3], lo.y);

@@ -94,6 +94,8 @@ TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std:
         tb.max_rows = std::max(tb.max_rows, (int)u.size());
         const int nch = ((int)u.size() + kEnsKc - 1) / kEnsKc;
         const int kpad = nch * kEnsKc;
+        // padding rows: the centring node (chosen below), whose centred state is exactly 0
+        const size_t pad0 = tb.rows.size() + u.size();
         for (int k = 0; k < kpad; ++k) tb.rows.push_back(k < (int)u.size() ? u[k] : -1);
         tb.row_off[tile + 1] = (int)tb.rows.size();
         slot.assign((size_t)kEnsTileNodes * kpad, 0xff);
@@ -119,6 +121,7 @@ TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std:
                              (X[3 * i + 2] - cz) * (X[3 * i + 2] - cz);
             if (d < best) { best = d; tb.centre[tile] = i; }
         }
+        for (size_t k = pad0; k < tb.rows.size(); ++k) tb.rows[k] = tb.centre[tile];
     }
     tb.nchunks = (int)tb.rows.size() / kEnsKc;
     return tb;

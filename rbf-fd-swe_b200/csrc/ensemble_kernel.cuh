@@ -15,9 +15,9 @@
 // stencil slot.
 //
 // Precision: both operands are split x ~ hi + lo, and D = A_hi B_hi + A_hi B_lo
-// + A_lo B_hi accumulates in FP32 in tensor memory; the split is 3xTF32 (both
-// parts exact TF32, |x - hi - lo| <= 2^-22 |x|) or split BF16 (2^-17), see
-// ens_operands.cuh.  The gathered states are
+// + A_lo B_hi accumulates in FP32 in tensor memory; the split is 3xTF32
+// (|x - hi - lo| <= 2^-21 |x| as the tensor core reads it) or split BF16
+// (2^-17), see ens_operands.cuh.  The gathered states are
 // centred on the state of one node of the tile (c[mf]) before the split;
 // c * sum_k W (row sums of the FP32 weights, summed in FP64) is added back in
 // the epilogue.  Derivative and hyperviscosity weights annihilate constants,
@@ -85,7 +85,7 @@ struct EnsArgs {
     int members;
     int mf;                // 4 * members (row length of the state arrays)
     const int* row_off;    // [ntiles + 1] offsets into rows, multiples of kEnsKc
-    const int* rows;       // unique neighbour rows of each tile, ascending; -1 pads
+    const int* rows;       // unique neighbour rows of each tile, ascending; padded with the centring node
     const uint32_t* jmap;  // [chunk][row group][node t]: stencil slot of each of the 4 rows, 255 = none
     const float4* W;       // [n][32] (Dx, Dy, Dz, L) per stencil slot
     const int* centre;     // [ntiles] node whose state centres the tile
@@ -390,8 +390,14 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
 #pragma unroll
                     for (int f = 0; f < 4; ++f) S[4 * o2 + f] = fmaf(cf[f], rs[o2], S[4 * o2 + f]);
                 const float q[4] = {o.own[pi].x, o.own[pi].y, o.own[pi].z, o.own[pi].w};
+                float pt[kPointStride];
+#pragma unroll
+                for (int pp = 0; pp < kPointStride / 4; ++pp) {
+                    const float4 pv = *reinterpret_cast<const float4*>(tb + t * kPointStride + 4 * pp);
+                    pt[4 * pp] = pv.x; pt[4 * pp + 1] = pv.y; pt[4 * pp + 2] = pv.z; pt[4 * pp + 3] = pv.w;
+                }
                 float F[4];
-                pointwise_rhs<float>(S, q, tb + t * kPointStride, a.gh0, F);
+                pointwise_rhs<float>(S, q, pt, a.gh0, F);
                 const long e4 = node * a.mf + mfb;
                 const long eh = node * members + member;
                 if (MODE == kEvalOnly) {

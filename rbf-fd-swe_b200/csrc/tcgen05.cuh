@@ -178,6 +178,13 @@ __device__ __forceinline__ float tf32_rna(float x) {
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return __uint_as_float(r);
 }
+// 3xTF32 split with lo left in FP32: hi = tf32_rna(x) and lo = x - hi exactly (hi has
+// 11 significant bits, so x - hi is representable).  The tensor core reads lo at TF32
+// precision (its low 13 bits dropped): |x - hi - lo_used| <= 2^-10 |lo| <= 2^-21 |x|.
+__device__ __forceinline__ void tf32_split_lo_fp32(float x, float& hi, float& lo) {
+    hi = tf32_rna(x);
+    lo = x - hi;
+}
 // 3xTF32 split x ~ hi + lo with both parts exact TF32: |x - hi - lo| <= 2^-22 |x|.
 __device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
     hi = tf32_rna(x);
