@@ -151,6 +151,24 @@ int swe_hist_close(void);
 int swe_hist_stats(long long* stats);
 
 /* ---------------------------------------------------------------------------
+ * Input generator on the GPU (grids beyond the shipped N=2562 file)
+ * ------------------------------------------------------------------------- */
+
+/* No reference counterpart: the reference reads its binary input
+ * (io/input.c:189-414) and does not ship the tool that produced it.  All
+ * pointers are device pointers.
+ * swe_gen_stencils: X [n][3] FP64 unit vectors -> idx [n][k] int32, 0-based, the
+ *   k nearest nodes by chordal distance, self first, then by distance, ties by
+ *   node index (k <= 32).
+ * swe_gen_weights: unit-sphere RBF-FD weights D [4][n][k] FP64 (Dx, Dy, Dz, L)
+ *   for those stencils: PHS r^7 + degree-4 tangent-plane polynomials for the
+ *   projected gradient, r^9 on tangent-plane distances for Delta^4; one local
+ *   solve (partial pivoting) per node and operator set.  The reader's scaling
+ *   (Dx/a, L*gamma; input.c:314-319) is applied later, as for a file. */
+int swe_gen_stencils(int n, int k, const double* X, int* idx);
+int swe_gen_weights(int n, int k, const double* X, const int* idx, double* D);
+
+/* ---------------------------------------------------------------------------
  * Batched-ensemble form (members share one grid; tcgen05 tensor cores)
  * ------------------------------------------------------------------------- */
 

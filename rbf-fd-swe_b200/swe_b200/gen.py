@@ -92,6 +92,40 @@ def icosahedral_nodes(level: int) -> np.ndarray:
     return V
 
 
+def _on_cuda(device) -> bool:
+    return str(device).startswith("cuda")
+
+
+def stencils_gpu(X: np.ndarray, nnbr: int = NNBR, device: str = "cuda") -> np.ndarray:
+    """The same stencils from the library's GPU kernel (swe_gen_stencils): k nearest by
+    chordal distance, self first, ties by node index."""
+    import torch
+
+    from . import capi
+    lib = capi.load()
+    Xt = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float64)).to(device)
+    out = torch.empty((len(X), nnbr), dtype=torch.int32, device=device)
+    with torch.cuda.device(Xt.device):
+        capi.check("swe_gen_stencils", lib.swe_gen_stencils(len(X), nnbr, Xt.data_ptr(), out.data_ptr()))
+    return out.cpu().numpy()
+
+
+def rbffd_weights_gpu(X: np.ndarray, idx: np.ndarray, device: str = "cuda"):
+    """The same unit-sphere weights from the library's GPU kernel (swe_gen_weights)."""
+    import torch
+
+    from . import capi
+    lib = capi.load()
+    N, n = idx.shape
+    Xt = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float64)).to(device)
+    It = torch.from_numpy(np.ascontiguousarray(idx, dtype=np.int32)).to(device)
+    D = torch.empty((4, N, n), dtype=torch.float64, device=device)
+    with torch.cuda.device(Xt.device):
+        capi.check("swe_gen_weights", lib.swe_gen_weights(N, n, Xt.data_ptr(), It.data_ptr(), D.data_ptr()))
+    D = D.cpu().numpy()
+    return D[0], D[1], D[2], D[3]
+
+
 def stencils(X: np.ndarray, nnbr: int = NNBR) -> np.ndarray:
     """0-based [N, nnbr] nearest-neighbour stencils, self first."""
     from scipy.spatial import cKDTree
@@ -199,12 +233,24 @@ def perturb_h(H: np.ndarray, seed: int, noise: float = NOISE) -> np.ndarray:
 
 
 def generate(level: int, seed: int = 0, dt: float | None = None, device: str = "cpu",
-             gamma_coef: float = GAMMA_COEF) -> SweInput:
-    """A complete input (H_100 left zero; oracle/fill_fc.py fills it)."""
+             gamma_coef: float = GAMMA_COEF, native: bool | None = None,
+             idx: np.ndarray | None = None) -> SweInput:
+    """A complete input (H_100 left zero; oracle/fill_fc.py fills it).
+
+    On a CUDA device the stencils and weights come from the library's GPU kernels
+    (native, the default there); on the CPU from scipy and torch.  `idx` (0-based
+    [N, nnbr], self first) fixes the stencils instead: nodes at an exact distance tie
+    for the last stencil place may be chosen differently by the two searches."""
     X = icosahedral_nodes(level)
     N = len(X)
-    idx = stencils(X)
-    Dx, Dy, Dz, L = rbffd_weights(X, idx, device=device)
+    if native is None:
+        native = _on_cuda(device)
+    if idx is None:
+        idx = stencils_gpu(X, device=device) if native else stencils(X)
+    if native:
+        Dx, Dy, Dz, L = rbffd_weights_gpu(X, idx, device=device)
+    else:
+        Dx, Dy, Dz, L = rbffd_weights(X, idx, device=device)
     H, ghm = tc5_state(X, seed)
     gradghm = np.stack([np.einsum("ij,ij->i", D, ghm[idx]) / A_EARTH for D in (Dx, Dy, Dz)], 1)
     eye = np.eye(3)
