@@ -168,6 +168,13 @@ int swe_hist_stats(long long* stats);
 int swe_gen_stencils(int n, int k, const double* X, int* idx);
 int swe_gen_weights(int n, int k, const double* X, const int* idx, double* D);
 
+/* Self-test of the bounded waits (no reference counterpart).  Launches one block
+ * that waits on an mbarrier nothing arrives on, with the time-bounded wait the
+ * pipelined kernels use; returns SWE_ERR_TIMEOUT once it gave up after about
+ * limit_s (0 < limit_s <= 2), with the context still usable.  waited_s (may
+ * be NULL) receives the time the kernel waited. */
+int swe_selftest_wait_timeout(double limit_s, double* waited_s);
+
 /* ---------------------------------------------------------------------------
  * Batched-ensemble form (members share one grid; tcgen05 tensor cores)
  * ------------------------------------------------------------------------- */

@@ -63,6 +63,7 @@ def load() -> ctypes.CDLL:
     lib.swe_cuda_kernel_info.argtypes = [vp]
     lib.swe_hist_open.argtypes = [ctypes.c_char_p, i]
     lib.swe_gen_stencils.argtypes = [i, i, vp, vp]
+    lib.swe_selftest_wait_timeout.argtypes = [d, vp]
     lib.swe_gen_weights.argtypes = [i, i, vp, vp, vp]
     lib.swe_hist_stats.argtypes = [vp]
     lib.swe_ens_init.argtypes = [i, i, i, d, d] + [vp] * 14
