@@ -93,24 +93,43 @@ __device__ __forceinline__ void load_row_cg(const double* p, double (&v)[4]) {
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
-// One warp, 4 nodes [base, base+4) of one member and one stage; the plain
-// stage kernel's math with L2-coherent loads of everything the kernel itself
-// writes (states change between stages inside one launch).
-__device__ void serve_group(const ReqDesc& r, int stage, long base, long end, double* __restrict__ Hm,
-                            double* __restrict__ Kam, double* __restrict__ Kbm, double* __restrict__ Dm,
-                            double (*red)[16], int k, int g) {
+// One warp, 4 nodes [base, base+4) of one member and one stage: the plain stage
+// kernel's math and data movement -- stencil indices prefetched one group ahead
+// (`nb` in: this group's, out: the next group's), the epilogue operands staged by
+// the node's 8 lanes into `ep` while the sums run -- with L2-coherent loads of
+// everything the kernel itself writes (states change between stages inside one
+// launch).
+constexpr int kSrvEp = kPointStride + 12;
+
+__device__ void serve_group(const ReqDesc& r, int stage, long base, long end, long next_base, int4& nb,
+                            double* __restrict__ Hm, double* __restrict__ Kam, double* __restrict__ Kbm,
+                            double* __restrict__ Dm, double (*red)[16], double (*ep)[kSrvEp], int k, int g) {
     const long i = base + g;
     const bool valid = i < end;
     const long ii = valid ? i : end - 1;
     const double* Kin = stage == 0 ? Hm : stage == 1 ? Kam : stage == 2 ? Kbm : Kam;
     double* Kout = stage == 0 ? Kam : stage == 1 ? Kbm : Kam;
-    const int4 nb = __ldg(r.idx + ii * 8 + k);
     const int nbr[4] = {nb.x, nb.y, nb.z, nb.w};
-    double w[kSlotChunks][4], kv[kSlotChunks][4];
-#pragma unroll
-    for (int m = 0; m < kSlotChunks; ++m) Quad<double>::load(r.W, ((ii * kSlotChunks + m) * 2) * 8 + k, w[m]);
+    double kv[kSlotChunks][4], w[kSlotChunks][4];
 #pragma unroll
     for (int m = 0; m < kSlotChunks; ++m) load_row_cg(Kin + 4L * nbr[m], kv[m]);
+#pragma unroll
+    for (int m = 0; m < kSlotChunks; ++m) Quad<double>::load(r.W, ((ii * kSlotChunks + m) * 2) * 8 + k, w[m]);
+    // epilogue operands: lanes 0-4 the pointwise record, 5-7 the own, H and D rows
+    {
+        double* e = ep[g];
+        double v[4];
+        if (k < 5) {
+            Quad<double>::load_row(r.PT + ii * kPointStride + 4 * k, v);
+#pragma unroll
+            for (int x = 0; x < 4; ++x) e[4 * k + x] = v[x];
+        } else {
+            load_row_cg((k == 5 ? Kin : k == 6 ? Hm : Dm) + 4 * ii, v);
+#pragma unroll
+            for (int x = 0; x < 4; ++x) e[kPointStride + 4 * (k - 5) + x] = v[x];
+        }
+    }
+    if (next_base < end) nb = __ldg(r.idx + min(next_base + g, end - 1) * 8 + k);
     double acc[16];
 #pragma unroll
     for (int t = 0; t < 16; ++t) acc[t] = 0.0;
@@ -126,11 +145,13 @@ __device__ void serve_group(const ReqDesc& r, int stage, long base, long end, do
     red[g][2 * k + 1] = r1;
     __syncwarp();
     if (k == 0 && valid) {
+        const double* e = ep[g];
         double s[16], q[4], F[4];
 #pragma unroll
         for (int t = 0; t < 16; ++t) s[t] = red[g][t];
-        load_row_cg(Kin + 4 * i, q);
-        pointwise_rhs(s, q, r.PT + i * kPointStride, r.gh0, F);
+#pragma unroll
+        for (int x = 0; x < 4; ++x) q[x] = e[kPointStride + x];
+        pointwise_rhs(s, q, e, r.gh0, F);
         const double dt = r.dt;
         if (stage == 0) {
             double kn[4];
@@ -139,25 +160,21 @@ __device__ void serve_group(const ReqDesc& r, int stage, long base, long end, do
             Quad<double>::store_row(Dm + 4 * i, F);
             Quad<double>::store_row(Kout + 4 * i, kn);
         } else if (stage < 3) {
-            double h[4], d[4], kn[4];
-            load_row_cg(Hm + 4 * i, h);
-            load_row_cg(Dm + 4 * i, d);
+            double d[4], kn[4];
             const double c = stage == 1 ? dt / 2.0 : dt;
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
-                d[t] = Quad<double>::axpy(d[t], 2.0, F[t]);
-                kn[t] = Quad<double>::axpy(h[t], c, F[t]);
+                d[t] = Quad<double>::axpy(e[kPointStride + 8 + t], 2.0, F[t]);
+                kn[t] = Quad<double>::axpy(e[kPointStride + 4 + t], c, F[t]);
             }
             Quad<double>::store_row(Dm + 4 * i, d);
             Quad<double>::store_row(Kout + 4 * i, kn);
         } else {
-            double h[4], d[4];
-            load_row_cg(Hm + 4 * i, h);
-            load_row_cg(Dm + 4 * i, d);
+            double h[4];
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
-                d[t] = Quad<double>::axpy(d[t], 1.0, F[t]);
-                h[t] = Quad<double>::update_h(h[t], dt / 6.0, d[t]);
+                const double d = Quad<double>::axpy(e[kPointStride + 8 + t], 1.0, F[t]);
+                h[t] = Quad<double>::update_h(e[kPointStride + 4 + t], dt / 6.0, d);
             }
             Quad<double>::store_row(Hm + 4 * i, h);
         }
@@ -178,6 +195,7 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
              unsigned long long* head, const ReqDesc* __restrict__ reqs, int* done, int* flags, int* mdone,
              unsigned long long* items_done, int* exiting, int* kerr) {
     __shared__ double red[kStageWarps][4][16];
+    __shared__ __align__(16) double ep[kStageWarps][4][kSrvEp];
     __shared__ long long s_pos;
     __shared__ Item s_item;
     __shared__ int s_ok;
@@ -247,8 +265,12 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
             const long off = 4L * r.n * it.member;
             const long begin = (long)it.chunk * r.chunk_nodes;
             const long end = min((long)r.n, begin + r.chunk_nodes);
-            for (long base = begin + warp * 4L; base < end; base += kStageWarps * 4L)
-                serve_group(r, stage, base, end, r.H + off, r.Ka + off, r.Kb + off, r.D + off, red[warp], k, g);
+            long base = begin + warp * 4L;
+            int4 nb = make_int4(0, 0, 0, 0);
+            if (base < end) nb = __ldg(r.idx + min(base + g, end - 1) * 8 + k);
+            for (; base < end; base += kStageWarps * 4L)
+                serve_group(r, stage, base, end, base + kStageWarps * 4L, nb, r.H + off, r.Ka + off, r.Kb + off,
+                            r.D + off, red[warp], ep[warp], k, g);
         }
         __threadfence();
         __syncthreads();
