@@ -247,12 +247,24 @@ struct Plain {
         const TmaArgs<T> ta{a, ntiles, err};
         const int g = std::max(1, std::min(ntiles, sms * Sh::kCtasPerSm));
         const int sm = TmaLayout<T, TILE>::kSmem;
+        // programmatic dependent launch: the kernel loads its static streams before
+        // griddepcontrol.wait (stage_tma.cuh)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(g);
+        cfg.blockDim = dim3(Sh::kThreads);
+        cfg.dynamicSmemBytes = sm;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
         switch (mode) {
-            case 0: stage_tma_kernel<T, kStage0, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
-            case 1: stage_tma_kernel<T, kStage1, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
-            case 2: stage_tma_kernel<T, kStage2, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
-            case 3: stage_tma_kernel<T, kStage3, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
-            default: stage_tma_kernel<T, kEvalOnly, TILE><<<g, Sh::kThreads, sm, stream>>>(ta); break;
+            case 0: cudaLaunchKernelEx(&cfg, stage_tma_kernel<T, kStage0, TILE>, ta); break;
+            case 1: cudaLaunchKernelEx(&cfg, stage_tma_kernel<T, kStage1, TILE>, ta); break;
+            case 2: cudaLaunchKernelEx(&cfg, stage_tma_kernel<T, kStage2, TILE>, ta); break;
+            case 3: cudaLaunchKernelEx(&cfg, stage_tma_kernel<T, kStage3, TILE>, ta); break;
+            default: cudaLaunchKernelEx(&cfg, stage_tma_kernel<T, kEvalOnly, TILE>, ta); break;
         }
     }
 

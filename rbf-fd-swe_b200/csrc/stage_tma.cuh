@@ -13,14 +13,24 @@
 // state arrays are L2-resident; a tile's neighbours are scattered rows, which
 // suits plain loads better than many small bulk copies), run the stencil sums,
 // reduction and pointwise/RK combine with every other operand in shared memory,
-// store their outputs and release the slot.  Every wait is bounded; a timeout
-// sets an error word and the kernel drains its outstanding copies and returns.
+// store their outputs and release the slot.  Launched with programmatic
+// dependent launch: the first tile's weights, indices and pointwise records are
+// requested before griddepcontrol.wait, so they load while the previous stage
+// finishes; every read of a state array comes after the wait.  Every wait is
+// bounded; a timeout sets an error word and the kernel drains its outstanding
+// copies and returns.
 #pragma once
 
 #include "stage_kernel.cuh"
 #include "tcgen05.cuh"
 
 namespace swe {
+
+// Programmatic dependent launch.  The previous stage's writes are visible only
+// after pdl_wait(); a CTA lets the next stage launch (pdl_trigger) only after its
+// own wait, so at most two consecutive stages are ever resident together.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 template <int TILE>
 struct TmaShape {
@@ -102,11 +112,20 @@ __global__ void __launch_bounds__(TmaShape<TILE>::kThreads, TmaShape<TILE>::kCta
                 tma::arrive_expect_tx(&full[s], tx);
             }
             __syncwarp();
+            // static streams (never written by a stage) first: for the first tile they
+            // load while the previous stage is still finishing
             switch (lane) {
                 case 0: tma::bulk_g2s(slot + Lay::oW, a.W + n0 * kSlotChunks * Quad<T>::kUnits * 8, nn * Lay::kWn,
                                       &full[s]); break;
                 case 1: tma::bulk_g2s(slot + Lay::oIdx, a.idx + n0 * 8, nn * Lay::kIdxn, &full[s]); break;
                 case 2: tma::bulk_g2s(slot + Lay::oPt, a.PT + n0 * kPointStride, nn * Lay::kPtn, &full[s]); break;
+                default: break;
+            }
+            if (it == 0) {
+                pdl_wait();
+                pdl_trigger();
+            }
+            switch (lane) {
                 case 3: tma::bulk_g2s(slot + Lay::oOwn, a.Kin + 4L * (n0 + a.pid0), nn * Lay::kRow, &full[s]); break;
                 case 4: if (need_hd) tma::bulk_g2s(slot + Lay::oH, a.H + 4L * n0, nn * Lay::kRow, &full[s]); break;
                 case 5: if (need_hd) tma::bulk_g2s(slot + Lay::oD, a.D + 4L * n0, nn * Lay::kRow, &full[s]); break;
@@ -124,6 +143,8 @@ __global__ void __launch_bounds__(TmaShape<TILE>::kThreads, TmaShape<TILE>::kCta
 // ---------------- consumers ----------------
     const int g = lane >> 3, k = lane & 7;
     constexpr int U = Quad<T>::kUnits;
+    pdl_wait();            // neighbour states come from the previous stage
+    pdl_trigger();
     int it = 0;
     for (int tile = blockIdx.x; tile < ta.ntiles; tile += gridDim.x, ++it) {
         const int s = it % Lay::kStages;
