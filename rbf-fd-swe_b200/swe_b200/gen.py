@@ -234,7 +234,7 @@ def perturb_h(H: np.ndarray, seed: int, noise: float = NOISE) -> np.ndarray:
 
 def generate(level: int, seed: int = 0, dt: float | None = None, device: str = "cpu",
              gamma_coef: float = GAMMA_COEF, native: bool | None = None,
-             idx: np.ndarray | None = None) -> SweInput:
+             idx: np.ndarray | None = None, nnbr: int = NNBR) -> SweInput:
     """A complete input (H_100 left zero; oracle/fill_fc.py fills it).
 
     On a CUDA device the stencils and weights come from the library's GPU kernels
@@ -246,7 +246,7 @@ def generate(level: int, seed: int = 0, dt: float | None = None, device: str = "
     if native is None:
         native = _on_cuda(device)
     if idx is None:
-        idx = stencils_gpu(X, device=device) if native else stencils(X)
+        idx = stencils_gpu(X, nnbr, device=device) if native else stencils(X, nnbr)
     if native:
         Dx, Dy, Dz, L = rbffd_weights_gpu(X, idx, device=device)
     else:

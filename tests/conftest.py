@@ -35,16 +35,16 @@ def pytest_collection_modifyitems(config, items):
 _grid_cache = {}
 
 
-def generated_input(level: int, seed: int = 1, fill_fc: bool = False):
+def generated_input(level: int, seed: int = 1, fill_fc: bool = False, nnbr: int = 31):
     """(path, SweInput) of a generated grid, written once per session under a temp dir."""
     import tempfile
 
     from swe_b200 import gen, swe_input
 
-    key = (level, seed, fill_fc)
+    key = (level, seed, fill_fc, nnbr)
     if key in _grid_cache:
         return _grid_cache[key]
-    d = gen.generate(level, seed=seed)
+    d = gen.generate(level, seed=seed, nnbr=nnbr)
     if fill_fc:
         import oracle
 

@@ -126,3 +126,15 @@ def test_ensemble_invariants_fp64(ens, model_l4):
 def test_rejects_bad_member_count(ens, model_l4):
     with pytest.raises(capi.SweError):
         ens.init(model_l4, 48)
+
+
+def test_short_stencils(ens):
+    """20-point stencils through the ensemble tables (fewer rows per tile, same bars)."""
+    _, d = generated_input(4, fill_fc=True, nnbr=20)
+    m = swe_input.to_model(d)
+    ens.init(m, 32)
+    K = _members(m, 32)
+    F = ens.eval_rhs(K)
+    port = oracle.Port(m, "fp64")
+    worst = max(cond_err(F[b], port.eval_rhs(K[b]), m, K[b]) for b in (0, 13, 31))
+    assert worst <= COND_BOUND["tf32x3"], worst
