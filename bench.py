@@ -594,7 +594,8 @@ def main():
     kinfo = plain.kernel_info()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(args.workload), "peak_source": peak_kind,
-                "kernel": "swe::stage_tma_kernel" if kinfo["in_use"] == "pipelined" else "swe::stage_kernel",
+                "kernel": {"pipelined": "swe::stage_tma_kernel", "register": "swe::stage_kernel",
+                           "lane": "swe::stage_lane_kernel"}[kinfo["in_use"]],
                 "kernel_us": round(t_kernel * 1e6, 2), "alg_bytes_per_node_stage": ALG_BYTES[prec],
                 "kernel_choice": kinfo}
 

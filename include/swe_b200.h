@@ -100,13 +100,18 @@ int swe_cuda_sync(void);
  * streams each tile's weights, indices, pointwise data and state rows into
  * shared memory with cp.async.bulk; tiles of 64 nodes, one CTA per SM, of 32
  * nodes, two CTAs per SM, or of 16 nodes, four CTAs per SM); 1 = the
- * register-streaming kernel.  All do the same arithmetic in the same order;
- * swe_cuda_init times the pipelined kernel with each tile and the register
- * kernel on the patch, keeps the pipelined kernel's fastest tile, and uses the
- * fastest kernel.  info[4] = {kernel in use (0/1), pipelined tile in nodes (0
- * if unavailable), ns per eval launch of kernel 0 (its fastest tile), of
- * kernel 1}.  swe_cuda_select_kernel also takes 2 / 3 / 4: the pipelined
- * kernel with 64- / 32- / 16-node tiles. */
+ * register-streaming kernel; 2 = the node-per-lane kernel (1, 2 or 4 lanes per
+ * node, each summing its slots serially, from a tile-transposed copy of the
+ * weights and indices).  Kernels 0 and 1 do the same arithmetic in the same
+ * order; kernel 2 sums the slots in another order and meets the same error
+ * bars.  swe_cuda_init times every kernel and shape on the patch, keeps the
+ * fastest shape of each, and uses the fastest kernel.  info[6] = {kernel in use
+ * (0/1/2), pipelined tile in nodes (0 if unavailable), ns per eval launch of
+ * kernel 0 (its fastest tile), of kernel 1, lanes per node of kernel 2, ns per
+ * eval launch of kernel 2 (its fastest shape)}.  swe_cuda_select_kernel takes
+ * which = 0 / 1 (kernels 0 / 1), 2 / 3 / 4 (the pipelined kernel with 64- / 32-
+ * / 16-node tiles), 5 (kernel 2) and 6 / 7 / 8 (kernel 2 with 1 / 2 / 4 lanes
+ * per node). */
 int swe_cuda_select_kernel(int which);
 int swe_cuda_kernel_info(int* info);
 

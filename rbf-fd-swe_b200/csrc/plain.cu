@@ -17,6 +17,7 @@
 #include "stage_kernel.cuh"
 #include "history.cuh"
 #include "stage_tma.cuh"
+#include "stage_lane.cuh"
 
 namespace swe {
 
@@ -77,6 +78,42 @@ static int pack_idx(const CallerLayout& cl, int n, int rows, int pid0, int nnbr,
             out[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)] = p;
         }
     return SWE_OK;
+}
+
+// Tile-transposed copies for the node-per-lane kernel (stage_lane.cuh): node i
+// = 32 b + t, slot j and 16-byte unit q go to unit ((b*32 + j)*U + q)*32 + t;
+// nodes past n in the last tile keep zero weights.
+template <typename T>
+static void pack_lane_weights(const CallerLayout& cl, int n, int nnbr, const T* Dx, const T* Dy, const T* Dz,
+                              const T* L, std::vector<T>& out) {
+    constexpr int U = Quad<T>::kUnits;
+    constexpr int per_unit = 16 / sizeof(T);
+    const long ntiles = (n + kLaneTile - 1) / kLaneTile;
+    out.assign((size_t)ntiles * kSlots * U * kLaneTile * per_unit, T(0));
+    const T* ops[4] = {Dx, Dy, Dz, L};
+    for (long i = 0; i < n; ++i) {
+        const long b = i / kLaneTile, t = i % kLaneTile;
+        for (int j = 0; j < nnbr; ++j) {
+            const long dm = cl.dm(i, j);
+            for (int op = 0; op < 4; ++op) {
+                const int q = op / per_unit, e = op % per_unit;
+                const size_t unit = (((size_t)b * kSlots + j) * U + q) * kLaneTile + t;
+                out[unit * per_unit + e] = ops[op][dm];
+            }
+        }
+    }
+}
+
+// The same gather rows as pack_idx's (already checked), as [tile][slot][32 nodes];
+// nodes past n in the last tile gather row pid0.
+static void pack_lane_idx(const std::vector<int>& packed, int n, int pid0, std::vector<int>& out) {
+    const long ntiles = (n + kLaneTile - 1) / kLaneTile;
+    out.assign((size_t)ntiles * kSlots * kLaneTile, pid0);
+    for (long i = 0; i < n; ++i) {
+        const long b = i / kLaneTile, t = i % kLaneTile;
+        for (int j = 0; j < kSlots; ++j)
+            out[((size_t)b * kSlots + j) * kLaneTile + t] = packed[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)];
+    }
 }
 
 template <typename T>
@@ -149,13 +186,15 @@ struct Plain {
     CallerLayout cl;
     double gh0 = 0, dt = 0;
     void *W = nullptr, *PT = nullptr, *H = nullptr, *Ka = nullptr, *Kb = nullptr, *D = nullptr, *F = nullptr,
-         *Kx = nullptr, *raw = nullptr;
+         *Kx = nullptr, *raw = nullptr, *Wl = nullptr;
     int* idx = nullptr;
+    int* idxl = nullptr;            // node-per-lane kernel: tile-transposed weights / indices
     double* inv = nullptr;
     int* err = nullptr;             // pipelined kernel: bounded-wait error word
     bool tma_ok = false;            // pipelined kernel set up
-    int kernel_choice = 0;          // 0 = bulk-copy pipelined kernel, 1 = register-streaming kernel
-    float tune_us[2] = {0.f, 0.f};  // eval-mode launch time of each kernel at init (pipelined: best tile)
+    int kernel_choice = 0;          // 0 = bulk-copy pipelined, 1 = register-streaming, 2 = node-per-lane kernel
+    float tune_us[3] = {0.f, 0.f, 0.f};  // eval-mode launch time of each kernel at init (its best shape)
+    int lane_lpn = 1;               // node-per-lane kernel: lanes per node (1, 2, 4)
     int tma_tile = 64;              // pipelined kernel: nodes per tile (64: 1 CTA/SM, 32: 2 CTAs/SM)
     int sms = 0;
     cudaStream_t stream = nullptr;
@@ -178,12 +217,15 @@ struct Plain {
         steps_done = 0;
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
-        for (void* p : {W, PT, H, Ka, Kb, D, F, Kx, raw}) if (p) cudaFree(p);
+        for (void* p : {W, PT, H, Ka, Kb, D, F, Kx, raw, Wl}) if (p) cudaFree(p);
         if (idx) cudaFree(idx);
+        if (idxl) cudaFree(idxl);
         if (inv) cudaFree(inv);
         if (err) cudaFree(err);
-        W = PT = H = Ka = Kb = D = F = Kx = raw = nullptr;
+        W = PT = H = Ka = Kb = D = F = Kx = raw = Wl = nullptr;
         idx = nullptr;
+        idxl = nullptr;
+        lane_lpn = 1;
         inv = nullptr;
         err = nullptr;
         tma_ok = false;
@@ -268,9 +310,38 @@ struct Plain {
         }
     }
 
+    template <typename T, int LPN>
+    void launch_lane(const StageArgs<T>& a, int mode) {
+        const LaneArgs<T> la{a, reinterpret_cast<const uint4*>(Wl), idxl};
+        const int units = ceil_div(n, kLaneTile / LPN);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(ceil_div(units, kLaneWarps));
+        cfg.blockDim = dim3(kLaneThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        switch (mode) {
+            case 0: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage0, LPN>, la); break;
+            case 1: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage1, LPN>, la); break;
+            case 2: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage2, LPN>, la); break;
+            case 3: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage3, LPN>, la); break;
+            default: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kEvalOnly, LPN>, la); break;
+        }
+    }
+
     template <typename T>
     void launch_t(int mode) {
         const StageArgs<T> a = args<T>(mode);
+        if (kernel_choice == 2) {
+            if (lane_lpn == 4) launch_lane<T, 4>(a, mode);
+            else if (lane_lpn == 2) launch_lane<T, 2>(a, mode);
+            else launch_lane<T, 1>(a, mode);
+            return;
+        }
         if (use_tma()) {
             if (tma_tile == 32) launch_tma<T, 32>(a, mode);
             else if (tma_tile == 16) launch_tma<T, 16>(a, mode);
@@ -340,6 +411,16 @@ static int upload_static(Plain& P, const void* x, const void* y, const void* z, 
     std::vector<int> ibuf;
     pack_weights<T>(P.cl, P.n, P.nnbr, (const T*)Dx, (const T*)Dy, (const T*)Dz, (const T*)L, wbuf);
     SWE_TRY(pack_idx(P.cl, P.n, P.rows, P.pid0, P.nnbr, idx, ibuf));
+    {
+        std::vector<T> wl;
+        std::vector<int> il;
+        pack_lane_weights<T>(P.cl, P.n, P.nnbr, (const T*)Dx, (const T*)Dy, (const T*)Dz, (const T*)L, wl);
+        pack_lane_idx(ibuf, P.n, P.pid0, il);
+        SWE_CUDA_TRY(cudaMalloc(&P.Wl, wl.size() * sizeof(T)));
+        SWE_CUDA_TRY(cudaMalloc(&P.idxl, il.size() * sizeof(int)));
+        SWE_CUDA_TRY(cudaMemcpy(P.Wl, wl.data(), wl.size() * sizeof(T), cudaMemcpyHostToDevice));
+        SWE_CUDA_TRY(cudaMemcpy(P.idxl, il.data(), il.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     pack_points<T>(P.cl, P.n, (const T*)x, (const T*)y, (const T*)z, (const T*)f, (const T*)ghm, (const T*)pu,
                    (const T*)pv, (const T*)pw, (const T*)gg, pbuf);
     SWE_CUDA_TRY(cudaMalloc(&P.W, wbuf.size() * sizeof(T)));
@@ -483,20 +564,23 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
     P.grid = std::max(1, std::min(want, sms * std::max(per_sm, 1)));
     P.sms = sms;
     P.ready = true;
-    // The stage kernels do identical arithmetic; keep the fastest for this patch:
-    // the register kernel, or the pipelined kernel with 64- or 32-node tiles (the
-    // pipelined kernel wins once every SM has many tiles).
+    // Keep the fastest stage kernel for this patch: the pipelined kernel with 64-,
+    // 32- or 16-node tiles, the register kernel, or the node-per-lane kernel with
+    // 1, 2 or 4 lanes per node.  (The first two do identical arithmetic; the
+    // node-per-lane kernel sums each node's slots in a different order.)
     {
         cudaEvent_t e0, e1;
         SWE_CUDA_TRY(cudaEventCreate(&e0));
         SWE_CUDA_TRY(cudaEventCreate(&e1));
         SWE_CUDA_TRY(cudaMemsetAsync(P.Kx, 0, srow, P.stream));
-        constexpr int kCand = 4;
-        const int cand_kernel[kCand] = {0, 0, 0, 1}, cand_tile[kCand] = {64, 32, 16, 64};
-        float us_c[kCand] = {0.f, 0.f, 0.f, 0.f};
+        constexpr int kCand = 7;
+        const int cand_kernel[kCand] = {0, 0, 0, 1, 2, 2, 2}, cand_tile[kCand] = {64, 32, 16, 64, 64, 64, 64};
+        const int cand_lpn[kCand] = {1, 1, 1, 1, 1, 2, 4};
+        float us_c[kCand] = {};
         for (int c = 0; c < kCand; ++c) {
             P.kernel_choice = cand_kernel[c];
             P.tma_tile = cand_tile[c];
+            P.lane_lpn = cand_lpn[c];
             for (int w = 0; w < 2; ++w) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
             SWE_CUDA_TRY(cudaEventRecord(e0, P.stream));
             for (int r = 0; r < 5; ++r) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
@@ -510,14 +594,22 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
         count_launch(7 * kCand);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        // the pipelined kernel keeps its fastest tile, also when the register kernel wins
-        int bt = 0;
-        for (int c = 1; c < kCand - 1; ++c)
+        // the pipelined and node-per-lane kernels keep their fastest shapes, also
+        // when another kernel wins
+        int bt = 0, bl = 4;
+        for (int c = 1; c < 3; ++c)
             if (us_c[c] < us_c[bt]) bt = c;
+        for (int c = 5; c < kCand; ++c)
+            if (us_c[c] < us_c[bl]) bl = c;
         P.tma_tile = cand_tile[bt];
+        P.lane_lpn = cand_lpn[bl];
         P.tune_us[0] = us_c[bt];
-        P.tune_us[1] = us_c[kCand - 1];
-        P.kernel_choice = P.tune_us[1] < P.tune_us[0] ? 1 : 0;
+        P.tune_us[1] = us_c[3];
+        P.tune_us[2] = us_c[bl];
+        int best = 0;
+        for (int k = 1; k < 3; ++k)
+            if (P.tune_us[k] < P.tune_us[best]) best = k;
+        P.kernel_choice = best;
         SWE_TRY(check_tma_err());
     }
     if ((st = P.build_graph()) != SWE_OK) return st;
@@ -613,18 +705,22 @@ int swe_cuda_sync(void) {
 
 int swe_cuda_select_kernel(int which) {
     SWE_TRY(require_ready());
-    if (which < 0 || which > 4) {
+    if (which < 0 || which > 8) {
         set_error("swe_cuda_select_kernel: 0 (pipelined), 1 (register), 2 / 3 / 4 (pipelined, 64 / 32 / 16-node tiles), "
-                  "got %d", which);
+                  "5 (node-per-lane), 6 / 7 / 8 (node-per-lane, 1 / 2 / 4 lanes per node), got %d", which);
         return SWE_ERR_ARG;
     }
     Plain& P = g_plain;
-    if (which != 1 && !P.tma_ok) { set_error("swe_cuda_select_kernel: the pipelined kernel is not set up"); return SWE_ERR_STATE; }
+    const bool piped = which == 0 || (which >= 2 && which <= 4);
+    if (piped && !P.tma_ok) { set_error("swe_cuda_select_kernel: the pipelined kernel is not set up"); return SWE_ERR_STATE; }
     SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
-    P.kernel_choice = which == 1 ? 1 : 0;
+    P.kernel_choice = piped ? 0 : (which == 1 ? 1 : 2);
     if (which == 2) P.tma_tile = 64;
     if (which == 3) P.tma_tile = 32;
     if (which == 4) P.tma_tile = 16;
+    if (which == 6) P.lane_lpn = 1;
+    if (which == 7) P.lane_lpn = 2;
+    if (which == 8) P.lane_lpn = 4;
     if (P.graph) cudaGraphExecDestroy(P.graph);
     P.graph = nullptr;
     return P.build_graph();
@@ -633,10 +729,12 @@ int swe_cuda_select_kernel(int which) {
 int swe_cuda_kernel_info(int* out) {
     SWE_TRY(require_ready());
     if (!out) { set_error("null out"); return SWE_ERR_ARG; }
-    out[0] = g_plain.use_tma() ? 0 : 1;
+    out[0] = g_plain.kernel_choice;
     out[1] = g_plain.tma_ok ? g_plain.tma_tile : 0;
     out[2] = (int)(g_plain.tune_us[0] * 1000.f);   // nanoseconds per eval launch, pipelined
     out[3] = (int)(g_plain.tune_us[1] * 1000.f);   // register-streaming
+    out[4] = g_plain.lane_lpn;
+    out[5] = (int)(g_plain.tune_us[2] * 1000.f);   // node-per-lane
     return SWE_OK;
 }
 

@@ -9,7 +9,9 @@ Parity bars:
   reference's own verify_output criterion, |H - H_100| <= 1e-9 (FP64) and
   <= 4e-2 (FP32) absolute (swe_config.h:80, :88);
 * the stage-by-stage API and the graph-captured step are bit-identical, and
-  reruns are bit-identical.
+  reruns are bit-identical;
+* the pipelined and register kernels agree bit for bit; the node-per-lane
+  kernel (another slot order) meets the same oracle bars.
 """
 import os
 
@@ -200,11 +202,47 @@ def test_pipelined_and_register_kernels_agree_bitwise(plain, prec):
         assert rel_err(F0, oracle.Port(m, "fp64").eval_rhs(K)).max() <= 1e-12
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_lane_kernel_matches_oracle(plain, prec):
+    """The node-per-lane kernel sums each node's slots serially per lane (1, 2 or 4
+    lanes per node) instead of in the 8-lane tree, so it is held to the oracle's bars
+    rather than to the other kernels' bits: eval_rhs within 1e-12 relative and a few
+    ulps of the condition scale (FP64), FP32 within the FP32 condition bound, and
+    7 RK4 steps within 1e-12 of the register kernel (FP64)."""
+    _, d = generated_input(6)
+    m, _ = layout.prepare(swe_input.to_model(d), use_rcm=True, simd_length=32)
+    plain.init_model(m, prec)
+    dt = np.float64 if prec == "fp64" else np.float32
+    K = _perturbed(m.H_init).astype(dt)
+    F64 = oracle.Port(m, "fp64").eval_rhs(K.astype(np.float64))
+    plain.select_kernel(1)
+    plain.set_state(m.H_init.astype(dt))
+    plain.step(7)
+    H_reg = plain.get_state().reshape(-1, 4)
+    for which, lpn in ((6, 1), (7, 2), (8, 4)):
+        plain.select_kernel(which)
+        info = plain.kernel_info()
+        assert info["in_use"] == "lane" and info["lanes_per_node"] == lpn
+        F = plain.eval_rhs(K)
+        if prec == "fp64":
+            assert rel_err(F, F64).max() <= 1e-12, lpn
+            assert cond_err(F, F64, m, K) <= 4e-16, lpn
+        else:
+            assert cond_err(F, F64, m, K) <= 4e-6, lpn
+        plain.set_state(m.H_init.astype(dt))
+        plain.step(7)
+        H = plain.get_state().reshape(-1, 4)
+        assert np.isfinite(H).all()
+        if prec == "fp64":
+            assert rel_err(H, H_reg).max() <= 1e-12, lpn
+
+
 def test_select_kernel_rejects_unknown_choice(plain, grid_l4):
     _, d = grid_l4
     plain.init_model(swe_input.to_model(d), "fp64")
-    with pytest.raises(capi.SweError):
-        plain.select_kernel(7)
+    for bad in (-1, 9):
+        with pytest.raises(capi.SweError):
+            plain.select_kernel(bad)
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
@@ -218,7 +256,7 @@ def test_short_stencils_match_oracle(plain, prec):
     dt = np.float64 if prec == "fp64" else np.float32
     K = _perturbed(m.H_init).astype(dt)
     port = oracle.Port(m, prec)
-    for which in (1, 2, 3, 4):                  # register, pipelined 64 / 32 / 16
+    for which in (1, 2, 3, 4, 6, 7, 8):         # register, pipelined 64 / 32 / 16, node-per-lane 1 / 2 / 4
         plain.select_kernel(which)
         F = plain.eval_rhs(K)
         want = port.eval_rhs(K)
