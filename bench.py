@@ -9,11 +9,14 @@ A step is one full RK4 step (4 fused stage kernels) of one state.
 
 One JSON line on rank 0.  `value` = node-stage updates/s (4 * N * steps / s)
 with the state resident in HBM, timed with CUDA events around each step on the
-library's stream, L2 flushed (a 256 MB write) between timed steps; `e2e` = the
+library's stream, L2 flushed between timed steps (a 256 MB write, then a 256 MB
+read so that the write's dirty lines are written back before the step: each
+step starts from a cold, clean L2); `e2e` = the
 same metric through the C ABI with host buffers (pinned H2D of the state,
 one RK4 step, D2H of the state every step); `roofline` = the fused stage
 kernel's algorithmic bytes (1396 B per FP64 node-stage, 760 B FP32) over its
-CUDA-event duration against the measured HBM copy bandwidth.  Multi-GPU runs
+average duration in the timed region (a timed step is the four stage kernels and
+nothing else, so step time / 4) against the measured HBM copy bandwidth.  Multi-GPU runs
 are independent replicas (the path does not shard across GPUs here): every
 rank steps its own state, time is the max over ranks, value is the sum.
 
@@ -55,7 +58,11 @@ ALG_BYTES = {"fp64": 1396, "fp32": 760}      # per node-stage (FP64: 4*31*8+31*4
 # plus per member 4*4 (K read once) + 14*4 (RK combine) + 4 (FP64 h registers)
 ENS_SHARED_BYTES = 4 * 31 * 4 + 31 * 4 + 17 * 4
 ENS_MEMBER_BYTES = 4 * 4 + 14 * 4 + 4
+# --plain-kernel choices -> swe_cuda_select_kernel codes
+PLAIN_KERNELS = {"auto": None, "register": 1, "pipelined64": 2, "pipelined32": 3, "pipelined16": 4,
+                 "lane1": 6, "lane2": 7, "lane4": 8, "lane1pf": 9, "lane2pf": 10, "lane4pf": 11}
 L2_FLUSH_BYTES = 256 << 20
+L2_NOTE = "flushed between timed steps: 256 MB write, then 256 MB read (cold, clean L2 at each step)"
 # DRAM bytes (read + write) per launch of the dominant kernel, from ncu captures of the same
 # command (dram__bytes_read.sum + dram__bytes_write.sum, averaged over the captured launches);
 # the profile summaries under profiles/ give the commands.
@@ -67,6 +74,25 @@ TRAFFIC_BYTES = {
     "ens_tf32_n163842_b64": 1041.20e6,  # swe::ens_stage_kernel<64, stage, 3xTF32>, 12 launches
     "ens_bf16_n163842_b64": 1041.46e6,  # swe::ens_stage_kernel<64, stage, BF16>, 12 launches
 }
+
+
+class L2Flush:
+    """Run between timed steps, untimed: a 256 MB write evicts every line of the
+    126 MB L2, and a 256 MB read then replaces the write's dirty lines, so their
+    write-back is not charged to the next step.  The step starts from an L2 that
+    holds none of its data."""
+
+    def __init__(self, device):
+        import torch
+
+        self.torch = torch
+        self.wr = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+        self.rd = torch.zeros(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+        self.out = torch.empty((), dtype=torch.float32, device=device)
+
+    def __call__(self):
+        self.wr.zero_()
+        self.torch.sum(self.rd, dim=0, out=self.out)
 
 
 def log(*a):
@@ -293,7 +319,7 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
     tune_ms = ens.tune().tolist()
     cfg = ens.config()
     stream = torch.cuda.ExternalStream(ens.stream())
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    flush = L2Flush(f"cuda:{local}")
     for _ in range(args.warmup):
         ens.step(1)
     ens.sync()
@@ -308,7 +334,7 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
         torch.cuda.profiler.start()
         with torch.cuda.stream(stream):
             for s in range(args.steps):
-                flush.zero_()
+                flush()
                 starts[s].record(stream)
                 ens.step(1)
                 stops[s].record(stream)
@@ -387,7 +413,7 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
             "data": "synthetic (seeded icosahedral grid, PHS RBF-FD weights, TC5 ICs, per-member 1e-3 h noise)",
             "config": {"workload": args.workload, "description": desc, "nodes": N, "members": members,
                        "dt": d.dt, "kernel_variant": cfg, "tune_ms_per_step": tune_ms,
-                       "l2": "flushed (256 MB write) between timed steps"},
+                       "l2": L2_NOTE},
             "plain_fp64_member_steps_per_s": plain_steps,
             "ratio_vs_plain_fp64": member_steps / plain_steps,
             "h_err_vs_fp64": {"steps": args.err_steps, "members": err_members,
@@ -490,6 +516,9 @@ def main():
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--budget-gb", type=float, default=80.0)
+    ap.add_argument("--plain-kernel", default="auto", choices=sorted(PLAIN_KERNELS),
+                    help="plain stage kernel: auto = the one swe_cuda_init timed fastest; the others pin a kernel "
+                         "and shape (for profiling runs, where the init-time timing is not representative)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     level, prec, desc = WORKLOADS[args.workload]
@@ -515,8 +544,10 @@ def main():
     plain = capi.Plain()
     capi.check("swe_cuda_select_device", plain.lib.swe_cuda_select_device(local))
     plain.init_model(pm, prec)
+    if args.plain_kernel != "auto":
+        plain.select_kernel(PLAIN_KERNELS[args.plain_kernel])
     stream = torch.cuda.ExternalStream(plain.stream())
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    flush = L2Flush(f"cuda:{local}")
 
     plain.set_state(pm.H_init)
     for _ in range(args.warmup):
@@ -535,7 +566,7 @@ def main():
         torch.cuda.profiler.start()                 # a profiler run with --profile-from-start off sees this loop only
         with torch.cuda.stream(stream):
             for s in range(args.steps):
-                flush.zero_()                       # L2 flush between timed steps (not timed)
+                flush()                       # L2 flush between timed steps (not timed)
                 starts[s].record(stream)
                 plain.step(1)
                 stops[s].record(stream)
@@ -551,7 +582,7 @@ def main():
         plain.set_timing(True)
         with torch.cuda.stream(stream):
             for s in range(max(3, args.steps // 4)):
-                flush.zero_()
+                flush()
                 for st in range(4):
                     plain.rk_substep(st)
         k_time, k_launches, _ = plain.timings()
@@ -589,14 +620,19 @@ def main():
 
     # ---- roofline of the fused stage kernel ------------------------------------------
     peak, peak_kind = measured_peak_hbm()
-    t_kernel = k_time / max(k_launches, 1)
+    # a timed step is the four stage kernels and nothing else: their average
+    # duration in the timed region is step time / 4 (stages overlap by
+    # programmatic dependent launch, which per-launch events would break up)
+    t_kernel = t_total / (4 * args.steps)
+    t_isolated = k_time / max(k_launches, 1)
     achieved = ALG_BYTES[prec] * N / t_kernel / 1e9
     kinfo = plain.kernel_info()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(args.workload), "peak_source": peak_kind,
                 "kernel": {"pipelined": "swe::stage_tma_kernel", "register": "swe::stage_kernel",
                            "lane": "swe::stage_lane_kernel"}[kinfo["in_use"]],
-                "kernel_us": round(t_kernel * 1e6, 2), "alg_bytes_per_node_stage": ALG_BYTES[prec],
+                "kernel_us": round(t_kernel * 1e6, 2), "kernel_us_isolated": round(t_isolated * 1e6, 2),
+                "alg_bytes_per_node_stage": ALG_BYTES[prec],
                 "kernel_choice": kinfo}
 
     cpu = None
@@ -615,7 +651,7 @@ def main():
             "data": "synthetic (seeded icosahedral grid, PHS RBF-FD weights, TC5 Gaussian-mountain ICs)",
             "config": {"workload": args.workload, "description": desc, "nodes": N, "nnbr": 31, "dt": d.dt,
                        "layout": "CFDL", "rcm": True, "parallelism": f"replicas x{world}",
-                       "l2": "flushed (256 MB write) between timed steps"},
+                       "l2": L2_NOTE},
             "e2e": {"value": e2e, "unit": "node-stage updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
             "gpu_launches": int(launches),

@@ -195,6 +195,7 @@ struct Plain {
     int kernel_choice = 0;          // 0 = bulk-copy pipelined, 1 = register-streaming, 2 = node-per-lane kernel
     float tune_us[3] = {0.f, 0.f, 0.f};  // eval-mode launch time of each kernel at init (its best shape)
     int lane_lpn = 1;               // node-per-lane kernel: lanes per node (1, 2, 4)
+    int lane_pf = 0;                // node-per-lane kernel: bulk L2 prefetch at warp start
     int tma_tile = 64;              // pipelined kernel: nodes per tile (64: 1 CTA/SM, 32: 2 CTAs/SM)
     int sms = 0;
     cudaStream_t stream = nullptr;
@@ -226,6 +227,7 @@ struct Plain {
         idx = nullptr;
         idxl = nullptr;
         lane_lpn = 1;
+        lane_pf = 0;
         inv = nullptr;
         err = nullptr;
         tma_ok = false;
@@ -312,7 +314,7 @@ struct Plain {
 
     template <typename T, int LPN>
     void launch_lane(const StageArgs<T>& a, int mode) {
-        const LaneArgs<T> la{a, reinterpret_cast<const uint4*>(Wl), idxl};
+        const LaneArgs<T> la{a, reinterpret_cast<const uint4*>(Wl), idxl, lane_pf};
         const int units = ceil_div(n, kLaneTile / LPN);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(ceil_div(units, kLaneWarps));
@@ -573,14 +575,17 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
         SWE_CUDA_TRY(cudaEventCreate(&e0));
         SWE_CUDA_TRY(cudaEventCreate(&e1));
         SWE_CUDA_TRY(cudaMemsetAsync(P.Kx, 0, srow, P.stream));
-        constexpr int kCand = 7;
-        const int cand_kernel[kCand] = {0, 0, 0, 1, 2, 2, 2}, cand_tile[kCand] = {64, 32, 16, 64, 64, 64, 64};
-        const int cand_lpn[kCand] = {1, 1, 1, 1, 1, 2, 4};
+        constexpr int kCand = 10;
+        const int cand_kernel[kCand] = {0, 0, 0, 1, 2, 2, 2, 2, 2, 2};
+        const int cand_tile[kCand] = {64, 32, 16, 64, 64, 64, 64, 64, 64, 64};
+        const int cand_lpn[kCand] = {1, 1, 1, 1, 1, 2, 4, 1, 2, 4};
+        const int cand_pf[kCand] = {0, 0, 0, 0, 0, 0, 0, 1, 1, 1};
         float us_c[kCand] = {};
         for (int c = 0; c < kCand; ++c) {
             P.kernel_choice = cand_kernel[c];
             P.tma_tile = cand_tile[c];
             P.lane_lpn = cand_lpn[c];
+            P.lane_pf = cand_pf[c];
             for (int w = 0; w < 2; ++w) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
             SWE_CUDA_TRY(cudaEventRecord(e0, P.stream));
             for (int r = 0; r < 5; ++r) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
@@ -603,6 +608,7 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
             if (us_c[c] < us_c[bl]) bl = c;
         P.tma_tile = cand_tile[bt];
         P.lane_lpn = cand_lpn[bl];
+        P.lane_pf = cand_pf[bl];
         P.tune_us[0] = us_c[bt];
         P.tune_us[1] = us_c[3];
         P.tune_us[2] = us_c[bl];
@@ -705,9 +711,10 @@ int swe_cuda_sync(void) {
 
 int swe_cuda_select_kernel(int which) {
     SWE_TRY(require_ready());
-    if (which < 0 || which > 8) {
+    if (which < 0 || which > 11) {
         set_error("swe_cuda_select_kernel: 0 (pipelined), 1 (register), 2 / 3 / 4 (pipelined, 64 / 32 / 16-node tiles), "
-                  "5 (node-per-lane), 6 / 7 / 8 (node-per-lane, 1 / 2 / 4 lanes per node), got %d", which);
+                  "5 (node-per-lane), 6 / 7 / 8 (node-per-lane, 1 / 2 / 4 lanes per node), 9 / 10 / 11 (the same "
+                  "with L2 prefetch), got %d", which);
         return SWE_ERR_ARG;
     }
     Plain& P = g_plain;
@@ -718,9 +725,10 @@ int swe_cuda_select_kernel(int which) {
     if (which == 2) P.tma_tile = 64;
     if (which == 3) P.tma_tile = 32;
     if (which == 4) P.tma_tile = 16;
-    if (which == 6) P.lane_lpn = 1;
-    if (which == 7) P.lane_lpn = 2;
-    if (which == 8) P.lane_lpn = 4;
+    if (which >= 6) {
+        P.lane_lpn = 1 << ((which - 6) % 3);
+        P.lane_pf = which >= 9 ? 1 : 0;
+    }
     if (P.graph) cudaGraphExecDestroy(P.graph);
     P.graph = nullptr;
     return P.build_graph();
@@ -735,6 +743,7 @@ int swe_cuda_kernel_info(int* out) {
     out[3] = (int)(g_plain.tune_us[1] * 1000.f);   // register-streaming
     out[4] = g_plain.lane_lpn;
     out[5] = (int)(g_plain.tune_us[2] * 1000.f);   // node-per-lane
+    out[6] = g_plain.lane_pf;
     return SWE_OK;
 }
 

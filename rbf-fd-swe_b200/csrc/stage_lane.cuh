@@ -34,6 +34,7 @@ struct LaneArgs {
     StageArgs<T> s;
     const uint4* Wl;   // [tile][slot][unit][32 nodes] 16-byte units (FP64: (Dx,Dy), (Dz,L); FP32: all four)
     const int* idxl;   // [tile][slot][32 nodes] gather rows
+    int l2_prefetch;   // 1: bulk L2 prefetch of each warp's contiguous blocks at its start
 };
 
 namespace lane {
@@ -57,6 +58,10 @@ __device__ __forceinline__ float4 ld_stream(const float4* p) {
                  : "l"(p));
     return v;
 }
+// L2 prefetch of a contiguous block (16-byte aligned address and size); completes on its own
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 // the four weights (Dx, Dy, Dz, L) of one slot of node t; units of a slot are 32 x 16 bytes apart
 __device__ __forceinline__ void weights(const uint4* u, double (&w)[4]) {
     const double2 a = ld_stream(reinterpret_cast<const double2*>(u));
@@ -79,9 +84,33 @@ __global__ void __launch_bounds__(kLaneThreads, 4) stage_lane_kernel(const LaneA
     const int lane = threadIdx.x & 31;
     const int tl = lane % kNpw, sub = lane / kNpw;
     const long node0 = ((long)blockIdx.x * kLaneWarps + (threadIdx.x >> 5)) * kNpw;
+    const int nvalid = (int)min((long)kNpw, (long)a.n - node0);
+    // With l2_prefetch, one lane requests the warp's contiguous blocks into L2 up
+    // front, so that the loads below wait on L2 rather than DRAM: this warp's share
+    // of its tile's weight and index blocks (static: before the wait, overlapping
+    // the previous stage), then its pointwise records and own / H / D rows.  That
+    // pays on small patches (latency-bound); on large ones the extra requests
+    // compete with the demand loads, so the init-time timing decides.
+    constexpr uint32_t kTileW = kSlots * U * kLaneTile * 16, kTileI = kSlots * kLaneTile * 4;
+    const bool pf = la.l2_prefetch != 0;
+    if (pf && lane == 0 && nvalid > 0) {
+        const long tb = node0 / kLaneTile;
+        const int wt = (int)(node0 % kLaneTile) / kNpw;        // warp within its tile
+        lane::prefetch_l2(reinterpret_cast<const unsigned char*>(la.Wl) + tb * kTileW + wt * (kTileW / LPN), kTileW / LPN);
+        lane::prefetch_l2(reinterpret_cast<const unsigned char*>(la.idxl) + tb * kTileI + wt * (kTileI / LPN), kTileI / LPN);
+        lane::prefetch_l2(a.PT + node0 * kPointStride, (uint32_t)(nvalid * kPointStride * sizeof(T)));
+    }
     lane::pdl_wait();          // neighbour states and H / D come from the previous stage
     lane::pdl_trigger();
-    if (node0 >= a.n) return;
+    if (nvalid <= 0) return;
+    if (pf && lane == 0) {
+        const uint32_t rows = (uint32_t)(nvalid * 4 * sizeof(T));
+        lane::prefetch_l2(a.Kin + 4 * (node0 + a.pid0), rows);
+        if (MODE != kStage0 && MODE != kEvalOnly) {
+            lane::prefetch_l2(a.H + 4 * node0, rows);
+            lane::prefetch_l2(a.D + 4 * node0, rows);
+        }
+    }
     // a warp's nodes lie in one tile of the packed arrays (kNpw divides 32); nodes
     // past n in the last tile have zero weights and gather a valid row
     const long i = node0 + tl;

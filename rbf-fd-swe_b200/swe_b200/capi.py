@@ -213,14 +213,14 @@ class Plain:
     def select_kernel(self, which: int) -> None:
         """0: bulk-copy pipelined stage kernel, 1: register-streaming kernel, 2 / 3 / 4: pipelined with
         64- / 32- / 16-node tiles, 5: node-per-lane kernel, 6 / 7 / 8: node-per-lane with 1 / 2 / 4 lanes
-        per node."""
+        per node, 9 / 10 / 11: the same with the bulk L2 prefetch."""
         check("swe_cuda_select_kernel", self.lib.swe_cuda_select_kernel(int(which)))
 
     def kernel_info(self) -> dict:
-        out = np.zeros(6, dtype=np.int32)
+        out = np.zeros(7, dtype=np.int32)
         check("swe_cuda_kernel_info", self.lib.swe_cuda_kernel_info(_p(out)))
         return {"in_use": ("pipelined", "register", "lane")[int(out[0])], "pipelined_available": bool(out[1]),
-                "pipelined_tile": int(out[1]), "lanes_per_node": int(out[4]),
+                "pipelined_tile": int(out[1]), "lanes_per_node": int(out[4]), "l2_prefetch": bool(out[6]),
                 "tune_us": {"pipelined": out[2] / 1e3, "register": out[3] / 1e3, "lane": out[5] / 1e3}}
 
     def invariants(self) -> np.ndarray:
