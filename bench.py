@@ -67,12 +67,15 @@ L2_NOTE = "flushed between timed steps: 256 MB write, then 256 MB read (cold, cl
 # command (dram__bytes_read.sum + dram__bytes_write.sum, averaged over the captured launches);
 # the profile summaries under profiles/ give the commands.
 TRAFFIC_BYTES = {
-    "plain_fp64_n40962": 57.09e6,       # swe::stage_kernel (register form), 8 launches, stages 0-3
-    "plain_fp64_n163842": 233.53e6,     # swe::stage_tma_kernel, 12 launches of the timed region
-    "plain_fp64_n655362": 945.25e6,     # swe::stage_tma_kernel, 12 launches
-    "plain_fp32_n655362": 512.92e6,     # swe::stage_tma_kernel, 12 launches
-    "ens_tf32_n163842_b64": 1041.20e6,  # swe::ens_stage_kernel<64, stage, 3xTF32>, 12 launches
-    "ens_bf16_n163842_b64": 1041.46e6,  # swe::ens_stage_kernel<64, stage, BF16>, 12 launches
+    # DRAM read + write bytes per stage launch, mean over 8 launches of the timed
+    # steps (ncu --cache-control none inside the bench's own flushed loop, so
+    # stage 0 of each step starts cold and stages 1-3 see what L2 kept)
+    "plain_fp64_n40962": 32.50e6,       # swe::stage_lane_kernel<double, *, 2>, L2 prefetch on
+    "plain_fp64_n163842": 197.34e6,     # swe::stage_lane_kernel<double, *, 2>
+    "plain_fp64_n655362": 948.31e6,     # swe::stage_lane_kernel<double, *, 2>
+    "plain_fp32_n655362": 506.57e6,     # swe::stage_lane_kernel<float, *, 1>
+    "ens_tf32_n163842_b64": 1041.20e6,  # swe::ens_stage_kernel<64, stage, 3xTF32>, 12 launches (cold)
+    "ens_bf16_n163842_b64": 1041.46e6,  # swe::ens_stage_kernel<64, stage, BF16>, 12 launches (cold)
 }
 
 
