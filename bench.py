@@ -58,9 +58,11 @@ ALG_BYTES = {"fp64": 1396, "fp32": 760}      # per node-stage (FP64: 4*31*8+31*4
 # plus per member 4*4 (K read once) + 14*4 (RK combine) + 4 (FP64 h registers)
 ENS_SHARED_BYTES = 4 * 31 * 4 + 31 * 4 + 17 * 4
 ENS_MEMBER_BYTES = 4 * 4 + 14 * 4 + 4
-# --plain-kernel choices -> swe_cuda_select_kernel codes
+# --plain-kernel choices -> swe_cuda_select_kernel codes (laneN: N lanes per node at 4 CTAs per
+# SM; "w": 5 CTAs per SM; "pf": with the L2 prefetch)
 PLAIN_KERNELS = {"auto": None, "register": 1, "pipelined64": 2, "pipelined32": 3, "pipelined16": 4,
-                 "lane1": 6, "lane2": 7, "lane4": 8, "lane1pf": 9, "lane2pf": 10, "lane4pf": 11}
+                 "lane1": 6, "lane2": 7, "lane4": 8, "lane1w": 9, "lane2w": 10, "lane4w": 11,
+                 "lane1pf": 12, "lane2pf": 13, "lane4pf": 14, "lane1wpf": 15, "lane2wpf": 16, "lane4wpf": 17}
 L2_FLUSH_BYTES = 256 << 20
 L2_NOTE = "flushed between timed steps: 256 MB write, then 256 MB read (cold, clean L2 at each step)"
 # DRAM bytes (read + write) per launch of the dominant kernel, from ncu captures of the same
@@ -70,10 +72,10 @@ TRAFFIC_BYTES = {
     # DRAM read + write bytes per stage launch, mean over 8 launches of the timed
     # steps (ncu --cache-control none inside the bench's own flushed loop, so
     # stage 0 of each step starts cold and stages 1-3 see what L2 kept)
-    "plain_fp64_n40962": 32.50e6,       # swe::stage_lane_kernel<double, *, 2>, L2 prefetch on
-    "plain_fp64_n163842": 197.34e6,     # swe::stage_lane_kernel<double, *, 2>
-    "plain_fp64_n655362": 948.31e6,     # swe::stage_lane_kernel<double, *, 2>
-    "plain_fp32_n655362": 506.57e6,     # swe::stage_lane_kernel<float, *, 1>
+    "plain_fp64_n40962": 32.50e6,       # swe::stage_lane_kernel<double, *, 2, 4>, L2 prefetch on
+    "plain_fp64_n163842": 197.34e6,     # swe::stage_lane_kernel<double, *, 2, 4>
+    "plain_fp64_n655362": 948.31e6,     # swe::stage_lane_kernel<double, *, 2, 4>
+    "plain_fp32_n655362": 506.57e6,     # swe::stage_lane_kernel<float, *, 1, 4>
     "ens_tf32_n163842_b64": 1041.20e6,  # swe::ens_stage_kernel<64, stage, 3xTF32>, 12 launches (cold)
     "ens_bf16_n163842_b64": 1041.46e6,  # swe::ens_stage_kernel<64, stage, BF16>, 12 launches (cold)
 }

@@ -196,6 +196,7 @@ struct Plain {
     float tune_us[3] = {0.f, 0.f, 0.f};  // eval-mode launch time of each kernel at init (its best shape)
     int lane_lpn = 1;               // node-per-lane kernel: lanes per node (1, 2, 4)
     int lane_pf = 0;                // node-per-lane kernel: bulk L2 prefetch at warp start
+    int lane_minb = 4;              // node-per-lane kernel: CTAs per SM of its register bound (4, 5)
     int tma_tile = 64;              // pipelined kernel: nodes per tile (64: 1 CTA/SM, 32: 2 CTAs/SM)
     int sms = 0;
     cudaStream_t stream = nullptr;
@@ -228,6 +229,7 @@ struct Plain {
         idxl = nullptr;
         lane_lpn = 1;
         lane_pf = 0;
+        lane_minb = 4;
         inv = nullptr;
         err = nullptr;
         tma_ok = false;
@@ -312,7 +314,7 @@ struct Plain {
         }
     }
 
-    template <typename T, int LPN>
+    template <typename T, int LPN, int MINB>
     void launch_lane(const StageArgs<T>& a, int mode) {
         const LaneArgs<T> la{a, reinterpret_cast<const uint4*>(Wl), idxl, lane_pf};
         const int units = ceil_div(n, kLaneTile / LPN);
@@ -327,11 +329,11 @@ struct Plain {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         switch (mode) {
-            case 0: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage0, LPN>, la); break;
-            case 1: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage1, LPN>, la); break;
-            case 2: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage2, LPN>, la); break;
-            case 3: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage3, LPN>, la); break;
-            default: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kEvalOnly, LPN>, la); break;
+            case 0: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage0, LPN, MINB>, la); break;
+            case 1: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage1, LPN, MINB>, la); break;
+            case 2: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage2, LPN, MINB>, la); break;
+            case 3: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage3, LPN, MINB>, la); break;
+            default: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kEvalOnly, LPN, MINB>, la); break;
         }
     }
 
@@ -339,9 +341,15 @@ struct Plain {
     void launch_t(int mode) {
         const StageArgs<T> a = args<T>(mode);
         if (kernel_choice == 2) {
-            if (lane_lpn == 4) launch_lane<T, 4>(a, mode);
-            else if (lane_lpn == 2) launch_lane<T, 2>(a, mode);
-            else launch_lane<T, 1>(a, mode);
+            if (lane_minb == 5) {
+                if (lane_lpn == 4) launch_lane<T, 4, 5>(a, mode);
+                else if (lane_lpn == 2) launch_lane<T, 2, 5>(a, mode);
+                else launch_lane<T, 1, 5>(a, mode);
+            } else {
+                if (lane_lpn == 4) launch_lane<T, 4, 4>(a, mode);
+                else if (lane_lpn == 2) launch_lane<T, 2, 4>(a, mode);
+                else launch_lane<T, 1, 4>(a, mode);
+            }
             return;
         }
         if (use_tma()) {
@@ -393,6 +401,15 @@ struct Plain {
 };
 
 static Plain g_plain;
+
+// Node-per-lane shape s in 0..11 (swe_cuda_select_kernel's 6 + s): lanes per node
+// 1 / 2 / 4 = s % 3, 5 CTAs per SM when (s / 3) % 2, L2 prefetch when s >= 6.
+static void lane_shape(Plain& P, int s) {
+    P.kernel_choice = 2;
+    P.lane_lpn = 1 << (s % 3);
+    P.lane_minb = (s / 3) % 2 ? 5 : 4;
+    P.lane_pf = s >= 6 ? 1 : 0;
+}
 
 template <typename T, int TILE>
 static int set_tma_attrs() {
@@ -575,40 +592,37 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
         SWE_CUDA_TRY(cudaEventCreate(&e0));
         SWE_CUDA_TRY(cudaEventCreate(&e1));
         SWE_CUDA_TRY(cudaMemsetAsync(P.Kx, 0, srow, P.stream));
-        constexpr int kCand = 10;
-        const int cand_kernel[kCand] = {0, 0, 0, 1, 2, 2, 2, 2, 2, 2};
-        const int cand_tile[kCand] = {64, 32, 16, 64, 64, 64, 64, 64, 64, 64};
-        const int cand_lpn[kCand] = {1, 1, 1, 1, 1, 2, 4, 1, 2, 4};
-        const int cand_pf[kCand] = {0, 0, 0, 0, 0, 0, 0, 1, 1, 1};
+        // candidates 0-2: pipelined 64 / 32 / 16; 3: register; 4-15: node-per-lane
+        // shape 6 + (c - 4) in swe_cuda_select_kernel's numbering
+        constexpr int kLane0 = 4, kCand = kLane0 + 12;
+        const int cand_tile[3] = {64, 32, 16};
         float us_c[kCand] = {};
         for (int c = 0; c < kCand; ++c) {
-            P.kernel_choice = cand_kernel[c];
-            P.tma_tile = cand_tile[c];
-            P.lane_lpn = cand_lpn[c];
-            P.lane_pf = cand_pf[c];
+            if (c < 3) { P.kernel_choice = 0; P.tma_tile = cand_tile[c]; }
+            else if (c == 3) P.kernel_choice = 1;
+            else lane_shape(P, c - kLane0);
             for (int w = 0; w < 2; ++w) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
             SWE_CUDA_TRY(cudaEventRecord(e0, P.stream));
-            for (int r = 0; r < 5; ++r) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
+            for (int r = 0; r < 10; ++r) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
             SWE_CUDA_TRY(cudaEventRecord(e1, P.stream));
             SWE_CUDA_TRY(cudaEventSynchronize(e1));
             SWE_CUDA_TRY(cudaGetLastError());
             float ms = 0.f;
             SWE_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-            us_c[c] = ms * 1e3f / 5.f;
+            us_c[c] = ms * 1e3f / 10.f;
         }
-        count_launch(7 * kCand);
+        count_launch(12 * kCand);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         // the pipelined and node-per-lane kernels keep their fastest shapes, also
         // when another kernel wins
-        int bt = 0, bl = 4;
+        int bt = 0, bl = kLane0;
         for (int c = 1; c < 3; ++c)
             if (us_c[c] < us_c[bt]) bt = c;
-        for (int c = 5; c < kCand; ++c)
+        for (int c = kLane0 + 1; c < kCand; ++c)
             if (us_c[c] < us_c[bl]) bl = c;
         P.tma_tile = cand_tile[bt];
-        P.lane_lpn = cand_lpn[bl];
-        P.lane_pf = cand_pf[bl];
+        lane_shape(P, bl - kLane0);
         P.tune_us[0] = us_c[bt];
         P.tune_us[1] = us_c[3];
         P.tune_us[2] = us_c[bl];
@@ -711,10 +725,10 @@ int swe_cuda_sync(void) {
 
 int swe_cuda_select_kernel(int which) {
     SWE_TRY(require_ready());
-    if (which < 0 || which > 11) {
+    if (which < 0 || which > 17) {
         set_error("swe_cuda_select_kernel: 0 (pipelined), 1 (register), 2 / 3 / 4 (pipelined, 64 / 32 / 16-node tiles), "
-                  "5 (node-per-lane), 6 / 7 / 8 (node-per-lane, 1 / 2 / 4 lanes per node), 9 / 10 / 11 (the same "
-                  "with L2 prefetch), got %d", which);
+                  "5 (node-per-lane), 6-17 (node-per-lane shapes: 6 + lanes index (1/2/4 lanes per node) "
+                  "+ 3 x (5 CTAs per SM) + 6 x (L2 prefetch)), got %d", which);
         return SWE_ERR_ARG;
     }
     Plain& P = g_plain;
@@ -725,10 +739,7 @@ int swe_cuda_select_kernel(int which) {
     if (which == 2) P.tma_tile = 64;
     if (which == 3) P.tma_tile = 32;
     if (which == 4) P.tma_tile = 16;
-    if (which >= 6) {
-        P.lane_lpn = 1 << ((which - 6) % 3);
-        P.lane_pf = which >= 9 ? 1 : 0;
-    }
+    if (which >= 6) lane_shape(P, which - 6);
     if (P.graph) cudaGraphExecDestroy(P.graph);
     P.graph = nullptr;
     return P.build_graph();
@@ -744,6 +755,7 @@ int swe_cuda_kernel_info(int* out) {
     out[4] = g_plain.lane_lpn;
     out[5] = (int)(g_plain.tune_us[2] * 1000.f);   // node-per-lane
     out[6] = g_plain.lane_pf;
+    out[7] = g_plain.lane_minb;
     return SWE_OK;
 }
 

@@ -15,7 +15,9 @@
 // 16-byte-per-lane (FP32) row and one slot's indices a contiguous 128-byte row.
 // Weights and indices are streamed with L1 no-allocate loads; the neighbour
 // gathers keep L1 to themselves.  One warp per unit of 32 / LPN nodes, no
-// persistent loop: the hardware scheduler balances the tail.  Programmatic
+// persistent loop: the hardware scheduler balances the tail.  MINB (4 or 5) is
+// the register bound's CTAs per SM: 5 trades load depth for a grid that fits in
+// one wave on mid-sized patches.  Programmatic
 // dependent launch lets the next stage's CTAs take free SMs while the last
 // wave of this stage finishes; every read of a state array comes after
 // griddepcontrol.wait.
@@ -74,8 +76,8 @@ __device__ __forceinline__ void weights(const uint4* u, float (&w)[4]) {
 }
 }  // namespace lane
 
-template <typename T, int MODE, int LPN>
-__global__ void __launch_bounds__(kLaneThreads, 4) stage_lane_kernel(const LaneArgs<T> la) {
+template <typename T, int MODE, int LPN, int MINB>
+__global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const LaneArgs<T> la) {
     static_assert(LPN == 1 || LPN == 2 || LPN == 4, "1, 2 or 4 lanes per node");
     constexpr int kNpw = 32 / LPN;          // nodes per warp
     constexpr int kJpl = kSlots / LPN;      // slots per lane

@@ -212,15 +212,21 @@ class Plain:
 
     def select_kernel(self, which: int) -> None:
         """0: bulk-copy pipelined stage kernel, 1: register-streaming kernel, 2 / 3 / 4: pipelined with
-        64- / 32- / 16-node tiles, 5: node-per-lane kernel, 6 / 7 / 8: node-per-lane with 1 / 2 / 4 lanes
-        per node, 9 / 10 / 11: the same with the bulk L2 prefetch."""
+        64- / 32- / 16-node tiles, 5: node-per-lane kernel, 6 + s: node-per-lane shape s (lane_shape())."""
         check("swe_cuda_select_kernel", self.lib.swe_cuda_select_kernel(int(which)))
 
+    @staticmethod
+    def lane_shape(lanes_per_node: int, ctas_per_sm: int = 4, l2_prefetch: bool = False) -> int:
+        """select_kernel code of a node-per-lane shape."""
+        s = {1: 0, 2: 1, 4: 2}[lanes_per_node] + (3 if ctas_per_sm == 5 else 0) + (6 if l2_prefetch else 0)
+        return 6 + s
+
     def kernel_info(self) -> dict:
-        out = np.zeros(7, dtype=np.int32)
+        out = np.zeros(8, dtype=np.int32)
         check("swe_cuda_kernel_info", self.lib.swe_cuda_kernel_info(_p(out)))
         return {"in_use": ("pipelined", "register", "lane")[int(out[0])], "pipelined_available": bool(out[1]),
                 "pipelined_tile": int(out[1]), "lanes_per_node": int(out[4]), "l2_prefetch": bool(out[6]),
+                "ctas_per_sm": int(out[7]),
                 "tune_us": {"pipelined": out[2] / 1e3, "register": out[3] / 1e3, "lane": out[5] / 1e3}}
 
     def invariants(self) -> np.ndarray:

@@ -219,32 +219,37 @@ def test_lane_kernel_matches_oracle(plain, prec):
     plain.set_state(m.H_init.astype(dt))
     plain.step(7)
     H_reg = plain.get_state().reshape(-1, 4)
-    F_nopf = {}
-    for which, lpn, pf in ((6, 1, False), (7, 2, False), (8, 4, False), (9, 1, True), (10, 2, True), (11, 4, True)):
-        plain.select_kernel(which)
-        info = plain.kernel_info()
-        assert info["in_use"] == "lane" and info["lanes_per_node"] == lpn and info["l2_prefetch"] == pf
-        F = plain.eval_rhs(K)
-        if pf:                        # the prefetch moves no arithmetic
-            assert np.array_equal(F, F_nopf[lpn]), lpn
-        F_nopf[lpn] = F
-        if prec == "fp64":
-            assert rel_err(F, F64).max() <= 1e-12, lpn
-            assert cond_err(F, F64, m, K) <= 4e-16, lpn
-        else:
-            assert cond_err(F, F64, m, K) <= 4e-6, lpn
-        plain.set_state(m.H_init.astype(dt))
-        plain.step(7)
-        H = plain.get_state().reshape(-1, 4)
-        assert np.isfinite(H).all()
-        if prec == "fp64":
-            assert rel_err(H, H_reg).max() <= 1e-12, lpn
+    F_first = {}
+    for pf in (False, True):
+        for ctas in (4, 5):
+            for lpn in (1, 2, 4):
+                plain.select_kernel(capi.Plain.lane_shape(lpn, ctas, pf))
+                info = plain.kernel_info()
+                assert info["in_use"] == "lane" and info["lanes_per_node"] == lpn
+                assert info["l2_prefetch"] == pf and info["ctas_per_sm"] == ctas
+                F = plain.eval_rhs(K)
+                # neither the prefetch nor the register bound moves any arithmetic
+                if lpn in F_first:
+                    assert np.array_equal(F, F_first[lpn]), (lpn, ctas, pf)
+                    continue
+                F_first[lpn] = F
+                if prec == "fp64":
+                    assert rel_err(F, F64).max() <= 1e-12, lpn
+                    assert cond_err(F, F64, m, K) <= 4e-16, lpn
+                else:
+                    assert cond_err(F, F64, m, K) <= 4e-6, lpn
+                plain.set_state(m.H_init.astype(dt))
+                plain.step(7)
+                H = plain.get_state().reshape(-1, 4)
+                assert np.isfinite(H).all()
+                if prec == "fp64":
+                    assert rel_err(H, H_reg).max() <= 1e-12, lpn
 
 
 def test_select_kernel_rejects_unknown_choice(plain, grid_l4):
     _, d = grid_l4
     plain.init_model(swe_input.to_model(d), "fp64")
-    for bad in (-1, 12):
+    for bad in (-1, 18):
         with pytest.raises(capi.SweError):
             plain.select_kernel(bad)
 
@@ -260,7 +265,7 @@ def test_short_stencils_match_oracle(plain, prec):
     dt = np.float64 if prec == "fp64" else np.float32
     K = _perturbed(m.H_init).astype(dt)
     port = oracle.Port(m, prec)
-    for which in (1, 2, 3, 4, 6, 7, 8, 10):     # register, pipelined 64 / 32 / 16, node-per-lane 1 / 2 / 4 (+ prefetch)
+    for which in (1, 2, 3, 4, 6, 7, 8, 10, 16):  # register, pipelined 64 / 32 / 16, node-per-lane shapes
         plain.select_kernel(which)
         F = plain.eval_rhs(K)
         want = port.eval_rhs(K)
