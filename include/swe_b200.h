@@ -85,7 +85,9 @@ int swe_cuda_eval_rhs(const void* K, void* F);
 
 /* One RK4 stage on the device-resident state; same stage semantics as
  * RK_substep (rk4_rbffd_swe.c:30-72).  The RHS, the stage combine and the
- * D/K (or H) update are one fused kernel per stage.  Asynchronous. */
+ * D/K (or H) update are one fused kernel per stage.  Asynchronous.  As in the
+ * reference's time loop, a step calls substeps 0, 1, 2, 3 in order: substep k
+ * reads the stage state that substep k-1 wrote. */
 int swe_cuda_rk_substep(int substep_id);
 
 /* nsteps full RK4 steps (4 stages each) from a captured CUDA graph.

@@ -191,6 +191,7 @@ struct Plain {
     int* idxl = nullptr;            // node-per-lane kernel: tile-transposed weights / indices
     double* inv = nullptr;
     int* err = nullptr;             // pipelined kernel: bounded-wait error word
+    int* err_host = nullptr;        // pinned copy of it, read back with the state
     bool tma_ok = false;            // pipelined kernel set up
     int kernel_choice = 0;          // 0 = bulk-copy pipelined, 1 = register-streaming, 2 = node-per-lane kernel
     float tune_us[3] = {0.f, 0.f, 0.f};  // eval-mode launch time of each kernel at init (its best shape)
@@ -224,6 +225,8 @@ struct Plain {
         if (idxl) cudaFree(idxl);
         if (inv) cudaFree(inv);
         if (err) cudaFree(err);
+        if (err_host) cudaFreeHost(err_host);
+        err_host = nullptr;
         W = PT = H = Ka = Kb = D = F = Kx = raw = Wl = nullptr;
         idx = nullptr;
         idxl = nullptr;
@@ -452,6 +455,8 @@ static int upload_static(Plain& P, const void* x, const void* y, const void* z, 
     {
         SWE_CUDA_TRY(cudaMalloc(&P.err, sizeof(int)));
         SWE_CUDA_TRY(cudaMemset(P.err, 0, sizeof(int)));
+        SWE_CUDA_TRY(cudaHostAlloc(&P.err_host, sizeof(int), cudaHostAllocDefault));
+        *P.err_host = 0;
         SWE_TRY((set_tma_attrs<T, 64>()));
         SWE_TRY((set_tma_attrs<T, 32>()));
         SWE_TRY((set_tma_attrs<T, 16>()));
@@ -459,12 +464,18 @@ static int upload_static(Plain& P, const void* x, const void* y, const void* z, 
     return SWE_OK;
 }
 
+// Reads the pipelined kernel's bounded-wait error word: enqueues its copy into
+// pinned memory and synchronises the stream once (callers that also read data
+// back enqueue their copy first, so one synchronisation serves both).
 static int check_tma_err() {
     Plain& P = g_plain;
-    if (!P.err) return SWE_OK;
-    int h = 0;
-    SWE_CUDA_TRY(cudaMemcpyAsync(&h, P.err, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+    if (!P.err || !P.err_host) {
+        SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+        return SWE_OK;
+    }
+    SWE_CUDA_TRY(cudaMemcpyAsync(P.err_host, P.err, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
     SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    const int h = *P.err_host;
     if (h) {
         set_error("stage kernel: a bounded wait on the bulk-copy pipeline ran out (code %d)", h);
         return SWE_ERR_TIMEOUT;
@@ -641,10 +652,15 @@ int swe_cuda_set_state(const void* Hh) {
     if (!Hh) { set_error("null H"); return SWE_ERR_ARG; }
     Plain& P = g_plain;
     const size_t bytes = P.fbytes(4L * P.rows);
-    SWE_CUDA_TRY(cudaMemcpyAsync(P.raw, Hh, bytes, cudaMemcpyHostToDevice, P.stream));
-    SWE_TRY(permute_state(P.raw, P.H, 0));
-    SWE_CUDA_TRY(cudaMemcpyAsync(P.Ka, P.H, bytes, cudaMemcpyDeviceToDevice, P.stream));
-    SWE_CUDA_TRY(cudaMemcpyAsync(P.Kb, P.H, bytes, cudaMemcpyDeviceToDevice, P.stream));
+    if (P.cl.layout & SWE_LAYOUT_CFDL) {
+        // CFDL's SVM_LIN_ID is node-major [p][4], the device layout: no permutation
+        SWE_CUDA_TRY(cudaMemcpyAsync(P.H, Hh, bytes, cudaMemcpyHostToDevice, P.stream));
+    } else {
+        SWE_CUDA_TRY(cudaMemcpyAsync(P.raw, Hh, bytes, cudaMemcpyHostToDevice, P.stream));
+        SWE_TRY(permute_state(P.raw, P.H, 0));
+    }
+    // (the K ping-pong buffers need no copy: stage 0 gathers from H and writes K
+    // before any stage reads it)
     P.steps_done = 0;
     return SWE_OK;
 }
@@ -654,10 +670,13 @@ int swe_cuda_get_state(void* Hh) {
     if (!Hh) { set_error("null H"); return SWE_ERR_ARG; }
     Plain& P = g_plain;
     const size_t bytes = P.fbytes(4L * P.rows);
-    SWE_TRY(permute_state(P.H, P.raw, 1));
-    SWE_CUDA_TRY(cudaMemcpyAsync(Hh, P.raw, bytes, cudaMemcpyDeviceToHost, P.stream));
-    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
-    return check_tma_err();
+    if (P.cl.layout & SWE_LAYOUT_CFDL) {
+        SWE_CUDA_TRY(cudaMemcpyAsync(Hh, P.H, bytes, cudaMemcpyDeviceToHost, P.stream));
+    } else {
+        SWE_TRY(permute_state(P.H, P.raw, 1));
+        SWE_CUDA_TRY(cudaMemcpyAsync(Hh, P.raw, bytes, cudaMemcpyDeviceToHost, P.stream));
+    }
+    return check_tma_err();   // one synchronisation covers the state copy and the error word
 }
 
 int swe_cuda_eval_rhs(const void* K, void* Fh) {
@@ -719,8 +738,7 @@ int swe_cuda_step(int nsteps) {
 
 int swe_cuda_sync(void) {
     SWE_TRY(require_ready());
-    SWE_CUDA_TRY(cudaStreamSynchronize(g_plain.stream));
-    return check_tma_err();
+    return check_tma_err();   // synchronises the stream
 }
 
 int swe_cuda_select_kernel(int which) {
