@@ -65,4 +65,10 @@ enum PointField { PT_X = 0, PT_Y, PT_Z, PT_F, PT_GHM, PT_PU, PT_PV = PT_PU + 3, 
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
+// Bulk prefetch of a contiguous block into L2 (address and size 16-byte aligned);
+// it completes on its own and costs the issuing thread no registers.
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 }  // namespace swe

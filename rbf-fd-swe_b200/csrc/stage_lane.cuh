@@ -60,10 +60,6 @@ __device__ __forceinline__ float4 ld_stream(const float4* p) {
                  : "l"(p));
     return v;
 }
-// L2 prefetch of a contiguous block (16-byte aligned address and size); completes on its own
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
 // the four weights (Dx, Dy, Dz, L) of one slot of node t; units of a slot are 32 x 16 bytes apart
 __device__ __forceinline__ void weights(const uint4* u, double (&w)[4]) {
     const double2 a = ld_stream(reinterpret_cast<const double2*>(u));
@@ -98,19 +94,19 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
     if (pf && lane == 0 && nvalid > 0) {
         const long tb = node0 / kLaneTile;
         const int wt = (int)(node0 % kLaneTile) / kNpw;        // warp within its tile
-        lane::prefetch_l2(reinterpret_cast<const unsigned char*>(la.Wl) + tb * kTileW + wt * (kTileW / LPN), kTileW / LPN);
-        lane::prefetch_l2(reinterpret_cast<const unsigned char*>(la.idxl) + tb * kTileI + wt * (kTileI / LPN), kTileI / LPN);
-        lane::prefetch_l2(a.PT + node0 * kPointStride, (uint32_t)(nvalid * kPointStride * sizeof(T)));
+        prefetch_l2_bulk(reinterpret_cast<const unsigned char*>(la.Wl) + tb * kTileW + wt * (kTileW / LPN), kTileW / LPN);
+        prefetch_l2_bulk(reinterpret_cast<const unsigned char*>(la.idxl) + tb * kTileI + wt * (kTileI / LPN), kTileI / LPN);
+        prefetch_l2_bulk(a.PT + node0 * kPointStride, (uint32_t)(nvalid * kPointStride * sizeof(T)));
     }
     lane::pdl_wait();          // neighbour states and H / D come from the previous stage
     lane::pdl_trigger();
     if (nvalid <= 0) return;
     if (pf && lane == 0) {
         const uint32_t rows = (uint32_t)(nvalid * 4 * sizeof(T));
-        lane::prefetch_l2(a.Kin + 4 * (node0 + a.pid0), rows);
+        prefetch_l2_bulk(a.Kin + 4 * (node0 + a.pid0), rows);
         if (MODE != kStage0 && MODE != kEvalOnly) {
-            lane::prefetch_l2(a.H + 4 * node0, rows);
-            lane::prefetch_l2(a.D + 4 * node0, rows);
+            prefetch_l2_bulk(a.H + 4 * node0, rows);
+            prefetch_l2_bulk(a.D + 4 * node0, rows);
         }
     }
     // a warp's nodes lie in one tile of the packed arrays (kNpw divides 32); nodes
