@@ -173,10 +173,13 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 // Round an FP32 value to the nearest TF32 (10 explicit mantissa bits), ties
 // away from zero; the result is exactly representable, so the tensor core's
 // own FP32 -> TF32 conversion leaves it unchanged.
+// x rounded to TF32 (10 explicit mantissa bits), to nearest with ties away from zero,
+// for finite x: half a TF32 ulp is added to the magnitude bits and the 13 bits below
+// the TF32 mantissa are cleared (a carry out of the mantissa moves the exponent up,
+// which is the correctly rounded result).  Two full-rate integer operations, which
+// the operand converters issue for every element they split.
 __device__ __forceinline__ float tf32_rna(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
 }
 // 3xTF32 split with lo left in FP32: hi = tf32_rna(x) and lo = x - hi exactly (hi has
 // 11 significant bits, so x - hi is representable).  The tensor core reads lo at TF32
