@@ -11,9 +11,11 @@
 // copy stream, so nothing polls across PCIe), waits (bounded) until the request's previous stage
 // has completed everywhere, runs the plain form's fused FP64 stage math on the
 // chunk for every member, and publishes completion counters; the last item of
-// a request raises its completion flag in host memory.  The per-node math is
-// that of the plain stage kernel, with the same packed weight layout and lane
-// split, so a request's result does not depend on what it was mixed with.
+// a request raises its completion flag in host memory.  Each work item runs the
+// plain form's node-per-lane split (stage_lane.cuh): two lanes per node over a
+// tile-transposed copy of the grid's weights and indices; the per-node math never
+// depends on the other items, so a request's result does not depend on what it
+// was mixed with.
 //
 // Waits are bounded (%globaltimer): an idle kernel exits after a while (the
 // scheduler relaunches it when work arrives) and a dependency that is never
@@ -36,6 +38,7 @@
 
 #include "common.cuh"
 #include "stage_kernel.cuh"
+#include "stage_lane.cuh"
 
 namespace swe {
 namespace srv {
@@ -51,6 +54,8 @@ struct alignas(16) ReqDesc {   // device table entry of an admitted request
     const uint4* W;      // grid: packed weights
     const int4* idx;     // grid: packed stencil indices
     const double* PT;    // grid: pointwise records
+    const uint4* Wl;     // grid: tile-transposed weights (node-per-lane split)
+    const int* idxl;     // grid: tile-transposed stencil indices
     int n;               // nodes
     int members;
     int chunk_nodes;     // nodes per work item
@@ -93,93 +98,74 @@ __device__ __forceinline__ void load_row_cg(const double* p, double (&v)[4]) {
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
-// One warp, 4 nodes [base, base+4) of one member and one stage: the plain stage
-// kernel's math and data movement -- stencil indices prefetched one group ahead
-// (`nb` in: this group's, out: the next group's), the epilogue operands staged by
-// the node's 8 lanes into `ep` while the sums run -- with L2-coherent loads of
-// everything the kernel itself writes (states change between stages inside one
-// launch).
-constexpr int kSrvEp = kPointStride + 12;
-
-__device__ void serve_group(const ReqDesc& r, int stage, long base, long end, long next_base, int4& nb,
-                            double* __restrict__ Hm, double* __restrict__ Kam, double* __restrict__ Kbm,
-                            double* __restrict__ Dm, double (*red)[16], double (*ep)[kSrvEp], int k, int g) {
-    const long i = base + g;
-    const bool valid = i < end;
-    const long ii = valid ? i : end - 1;
+// One warp, 16 nodes [base, base + 16) of one member and one stage, two lanes per
+// node: the node-per-lane stage kernel's math and data movement (stage_lane.cuh),
+// with L2-coherent loads of everything the kernel itself writes (states change
+// between stages inside one launch).  Nodes at or past `end` belong to another
+// work item (or pad the last tile): they are computed on valid rows and not stored.
+constexpr int kSrvLpn = 2, kSrvNpw = 32 / kSrvLpn;
+__device__ void serve_lanes(const ReqDesc& r, int stage, long base, long end, double* __restrict__ Hm,
+                            double* __restrict__ Kam, double* __restrict__ Kbm, double* __restrict__ Dm, int lane) {
     const double* Kin = stage == 0 ? Hm : stage == 1 ? Kam : stage == 2 ? Kbm : Kam;
     double* Kout = stage == 0 ? Kam : stage == 1 ? Kbm : Kam;
-    const int nbr[4] = {nb.x, nb.y, nb.z, nb.w};
-    double kv[kSlotChunks][4], w[kSlotChunks][4];
-#pragma unroll
-    for (int m = 0; m < kSlotChunks; ++m) load_row_cg(Kin + 4L * nbr[m], kv[m]);
-#pragma unroll
-    for (int m = 0; m < kSlotChunks; ++m) Quad<double>::load(r.W, ((ii * kSlotChunks + m) * 2) * 8 + k, w[m]);
-    // epilogue operands: lanes 0-4 the pointwise record, 5-7 the own, H and D rows
-    {
-        double* e = ep[g];
-        double v[4];
-        if (k < 5) {
-            Quad<double>::load_row(r.PT + ii * kPointStride + 4 * k, v);
-#pragma unroll
-            for (int x = 0; x < 4; ++x) e[4 * k + x] = v[x];
-        } else {
-            load_row_cg((k == 5 ? Kin : k == 6 ? Hm : Dm) + 4 * ii, v);
-#pragma unroll
-            for (int x = 0; x < 4; ++x) e[kPointStride + 4 * (k - 5) + x] = v[x];
-        }
-    }
-    if (next_base < end) nb = __ldg(r.idx + min(next_base + g, end - 1) * 8 + k);
+    const int tl = lane % kSrvNpw, sub = lane / kSrvNpw;
+    const long i = base + tl;
+    const long tile = i / kLaneTile;
+    const int t = (int)(i % kLaneTile);
+    const int* ip = r.idxl + (tile * kSlots + sub) * kLaneTile + t;
+    const uint4* wp = r.Wl + (tile * kSlots + sub) * 2 * kLaneTile + t;
     double acc[16];
 #pragma unroll
-    for (int t = 0; t < 16; ++t) acc[t] = 0.0;
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
 #pragma unroll
-    for (int m = 0; m < kSlotChunks; ++m)
+    for (int jj = 0; jj < kSlots / kSrvLpn; ++jj) {
+        const int p = lane::ld_stream(ip + jj * kSrvLpn * kLaneTile);
+        double w[4], kv[4];
+        lane::weights(wp + jj * kSrvLpn * 2 * kLaneTile, w);
+        load_row_cg(Kin + 4L * p, kv);
 #pragma unroll
         for (int op = 0; op < 4; ++op)
 #pragma unroll
-            for (int f = 0; f < 4; ++f) acc[op * 4 + f] += w[m][op] * kv[m][f];
-    double r0, r1;
-    reduce_scatter8(acc, k, r0, r1);
-    red[g][2 * k] = r0;
-    red[g][2 * k + 1] = r1;
-    __syncwarp();
-    if (k == 0 && valid) {
-        const double* e = ep[g];
-        double s[16], q[4], F[4];
+            for (int f = 0; f < 4; ++f) acc[op * 4 + f] += w[op] * kv[f];
+    }
 #pragma unroll
-        for (int t = 0; t < 16; ++t) s[t] = red[g][t];
+    for (int o = kSrvNpw; o < 32; o <<= 1)
 #pragma unroll
-        for (int x = 0; x < 4; ++x) q[x] = e[kPointStride + x];
-        pointwise_rhs(s, q, e, r.gh0, F);
-        const double dt = r.dt;
-        if (stage == 0) {
+        for (int q = 0; q < 16; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    if (sub != 0 || i >= end) return;
+    double q[4], F[4];
+    load_row_cg(Kin + 4 * i, q);
+    pointwise_rhs(acc, q, r.PT + i * kPointStride, r.gh0, F);
+    const double dt = r.dt;
+    if (stage == 0) {
+        double kn[4];
+#pragma unroll
+        for (int x = 0; x < 4; ++x) kn[x] = Quad<double>::axpy(q[x], dt / 2.0, F[x]);
+        Quad<double>::store_row(Dm + 4 * i, F);
+        Quad<double>::store_row(Kout + 4 * i, kn);
+    } else {
+        double h[4], d[4];
+        load_row_cg(Hm + 4 * i, h);
+        load_row_cg(Dm + 4 * i, d);
+        if (stage < 3) {
+            const double c = stage == 1 ? dt / 2.0 : dt;
             double kn[4];
 #pragma unroll
-            for (int t = 0; t < 4; ++t) kn[t] = Quad<double>::axpy(q[t], dt / 2.0, F[t]);
-            Quad<double>::store_row(Dm + 4 * i, F);
-            Quad<double>::store_row(Kout + 4 * i, kn);
-        } else if (stage < 3) {
-            double d[4], kn[4];
-            const double c = stage == 1 ? dt / 2.0 : dt;
-#pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                d[t] = Quad<double>::axpy(e[kPointStride + 8 + t], 2.0, F[t]);
-                kn[t] = Quad<double>::axpy(e[kPointStride + 4 + t], c, F[t]);
+            for (int x = 0; x < 4; ++x) {
+                d[x] = Quad<double>::axpy(d[x], 2.0, F[x]);
+                kn[x] = Quad<double>::axpy(h[x], c, F[x]);
             }
             Quad<double>::store_row(Dm + 4 * i, d);
             Quad<double>::store_row(Kout + 4 * i, kn);
         } else {
-            double h[4];
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                const double d = Quad<double>::axpy(e[kPointStride + 8 + t], 1.0, F[t]);
-                h[t] = Quad<double>::update_h(e[kPointStride + 4 + t], dt / 6.0, d);
+            for (int x = 0; x < 4; ++x) {
+                d[x] = Quad<double>::axpy(d[x], 1.0, F[x]);
+                h[x] = Quad<double>::update_h(h[x], dt / 6.0, d[x]);
             }
             Quad<double>::store_row(Hm + 4 * i, h);
         }
     }
-    __syncwarp();
 }
 
 // Exit is collective: the first CTA that has found the queue empty for kIdleNs
@@ -194,13 +180,11 @@ __global__ void __launch_bounds__(kThreads, 2)
 serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, long long ring_cap,
              unsigned long long* head, const ReqDesc* __restrict__ reqs, int* done, int* flags, int* mdone,
              unsigned long long* items_done, int* exiting, int* kerr) {
-    __shared__ double red[kStageWarps][4][16];
-    __shared__ __align__(16) double ep[kStageWarps][4][kSrvEp];
     __shared__ long long s_pos;
     __shared__ Item s_item;
     __shared__ int s_ok;
     __shared__ ReqDesc s_req;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 3, k = lane & 7;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long idle_since = globaltimer();
     while (true) {
         if (threadIdx.x == 0) {
@@ -265,12 +249,9 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
             const long off = 4L * r.n * it.member;
             const long begin = (long)it.chunk * r.chunk_nodes;
             const long end = min((long)r.n, begin + r.chunk_nodes);
-            long base = begin + warp * 4L;
-            int4 nb = make_int4(0, 0, 0, 0);
-            if (base < end) nb = __ldg(r.idx + min(base + g, end - 1) * 8 + k);
-            for (; base < end; base += kStageWarps * 4L)
-                serve_group(r, stage, base, end, base + kStageWarps * 4L, nb, r.H + off, r.Ka + off, r.Kb + off,
-                            r.D + off, red[warp], ep[warp], k, g);
+            // chunks start on 32-node tiles, so a warp's 16 nodes lie in one tile
+            for (long base = begin + warp * (long)kSrvNpw; base < end; base += kStageWarps * (long)kSrvNpw)
+                serve_lanes(r, stage, base, end, r.H + off, r.Ka + off, r.Kb + off, r.D + off, lane);
         }
         __threadfence();
         __syncthreads();
@@ -301,6 +282,8 @@ struct Grid {
     void* W = nullptr;
     int* idx = nullptr;
     void* PT = nullptr;
+    void* Wl = nullptr;     // tile-transposed copies for the node-per-lane split
+    int* idxl = nullptr;
 };
 
 struct Request {
@@ -481,6 +464,8 @@ struct Server {
         d.W = reinterpret_cast<const uint4*>(G.W);
         d.idx = reinterpret_cast<const int4*>(G.idx);
         d.PT = reinterpret_cast<const double*>(G.PT);
+        d.Wl = reinterpret_cast<const uint4*>(G.Wl);
+        d.idxl = G.idxl;
         d.n = G.n;
         d.members = r.members;
         d.chunk_nodes = chunk_nodes(G.n);
@@ -735,18 +720,40 @@ int swe_srv_add_grid(int n, int nnbr, double gh0, double dt, const int* idx, con
             r[PT_PW + c] = p_w[i * 3 + c]; r[PT_GG + c] = gradghm[i * 3 + c];
         }
     }
+    // tile-transposed copies (as the plain form's node-per-lane kernel reads them):
+    // node i = 32 b + t, slot j, unit q at 16-byte unit ((b*32 + j)*2 + q)*32 + t;
+    // padded slots and nodes carry zero weights and gather a valid row
+    const long ntiles = (n + kLaneTile - 1) / kLaneTile;
+    std::vector<double> wlbuf((size_t)ntiles * kSlots * 2 * kLaneTile * 2, 0.0);
+    std::vector<int> ilbuf((size_t)ntiles * kSlots * kLaneTile, 0);
+    for (long i = 0; i < n; ++i) {
+        const long b = i / kLaneTile, t = i % kLaneTile;
+        for (int j = 0; j < kSlots; ++j) {
+            ilbuf[((size_t)b * kSlots + j) * kLaneTile + t] = ibuf[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)];
+            if (j >= nnbr) continue;
+            for (int op = 0; op < 4; ++op) {
+                const size_t unit = (((size_t)b * kSlots + j) * 2 + op / 2) * kLaneTile + t;
+                wlbuf[unit * 2 + op % 2] = ops[op][i * nnbr + j];
+            }
+        }
+    }
     Grid G;
     G.n = n; G.nnbr = nnbr; G.gh0 = gh0; G.dt = dt;
     cudaError_t e;
     if ((e = cudaMalloc(&G.W, wbuf.size() * 8)) != cudaSuccess ||
         (e = cudaMalloc(&G.idx, ibuf.size() * 4)) != cudaSuccess ||
-        (e = cudaMalloc(&G.PT, pbuf.size() * 8)) != cudaSuccess) {
+        (e = cudaMalloc(&G.PT, pbuf.size() * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&G.Wl, wlbuf.size() * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&G.idxl, ilbuf.size() * 4)) != cudaSuccess) {
         set_error("swe_srv_add_grid: %s", cudaGetErrorString(e));
+        for (void* p : {G.W, (void*)G.idx, G.PT, G.Wl, (void*)G.idxl}) if (p) cudaFree(p);
         return -SWE_ERR_NOMEM;
     }
     cudaMemcpy(G.W, wbuf.data(), wbuf.size() * 8, cudaMemcpyHostToDevice);
     cudaMemcpy(G.idx, ibuf.data(), ibuf.size() * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(G.PT, pbuf.data(), pbuf.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(G.Wl, wlbuf.data(), wlbuf.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(G.idxl, ilbuf.data(), ilbuf.size() * 4, cudaMemcpyHostToDevice);
     std::lock_guard<std::mutex> lock(g_srv->mu);
     g_srv->grids.push_back(G);
     return (int)g_srv->grids.size() - 1;
@@ -876,6 +883,8 @@ int swe_srv_stop(void) {
         cudaFree(G.W);
         cudaFree(G.idx);
         cudaFree(G.PT);
+        cudaFree(G.Wl);
+        cudaFree(G.idxl);
     }
     cudaFree(S->arena);
     cudaFree(S->head);
