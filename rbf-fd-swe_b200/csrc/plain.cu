@@ -18,6 +18,7 @@
 #include "history.cuh"
 #include "stage_tma.cuh"
 #include "stage_lane.cuh"
+#include "pack.cuh"
 
 namespace swe {
 
@@ -34,101 +35,6 @@ void set_error(const char* fmt, ...) {
 }
 
 void count_launch(long long n) { g_launches += n; }
-
-// ---------------------------------------------------------------------------
-// Packing of the static data (host) -----------------------------------------
-
-// Weights of node i, slot j = 8m + k, packed in 16-byte units at
-// unit ((i*4 + m)*U + q)*8 + k; unit q of FP64 holds (Dx, Dy) or (Dz, L),
-// the single FP32 unit holds (Dx, Dy, Dz, L).  Slots j >= nnbr are zero.
-template <typename T>
-static void pack_weights(const CallerLayout& cl, int n, int nnbr, const T* Dx, const T* Dy, const T* Dz,
-                         const T* L, std::vector<T>& out) {
-    constexpr int U = Quad<T>::kUnits;
-    constexpr int per_unit = 16 / sizeof(T);
-    out.assign((size_t)n * kSlotChunks * U * 8 * per_unit, T(0));
-    const T* ops[4] = {Dx, Dy, Dz, L};
-    for (long i = 0; i < n; ++i)
-        for (int j = 0; j < nnbr; ++j) {
-            const int m = j / 8, k = j % 8;
-            const long dm = cl.dm(i, j);
-            for (int op = 0; op < 4; ++op) {
-                const int q = op / per_unit, e = op % per_unit;
-                const size_t unit = (((size_t)i * kSlotChunks + m) * U + q) * 8 + k;
-                out[unit * per_unit + e] = ops[op][dm];
-            }
-        }
-}
-
-// idx of node i for lane k: int4 (slots k, k+8, k+16, k+24); padded slots
-// point at the node's own row (their weights are zero).
-static int pack_idx(const CallerLayout& cl, int n, int rows, int pid0, int nnbr, const int* idx,
-                    std::vector<int>& out) {
-    out.assign((size_t)n * kSlots, 0);
-    for (long i = 0; i < n; ++i)
-        for (int j = 0; j < kSlots; ++j) {
-            int p = (int)i + pid0;
-            if (j < nnbr) {
-                p = idx[cl.dm(i, j)];
-                if (p < 0 || p >= rows) {
-                    set_error("idx[node %ld][nbr %d] = %d outside the patch [0, %d)", i, j, p, rows);
-                    return SWE_ERR_INDEX;
-                }
-            }
-            out[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)] = p;
-        }
-    return SWE_OK;
-}
-
-// Tile-transposed copies for the node-per-lane kernel (stage_lane.cuh): node i
-// = 32 b + t, slot j and 16-byte unit q go to unit ((b*32 + j)*U + q)*32 + t;
-// nodes past n in the last tile keep zero weights.
-template <typename T>
-static void pack_lane_weights(const CallerLayout& cl, int n, int nnbr, const T* Dx, const T* Dy, const T* Dz,
-                              const T* L, std::vector<T>& out) {
-    constexpr int U = Quad<T>::kUnits;
-    constexpr int per_unit = 16 / sizeof(T);
-    const long ntiles = (n + kLaneTile - 1) / kLaneTile;
-    out.assign((size_t)ntiles * kSlots * U * kLaneTile * per_unit, T(0));
-    const T* ops[4] = {Dx, Dy, Dz, L};
-    for (long i = 0; i < n; ++i) {
-        const long b = i / kLaneTile, t = i % kLaneTile;
-        for (int j = 0; j < nnbr; ++j) {
-            const long dm = cl.dm(i, j);
-            for (int op = 0; op < 4; ++op) {
-                const int q = op / per_unit, e = op % per_unit;
-                const size_t unit = (((size_t)b * kSlots + j) * U + q) * kLaneTile + t;
-                out[unit * per_unit + e] = ops[op][dm];
-            }
-        }
-    }
-}
-
-// The same gather rows as pack_idx's (already checked), as [tile][slot][32 nodes];
-// nodes past n in the last tile gather row pid0.
-static void pack_lane_idx(const std::vector<int>& packed, int n, int pid0, std::vector<int>& out) {
-    const long ntiles = (n + kLaneTile - 1) / kLaneTile;
-    out.assign((size_t)ntiles * kSlots * kLaneTile, pid0);
-    for (long i = 0; i < n; ++i) {
-        const long b = i / kLaneTile, t = i % kLaneTile;
-        for (int j = 0; j < kSlots; ++j)
-            out[((size_t)b * kSlots + j) * kLaneTile + t] = packed[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)];
-    }
-}
-
-template <typename T>
-static void pack_points(const CallerLayout& cl, int n, const T* x, const T* y, const T* z, const T* f,
-                        const T* ghm, const T* pu, const T* pv, const T* pw, const T* gg, std::vector<T>& out) {
-    out.assign((size_t)n * kPointStride, T(0));
-    for (long i = 0; i < n; ++i) {
-        T* r = &out[(size_t)i * kPointStride];
-        r[PT_X] = x[i]; r[PT_Y] = y[i]; r[PT_Z] = z[i]; r[PT_F] = f[i]; r[PT_GHM] = ghm[i];
-        for (int c = 0; c < 3; ++c) {
-            const long v = cl.vect(i, c);
-            r[PT_PU + c] = pu[v]; r[PT_PV + c] = pv[v]; r[PT_PW + c] = pw[v]; r[PT_GG + c] = gg[v];
-        }
-    }
-}
 
 // ---------------------------------------------------------------------------
 // Device helpers ---------------------------------------------------------------
@@ -429,28 +335,16 @@ template <typename T>
 static int upload_static(Plain& P, const void* x, const void* y, const void* z, const void* f, const void* ghm,
                          const void* pu, const void* pv, const void* pw, const void* gg, const int* idx,
                          const void* Dx, const void* Dy, const void* Dz, const void* L) {
-    std::vector<T> wbuf, pbuf;
-    std::vector<int> ibuf;
-    pack_weights<T>(P.cl, P.n, P.nnbr, (const T*)Dx, (const T*)Dy, (const T*)Dz, (const T*)L, wbuf);
-    SWE_TRY(pack_idx(P.cl, P.n, P.rows, P.pid0, P.nnbr, idx, ibuf));
-    {
-        std::vector<T> wl;
-        std::vector<int> il;
-        pack_lane_weights<T>(P.cl, P.n, P.nnbr, (const T*)Dx, (const T*)Dy, (const T*)Dz, (const T*)L, wl);
-        pack_lane_idx(ibuf, P.n, P.pid0, il);
-        SWE_CUDA_TRY(cudaMalloc(&P.Wl, wl.size() * sizeof(T)));
-        SWE_CUDA_TRY(cudaMalloc(&P.idxl, il.size() * sizeof(int)));
-        SWE_CUDA_TRY(cudaMemcpy(P.Wl, wl.data(), wl.size() * sizeof(T), cudaMemcpyHostToDevice));
-        SWE_CUDA_TRY(cudaMemcpy(P.idxl, il.data(), il.size() * sizeof(int), cudaMemcpyHostToDevice));
-    }
-    pack_points<T>(P.cl, P.n, (const T*)x, (const T*)y, (const T*)z, (const T*)f, (const T*)ghm, (const T*)pu,
-                   (const T*)pv, (const T*)pw, (const T*)gg, pbuf);
-    SWE_CUDA_TRY(cudaMalloc(&P.W, wbuf.size() * sizeof(T)));
-    SWE_CUDA_TRY(cudaMalloc(&P.idx, ibuf.size() * sizeof(int)));
-    SWE_CUDA_TRY(cudaMalloc(&P.PT, pbuf.size() * sizeof(T)));
-    SWE_CUDA_TRY(cudaMemcpy(P.W, wbuf.data(), wbuf.size() * sizeof(T), cudaMemcpyHostToDevice));
-    SWE_CUDA_TRY(cudaMemcpy(P.idx, ibuf.data(), ibuf.size() * sizeof(int), cudaMemcpyHostToDevice));
-    SWE_CUDA_TRY(cudaMemcpy(P.PT, pbuf.data(), pbuf.size() * sizeof(T), cudaMemcpyHostToDevice));
+    // the caller's arrays go to the device once; every device layout is packed there (pack.cuh)
+    PackedStatic<T> ps;
+    SWE_TRY(pack_static_device<T>(P.cl, P.n, P.rows, P.pid0, P.nnbr, (const T*)Dx, (const T*)Dy, (const T*)Dz,
+                                  (const T*)L, idx, (const T*)x, (const T*)y, (const T*)z, (const T*)f,
+                                  (const T*)ghm, (const T*)pu, (const T*)pv, (const T*)pw, (const T*)gg, ps));
+    P.W = ps.W;
+    P.idx = ps.idx;
+    P.Wl = ps.Wl;
+    P.idxl = ps.idxl;
+    P.PT = ps.PT;
     P.tma_ok = true;
     {
         SWE_CUDA_TRY(cudaMalloc(&P.err, sizeof(int)));

@@ -39,6 +39,7 @@
 #include "common.cuh"
 #include "stage_kernel.cuh"
 #include "stage_lane.cuh"
+#include "pack.cuh"
 
 namespace swe {
 namespace srv {
@@ -696,64 +697,23 @@ int swe_srv_add_grid(int n, int nnbr, double gh0, double dt, const int* idx, con
                      const double* gradghm) {
     if (!g_srv) { set_error("swe_srv_add_grid: server not started"); return -SWE_ERR_STATE; }
     if (n <= 0 || nnbr <= 0 || nnbr > kSlots) { set_error("swe_srv_add_grid: bad sizes"); return -SWE_ERR_ARG; }
-    // pack exactly as the plain form packs a CFDL patch (node order as given)
-    std::vector<double> wbuf((size_t)n * kSlotChunks * 2 * 8 * 2, 0.0), pbuf((size_t)n * kPointStride, 0.0);
-    std::vector<int> ibuf((size_t)n * kSlots, 0);
-    const double* ops[4] = {Dx, Dy, Dz, L};
-    for (long i = 0; i < n; ++i) {
-        for (int j = 0; j < kSlots; ++j) {
-            int p = (int)i;
-            if (j < nnbr) {
-                p = idx[i * nnbr + j];
-                if (p < 0 || p >= n) { set_error("swe_srv_add_grid: idx out of range"); return -SWE_ERR_INDEX; }
-                for (int op = 0; op < 4; ++op) {
-                    const size_t unit = (((size_t)i * kSlotChunks + j / 8) * 2 + op / 2) * 8 + j % 8;
-                    wbuf[unit * 2 + op % 2] = ops[op][i * nnbr + j];
-                }
-            }
-            ibuf[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)] = p;
-        }
-        double* r = &pbuf[(size_t)i * kPointStride];
-        r[PT_X] = x[i]; r[PT_Y] = y[i]; r[PT_Z] = z[i]; r[PT_F] = f[i]; r[PT_GHM] = ghm[i];
-        for (int c = 0; c < 3; ++c) {
-            r[PT_PU + c] = p_u[i * 3 + c]; r[PT_PV + c] = p_v[i * 3 + c];
-            r[PT_PW + c] = p_w[i * 3 + c]; r[PT_GG + c] = gradghm[i * 3 + c];
-        }
-    }
-    // tile-transposed copies (as the plain form's node-per-lane kernel reads them):
-    // node i = 32 b + t, slot j, unit q at 16-byte unit ((b*32 + j)*2 + q)*32 + t;
-    // padded slots and nodes carry zero weights and gather a valid row
-    const long ntiles = (n + kLaneTile - 1) / kLaneTile;
-    std::vector<double> wlbuf((size_t)ntiles * kSlots * 2 * kLaneTile * 2, 0.0);
-    std::vector<int> ilbuf((size_t)ntiles * kSlots * kLaneTile, 0);
-    for (long i = 0; i < n; ++i) {
-        const long b = i / kLaneTile, t = i % kLaneTile;
-        for (int j = 0; j < kSlots; ++j) {
-            ilbuf[((size_t)b * kSlots + j) * kLaneTile + t] = ibuf[((size_t)i * 8 + (j % 8)) * 4 + (j / 8)];
-            if (j >= nnbr) continue;
-            for (int op = 0; op < 4; ++op) {
-                const size_t unit = (((size_t)b * kSlots + j) * 2 + op / 2) * kLaneTile + t;
-                wlbuf[unit * 2 + op % 2] = ops[op][i * nnbr + j];
-            }
-        }
-    }
+    // packed on the device exactly as the plain form packs a patch in the default
+    // layout (node order as given, rows of nnbr stencil slots)
+    CallerLayout cl;
+    cl.layout = 0;
+    cl.S = 1;
+    cl.pnbr = nnbr;
+    PackedStatic<double> ps;
+    const int st = pack_static_device<double>(cl, n, n, 0, nnbr, Dx, Dy, Dz, L, idx, x, y, z, f, ghm, p_u, p_v, p_w,
+                                              gradghm, ps);
+    if (st != SWE_OK) return -st;
     Grid G;
     G.n = n; G.nnbr = nnbr; G.gh0 = gh0; G.dt = dt;
-    cudaError_t e;
-    if ((e = cudaMalloc(&G.W, wbuf.size() * 8)) != cudaSuccess ||
-        (e = cudaMalloc(&G.idx, ibuf.size() * 4)) != cudaSuccess ||
-        (e = cudaMalloc(&G.PT, pbuf.size() * 8)) != cudaSuccess ||
-        (e = cudaMalloc(&G.Wl, wlbuf.size() * 8)) != cudaSuccess ||
-        (e = cudaMalloc(&G.idxl, ilbuf.size() * 4)) != cudaSuccess) {
-        set_error("swe_srv_add_grid: %s", cudaGetErrorString(e));
-        for (void* p : {G.W, (void*)G.idx, G.PT, G.Wl, (void*)G.idxl}) if (p) cudaFree(p);
-        return -SWE_ERR_NOMEM;
-    }
-    cudaMemcpy(G.W, wbuf.data(), wbuf.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(G.idx, ibuf.data(), ibuf.size() * 4, cudaMemcpyHostToDevice);
-    cudaMemcpy(G.PT, pbuf.data(), pbuf.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(G.Wl, wlbuf.data(), wlbuf.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(G.idxl, ilbuf.data(), ilbuf.size() * 4, cudaMemcpyHostToDevice);
+    G.W = ps.W;
+    G.idx = ps.idx;
+    G.PT = ps.PT;
+    G.Wl = ps.Wl;
+    G.idxl = ps.idxl;
     std::lock_guard<std::mutex> lock(g_srv->mu);
     g_srv->grids.push_back(G);
     return (int)g_srv->grids.size() - 1;

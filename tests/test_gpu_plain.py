@@ -246,6 +246,24 @@ def test_lane_kernel_matches_oracle(plain, prec):
                     assert rel_err(H, H_reg).max() <= 1e-12, lpn
 
 
+def test_init_rejects_out_of_range_index(plain, grid_l4):
+    """The static data is packed on the device; a stencil index outside the patch
+    is reported with its (node, slot), first in row-major order, and the library
+    stays usable."""
+    import dataclasses
+
+    _, d = grid_l4
+    m = swe_input.to_model(d)
+    idx = m.idx.copy()
+    idx[7, 3] = m.N + 5
+    idx[9, 0] = -1
+    with pytest.raises(capi.SweError, match=r"idx\[node 7\]\[nbr 3\] = %d outside the patch" % (m.N + 5)):
+        plain.init_model(dataclasses.replace(m, idx=idx), "fp64")
+    plain.init_model(m, "fp64")
+    F = plain.eval_rhs(m.H_init)
+    assert rel_err(F, oracle.Port(m, "fp64").eval_rhs(m.H_init)).max() <= 1e-12
+
+
 def test_select_kernel_rejects_unknown_choice(plain, grid_l4):
     _, d = grid_l4
     plain.init_model(swe_input.to_model(d), "fp64")
