@@ -65,6 +65,12 @@ enum PointField { PT_X = 0, PT_Y, PT_Z, PT_F, PT_GHM, PT_PU, PT_PV = PT_PU + 3, 
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
+// Programmatic dependent launch.  The previous stage's writes are visible only
+// after pdl_wait(); a CTA lets the next stage launch (pdl_trigger) only after its
+// own wait, so at most two consecutive stages are ever resident together.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Bulk prefetch of a contiguous block into L2 (address and size 16-byte aligned);
 // it completes on its own and costs the issuing thread no registers.
 __device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {

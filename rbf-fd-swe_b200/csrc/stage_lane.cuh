@@ -40,8 +40,6 @@ struct LaneArgs {
 };
 
 namespace lane {
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 __device__ __forceinline__ int ld_stream(const int* p) {
     int v;
@@ -98,8 +96,8 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
         prefetch_l2_bulk(reinterpret_cast<const unsigned char*>(la.idxl) + tb * kTileI + wt * (kTileI / LPN), kTileI / LPN);
         prefetch_l2_bulk(a.PT + node0 * kPointStride, (uint32_t)(nvalid * kPointStride * sizeof(T)));
     }
-    lane::pdl_wait();          // neighbour states and H / D come from the previous stage
-    lane::pdl_trigger();
+    pdl_wait();                // neighbour states and H / D come from the previous stage
+    pdl_trigger();
     if (nvalid <= 0) return;
     if (pf && lane == 0) {
         const uint32_t rows = (uint32_t)(nvalid * 4 * sizeof(T));

@@ -26,11 +26,6 @@
 
 namespace swe {
 
-// Programmatic dependent launch.  The previous stage's writes are visible only
-// after pdl_wait(); a CTA lets the next stage launch (pdl_trigger) only after its
-// own wait, so at most two consecutive stages are ever resident together.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 template <int TILE>
 struct TmaShape {
