@@ -71,6 +71,24 @@ def test_drop_in_all_reference_layouts(plain, lay, rcm, grid_l4):
         assert rel_err(F, F_ref).max() <= 1e-12
 
 
+@pytest.mark.parametrize("lay", oracle.LAYOUTS)
+@pytest.mark.parametrize("rcm", [0, 1])
+def test_drop_in_all_reference_layouts_fp32(plain, lay, rcm, grid_l4):
+    """The same through the reference's FP32 builds: F within the FP32 bound of the
+    condition-normalised error (two FP32 summation orders of the same formula)."""
+    if not oracle.reference_available("fp32", lay):
+        pytest.skip("reference not built")
+    path, d = grid_l4
+    ref = oracle.Ref(path, "fp32", lay, use_rcm=rcm)
+    plain.init_psmd(ref.psmd_ptr(), 4, ref.layout_flags, ref.simd_length)
+    m = layout.reorder(swe_input.to_model(d), ref.mapping())
+    for K in (ref.H_init(), _perturbed(ref.H_init()).astype(np.float32)):
+        F = ref.state_to_canonical(plain.eval_rhs(K))[: m.N]
+        F_ref = ref.state_to_canonical(ref.eval_rhs(K))[: m.N]
+        Kc = ref.state_to_canonical(K)[: m.N]
+        assert cond_err(F, F_ref, m, Kc) <= 4e-6
+
+
 @pytest.mark.parametrize("lay", ["cfdl", "default"])
 def test_shipped_input_100_steps_verify(plain, shipped_input, lay):
     """The reference's own end-to-end check on its shipped input, through its PSMD."""
@@ -155,11 +173,18 @@ def test_padded_weight_columns_are_never_read(plain):
 
 
 def test_out_of_range_index_is_rejected(plain):
+    """The static data is packed on the device; the first out-of-range stencil index
+    in row-major order is reported with its (node, slot), and the library stays usable."""
     m = swe_input.load_model(os.path.join(GOLDEN, "icos162_seed7.bin"))
+    good = m.idx.copy()
     m.idx[7, 3] = m.N + 5
-    with pytest.raises(capi.SweError) as e:
+    m.idx[9, 0] = -1
+    with pytest.raises(capi.SweError, match=r"idx\[node 7\]\[nbr 3\] = %d outside the patch" % (m.N + 5)) as e:
         plain.init_model(m, "fp64")
     assert e.value.status == 5
+    m.idx[:] = good
+    plain.init_model(m, "fp64")
+    assert rel_err(plain.eval_rhs(m.H_init), oracle.Port(m, "fp64").eval_rhs(m.H_init)).max() <= 1e-12
 
 
 def test_invariants_match_oracle(plain, grid_l4):
@@ -244,24 +269,6 @@ def test_lane_kernel_matches_oracle(plain, prec):
                 assert np.isfinite(H).all()
                 if prec == "fp64":
                     assert rel_err(H, H_reg).max() <= 1e-12, lpn
-
-
-def test_init_rejects_out_of_range_index(plain, grid_l4):
-    """The static data is packed on the device; a stencil index outside the patch
-    is reported with its (node, slot), first in row-major order, and the library
-    stays usable."""
-    import dataclasses
-
-    _, d = grid_l4
-    m = swe_input.to_model(d)
-    idx = m.idx.copy()
-    idx[7, 3] = m.N + 5
-    idx[9, 0] = -1
-    with pytest.raises(capi.SweError, match=r"idx\[node 7\]\[nbr 3\] = %d outside the patch" % (m.N + 5)):
-        plain.init_model(dataclasses.replace(m, idx=idx), "fp64")
-    plain.init_model(m, "fp64")
-    F = plain.eval_rhs(m.H_init)
-    assert rel_err(F, oracle.Port(m, "fp64").eval_rhs(m.H_init)).max() <= 1e-12
 
 
 def test_select_kernel_rejects_unknown_choice(plain, grid_l4):
