@@ -76,3 +76,20 @@ def test_single_process_is_its_own_job(monkeypatch):
     bench.init_replicas("gloo")                        # no process group for one process
     assert bench.max_over_ranks(3.5) == 3.5
     assert bench.job_rate(10.0, 2.0) == 5.0
+
+
+def test_plain_kernel_names_match_selection_codes():
+    """bench.py --plain-kernel names map to the swe_cuda_select_kernel codes that the
+    wrapper's lane_shape() gives for the same node-per-lane shape."""
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "rbf-fd-swe_b200"))
+    import bench
+    from swe_b200 import capi
+
+    for lanes in (1, 2, 4):
+        for wide, ctas in (("", 4), ("w", 5)):
+            for pf in (False, True):
+                name = f"lane{lanes}{wide}{'pf' if pf else ''}"
+                assert bench.PLAIN_KERNELS[name] == capi.Plain.lane_shape(lanes, ctas, pf), name
+    codes = [v for v in bench.PLAIN_KERNELS.values() if v is not None]
+    assert len(codes) == len(set(codes)) and max(codes) == 17 and min(codes) == 1
