@@ -2,25 +2,25 @@
 //
 // Same stage semantics as stage_kernel.cuh (eval_RHS_swe plus the RK4 stage
 // combine, swe_code/main/rk4_rbffd_swe.c:30-186 and :285-353), with a work split
-// that needs no cross-lane reduction in its default shape: each of a node's
-// LPN lanes (1, 2 or 4) sums the slots j = sub, sub + LPN, ... of the node
-// serially -- with LPN = 1 that is the reference's own slot order -- and the
-// LPN partial sums meet in a butterfly of log2(LPN) shuffle steps.  Lane sub 0
-// of every node then runs the pointwise part and the stage combine, so up to
-// all 32 lanes of a warp are busy in the epilogue.
+// that needs little or no cross-lane reduction: each of a node's LPN lanes (1, 2
+// or 4) sums the slots j = sub, sub + LPN, ... of the node serially -- with
+// LPN = 1 that is the reference's own slot order -- and the LPN partial sums
+// meet in a butterfly of log2(LPN) shuffle steps.  Lane sub 0 of every node then
+// runs the pointwise part and the stage combine, so up to all 32 lanes of a warp
+// are busy in the epilogue.
 //
 // The stencil weights and indices live in a second, tile-transposed copy
-// (pack_lane_* in plain.cu): per 32-node tile, slot-major, node-minor, so one
-// slot's weights of a warp's nodes are one contiguous 512-byte (FP64: two) or
-// 16-byte-per-lane (FP32) row and one slot's indices a contiguous 128-byte row.
-// Weights and indices are streamed with L1 no-allocate loads; the neighbour
-// gathers keep L1 to themselves.  One warp per unit of 32 / LPN nodes, no
-// persistent loop: the hardware scheduler balances the tail.  MINB (4 or 5) is
-// the register bound's CTAs per SM: 5 trades load depth for a grid that fits in
-// one wave on mid-sized patches.  Programmatic
-// dependent launch lets the next stage's CTAs take free SMs while the last
-// wave of this stage finishes; every read of a state array comes after
-// griddepcontrol.wait.
+// (pack_stencils_kernel in pack.cuh): per 32-node tile, slot-major, node-minor,
+// so one slot's weights of a warp's nodes are one contiguous 512-byte (FP64:
+// two) or 16-byte-per-lane (FP32) row and one slot's indices a contiguous
+// 128-byte row.  Weights and indices are streamed with L1 no-allocate loads; the
+// neighbour gathers keep L1 to themselves.  One warp per unit of 32 / LPN nodes,
+// no persistent loop: the hardware scheduler balances the tail.  MINB (4 or 5)
+// is the register bound's CTAs per SM: 5 trades load depth for a grid that fits
+// in one wave on mid-sized patches.  Programmatic dependent launch lets the next
+// stage's CTAs take free SMs while the last wave of this stage finishes; every
+// read of a state array comes after griddepcontrol.wait.  swe_cuda_init times
+// the shapes (LPN x MINB x L2 prefetch) and keeps the fastest.
 #pragma once
 
 #include "stage_kernel.cuh"
