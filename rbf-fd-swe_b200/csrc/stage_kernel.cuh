@@ -37,7 +37,7 @@ struct StageArgs {
     int pid0;           // compute_pid_s: row of node 0 in the gather source
     const T* Kin;       // gather source [rows][4]
     const int4* idx;    // [n][8] int4: slots (k, k+8, k+16, k+24) of lane k
-    const uint4* W;     // packed weights, see pack_weights()
+    const uint4* W;     // packed weights, see pack_stencils_kernel (pack.cuh)
     const T* PT;        // [n][kPointStride] pointwise data
     T* H;               // [n][4] RK base state (stages) -- also the gather source of stage 0
     T* D;               // [n][4] RK accumulator
