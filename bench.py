@@ -53,6 +53,21 @@ WORKLOADS = {
     "serve_mix": (0, "serve", "serving: Poisson arrivals over N in {2562, 10242, 40962, 163842}, 1-32 members, "
                               "10-500 steps, 80 GB budget, FP64"),
 }
+# The reference's own recorded rate for a workload's metric and configuration, where one
+# exists: Eval_Rhs at N=40962 in the CFDL layout took 1.267690e-3 s per RK4 step (4
+# eval_RHS calls) with its OpenACC build on a V100 (run/psg/output/output_cfdl.txt:41;
+# precision not recorded) = 4 * 40962 / 1.267690e-3 node-stage updates/s.
+RECORDED_RATE = {"plain_fp64_n40962": (4 * 40962 / 1.267690e-3,
+                                       "reference run log run/psg/output/output_cfdl.txt:41 "
+                                       "(Eval_Rhs, N=40962, CFDL, OpenACC on V100)")}
+
+
+def vs_recorded(workload: str, value: float):
+    """(value / the reference's recorded rate, its source), or (None, None)."""
+    rec = RECORDED_RATE.get(workload)
+    return (value / rec[0], rec[1]) if rec else (None, None)
+
+
 ALG_BYTES = {"fp64": 1396, "fp32": 760}      # per node-stage (FP64: 4*31*8+31*4+17*8+4*8+14*8)
 # batched form, per node-stage: shared 4*31*4 (weights) + 31*4 (idx) + 17*4 (pointwise)
 # plus per member 4*4 (K read once) + 14*4 (RK combine) + 4 (FP64 h registers)
@@ -294,7 +309,8 @@ def run_reference(args, level, prec, wl):
         "value": base["value"], "unit": "node-stage updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * 4.0 * d.N / base["value"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32", "data": "synthetic",
+        "vs_baseline": vs_recorded(wl, base["value"])[0], "vs_baseline_source": vs_recorded(wl, base["value"])[1],
+        "dtype": "f64" if prec == "fp64" else "f32", "data": "synthetic",
         "config": {"workload": wl, "nodes": d.N, "nnbr": 31, "dt": d.dt, "layout": "CFDL", "rcm": True},
         "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": "node-stage updates/s", "h2d_bytes_per_step": 0,
@@ -652,7 +668,9 @@ def main():
             "metric": "node-stage updates/s (RK4 + RBF-FD stage, plain form)",
             "value": value, "unit": "node-stage updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32",
+            "scaling": "weak", "vs_baseline": vs_recorded(args.workload, value)[0],
+            "vs_baseline_source": vs_recorded(args.workload, value)[1],
+            "dtype": "f64" if prec == "fp64" else "f32",
             "data": "synthetic (seeded icosahedral grid, PHS RBF-FD weights, TC5 Gaussian-mountain ICs)",
             "config": {"workload": args.workload, "description": desc, "nodes": N, "nnbr": 31, "dt": d.dt,
                        "layout": "CFDL", "rcm": True, "parallelism": f"replicas x{world}",
