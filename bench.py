@@ -74,10 +74,11 @@ ALG_BYTES = {"fp64": 1396, "fp32": 760}      # per node-stage (FP64: 4*31*8+31*4
 ENS_SHARED_BYTES = 4 * 31 * 4 + 31 * 4 + 17 * 4
 ENS_MEMBER_BYTES = 4 * 4 + 14 * 4 + 4
 # --plain-kernel choices -> swe_cuda_select_kernel codes (laneN: N lanes per node at 4 CTAs per
-# SM; "w": 5 CTAs per SM; "pf": with the L2 prefetch)
+# SM; "w": 5 CTAs per SM; "d": 3 CTAs per SM; "pf": with the L2 prefetch)
 PLAIN_KERNELS = {"auto": None, "register": 1, "pipelined64": 2, "pipelined32": 3, "pipelined16": 4,
                  "lane1": 6, "lane2": 7, "lane4": 8, "lane1w": 9, "lane2w": 10, "lane4w": 11,
-                 "lane1pf": 12, "lane2pf": 13, "lane4pf": 14, "lane1wpf": 15, "lane2wpf": 16, "lane4wpf": 17}
+                 "lane1pf": 12, "lane2pf": 13, "lane4pf": 14, "lane1wpf": 15, "lane2wpf": 16, "lane4wpf": 17,
+                 "lane1d": 18, "lane2d": 19, "lane4d": 20, "lane1dpf": 21, "lane2dpf": 22, "lane4dpf": 23}
 L2_FLUSH_BYTES = 256 << 20
 L2_NOTE = "flushed between timed steps: 256 MB write, then 256 MB read (cold, clean L2 at each step)"
 # DRAM bytes (read + write) per launch of the dominant kernel, from ncu captures of the same

@@ -106,18 +106,19 @@ int swe_cuda_sync(void);
  * node, each summing its slots serially, from a tile-transposed copy of the
  * weights and indices).  Kernels 0 and 1 do the same arithmetic in the same
  * order; kernel 2 sums the slots in another order and meets the same error
- * bars; it runs at 4 or 5 CTAs per SM and can bulk-prefetch each warp's
+ * bars; it runs at 3, 4 or 5 CTAs per SM and can bulk-prefetch each warp's
  * contiguous blocks into L2 at its start).  swe_cuda_init times every kernel
  * and shape on the patch, keeps the fastest shape of each, and uses the fastest
  * kernel.  info[8] = {kernel in use (0/1/2), pipelined tile in nodes (0 if
  * unavailable), ns per eval launch of kernel 0 (its fastest tile), of kernel 1,
  * lanes per node of kernel 2, ns per eval launch of kernel 2 (its fastest
- * shape), kernel 2's L2 prefetch (0/1), kernel 2's CTAs per SM (4/5)}.
+ * shape), kernel 2's L2 prefetch (0/1), kernel 2's CTAs per SM (3/4/5)}.
  * swe_cuda_select_kernel takes which = 0 / 1 (kernels 0 / 1), 2 / 3 / 4 (the
  * pipelined kernel with 64- / 32- / 16-node tiles), 5 (kernel 2, its current
- * shape) and 6 + s for kernel 2's shape s in 0..11: 1 / 2 / 4 lanes per node
- * for s % 3 = 0 / 1 / 2, 5 CTAs per SM when (s / 3) is odd, the L2 prefetch
- * when s >= 6. */
+ * shape) and 6 + s for kernel 2's shape s in 0..17: 1 / 2 / 4 lanes per node
+ * for s % 3 = 0 / 1 / 2; for s < 12, 5 CTAs per SM when (s / 3) is odd (else
+ * 4) and the L2 prefetch when s >= 6; for s >= 12, 3 CTAs per SM and the L2
+ * prefetch when s >= 15. */
 int swe_cuda_select_kernel(int which);
 int swe_cuda_kernel_info(int* info);
 

@@ -103,7 +103,7 @@ struct Plain {
     float tune_us[3] = {0.f, 0.f, 0.f};  // eval-mode launch time of each kernel at init (its best shape)
     int lane_lpn = 1;               // node-per-lane kernel: lanes per node (1, 2, 4)
     int lane_pf = 0;                // node-per-lane kernel: bulk L2 prefetch at warp start
-    int lane_minb = 4;              // node-per-lane kernel: CTAs per SM of its register bound (4, 5)
+    int lane_minb = 4;              // node-per-lane kernel: CTAs per SM of its register bound (3, 4, 5)
     int tma_tile = 64;              // pipelined kernel: nodes per tile (64: 1 CTA/SM, 32: 2 CTAs/SM)
     int sms = 0;
     cudaStream_t stream = nullptr;
@@ -250,7 +250,11 @@ struct Plain {
     void launch_t(int mode) {
         const StageArgs<T> a = args<T>(mode);
         if (kernel_choice == 2) {
-            if (lane_minb == 5) {
+            if (lane_minb == 3) {
+                if (lane_lpn == 4) launch_lane<T, 4, 3>(a, mode);
+                else if (lane_lpn == 2) launch_lane<T, 2, 3>(a, mode);
+                else launch_lane<T, 1, 3>(a, mode);
+            } else if (lane_minb == 5) {
                 if (lane_lpn == 4) launch_lane<T, 4, 5>(a, mode);
                 else if (lane_lpn == 2) launch_lane<T, 2, 5>(a, mode);
                 else launch_lane<T, 1, 5>(a, mode);
@@ -311,13 +315,19 @@ struct Plain {
 
 static Plain g_plain;
 
-// Node-per-lane shape s in 0..11 (swe_cuda_select_kernel's 6 + s): lanes per node
-// 1 / 2 / 4 = s % 3, 5 CTAs per SM when (s / 3) % 2, L2 prefetch when s >= 6.
+// Node-per-lane shape s in 0..17 (swe_cuda_select_kernel's 6 + s): lanes per node
+// 1 / 2 / 4 = s % 3; s < 12: 5 CTAs per SM when (s / 3) % 2 (else 4), L2 prefetch
+// when s >= 6; s >= 12: 3 CTAs per SM, L2 prefetch when s >= 15.
 static void lane_shape(Plain& P, int s) {
     P.kernel_choice = 2;
     P.lane_lpn = 1 << (s % 3);
-    P.lane_minb = (s / 3) % 2 ? 5 : 4;
-    P.lane_pf = s >= 6 ? 1 : 0;
+    if (s < 12) {
+        P.lane_minb = (s / 3) % 2 ? 5 : 4;
+        P.lane_pf = s >= 6 ? 1 : 0;
+    } else {
+        P.lane_minb = 3;
+        P.lane_pf = s >= 15 ? 1 : 0;
+    }
 }
 
 template <typename T, int TILE>
@@ -497,9 +507,9 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
         SWE_CUDA_TRY(cudaEventCreate(&e0));
         SWE_CUDA_TRY(cudaEventCreate(&e1));
         SWE_CUDA_TRY(cudaMemsetAsync(P.Kx, 0, srow, P.stream));
-        // candidates 0-2: pipelined 64 / 32 / 16; 3: register; 4-15: node-per-lane
+        // candidates 0-2: pipelined 64 / 32 / 16; 3: register; 4-21: node-per-lane
         // shape 6 + (c - 4) in swe_cuda_select_kernel's numbering
-        constexpr int kLane0 = 4, kCand = kLane0 + 12;
+        constexpr int kLane0 = 4, kCand = kLane0 + 18;
         const int cand_tile[3] = {64, 32, 16};
         float us_c[kCand] = {};
         for (int c = 0; c < kCand; ++c) {
@@ -637,10 +647,11 @@ int swe_cuda_sync(void) {
 
 int swe_cuda_select_kernel(int which) {
     SWE_TRY(require_ready());
-    if (which < 0 || which > 17) {
+    if (which < 0 || which > 23) {
         set_error("swe_cuda_select_kernel: 0 (pipelined), 1 (register), 2 / 3 / 4 (pipelined, 64 / 32 / 16-node tiles), "
                   "5 (node-per-lane), 6-17 (node-per-lane shapes: 6 + lanes index (1/2/4 lanes per node) "
-                  "+ 3 x (5 CTAs per SM) + 6 x (L2 prefetch)), got %d", which);
+                  "+ 3 x (5 CTAs per SM) + 6 x (L2 prefetch)), 18-23 (the same at 3 CTAs per SM: 18 + lanes "
+                  "index + 3 x (L2 prefetch)), got %d", which);
         return SWE_ERR_ARG;
     }
     Plain& P = g_plain;

@@ -217,8 +217,11 @@ class Plain:
 
     @staticmethod
     def lane_shape(lanes_per_node: int, ctas_per_sm: int = 4, l2_prefetch: bool = False) -> int:
-        """select_kernel code of a node-per-lane shape."""
-        s = {1: 0, 2: 1, 4: 2}[lanes_per_node] + (3 if ctas_per_sm == 5 else 0) + (6 if l2_prefetch else 0)
+        """select_kernel code of a node-per-lane shape (3, 4 or 5 CTAs per SM)."""
+        li = {1: 0, 2: 1, 4: 2}[lanes_per_node]
+        if ctas_per_sm == 3:
+            return 18 + li + (3 if l2_prefetch else 0)
+        s = li + (3 if ctas_per_sm == 5 else 0) + (6 if l2_prefetch else 0)
         return 6 + s
 
     def kernel_info(self) -> dict:

@@ -87,9 +87,9 @@ def test_plain_kernel_names_match_selection_codes():
     from swe_b200 import capi
 
     for lanes in (1, 2, 4):
-        for wide, ctas in (("", 4), ("w", 5)):
+        for wide, ctas in (("", 4), ("w", 5), ("d", 3)):
             for pf in (False, True):
                 name = f"lane{lanes}{wide}{'pf' if pf else ''}"
                 assert bench.PLAIN_KERNELS[name] == capi.Plain.lane_shape(lanes, ctas, pf), name
     codes = [v for v in bench.PLAIN_KERNELS.values() if v is not None]
-    assert len(codes) == len(set(codes)) and max(codes) == 17 and min(codes) == 1
+    assert len(codes) == len(set(codes)) and max(codes) == 23 and min(codes) == 1

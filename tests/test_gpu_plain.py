@@ -246,7 +246,7 @@ def test_lane_kernel_matches_oracle(plain, prec):
     H_reg = plain.get_state().reshape(-1, 4)
     F_first = {}
     for pf in (False, True):
-        for ctas in (4, 5):
+        for ctas in (4, 5, 3):
             for lpn in (1, 2, 4):
                 plain.select_kernel(capi.Plain.lane_shape(lpn, ctas, pf))
                 info = plain.kernel_info()
@@ -274,7 +274,7 @@ def test_lane_kernel_matches_oracle(plain, prec):
 def test_select_kernel_rejects_unknown_choice(plain, grid_l4):
     _, d = grid_l4
     plain.init_model(swe_input.to_model(d), "fp64")
-    for bad in (-1, 18):
+    for bad in (-1, 24):
         with pytest.raises(capi.SweError):
             plain.select_kernel(bad)
 
