@@ -397,14 +397,18 @@ def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
     for _ in range(3):
         plain.step(1)
     plain.sync()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # timed as the ensemble steps are: one step per pair of events, L2 flushed between
     pstream = torch.cuda.ExternalStream(plain.stream())
+    p_starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    p_stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with torch.cuda.stream(pstream):
-        e0.record(pstream)
-        plain.step(args.steps)
-        e1.record(pstream)
+        for s in range(args.steps):
+            flush()
+            p_starts[s].record(pstream)
+            plain.step(1)
+            p_stops[s].record(pstream)
     torch.cuda.synchronize()
-    plain_steps = args.steps / (e0.elapsed_time(e1) * 1e-3)
+    plain_steps = args.steps / sum(a.elapsed_time(b) * 1e-3 for a, b in zip(p_starts, p_stops))
 
     # h error after err_steps steps against the plain FP64 GPU run of the same members
     # (natural node order, as the ensemble exchanges states)
