@@ -19,7 +19,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import GOLDEN, cond_err, generated_input, rel_err
+from conftest import GOLDEN, abs_rhs, cond_err, generated_input, rel_err
 from swe_b200 import capi, layout, swe_input
 
 pytestmark = pytest.mark.gpu
@@ -148,6 +148,35 @@ def test_fp32_form(plain, grid_l4):
     plain.step(100)
     H = plain.get_state().reshape(-1, 4)
     assert np.abs(H - m.H_100).max() <= 4e-2          # the reference's FP32 TOLERANCE
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_patch_with_halo_rows(plain, grid_l4, prec):
+    """A patch as the reference's MPI decomposition builds one (init_patches.c): the
+    compute rows start at compute_pid_s inside a longer gather patch, and stencil
+    indices refer to patch rows, some of them halo rows.  eval_rhs of the compute
+    rows matches the oracle's rows of the whole grid, for every kernel and shape."""
+    _, d = grid_l4
+    m = swe_input.to_model(d)
+    pid0, nc = 100, 1000                              # compute rows [100, 1100) of 2562
+    dt = np.float64 if prec == "fp64" else np.float32
+    rows = slice(pid0, pid0 + nc)
+    arrays = {k: np.ascontiguousarray(getattr(m, k)[rows], dtype=dt)
+              for k in ("x", "y", "z", "f", "ghm", "p_u", "p_v", "p_w", "gradghm", "Dx", "Dy", "Dz", "L")}
+    arrays["idx"] = np.ascontiguousarray(m.idx[rows], dtype=np.int32)
+    assert (arrays["idx"] < pid0).any() and (arrays["idx"] >= pid0 + nc).any()   # halo rows on both sides
+    plain.init(np.dtype(dt).itemsize, capi.SWE_LAYOUT_CFDL, 1, nc, m.N, pid0, m.Nnbr, m.Nnbr, m.gh0, m.dt, arrays)
+    K = _perturbed(m.H_init).astype(dt)
+    want64 = oracle.Port(m, "fp64").eval_rhs(K.astype(np.float64)).reshape(-1, 4)[rows]
+    for which in (1, 3, 4, 6, 7, 8, 15, 18, 19):
+        plain.select_kernel(which)
+        F = plain.eval_rhs(K).reshape(-1, 4)
+        assert F.shape == (nc, 4)
+        if prec == "fp64":
+            assert rel_err(F, want64).max() <= 1e-12, which
+        else:
+            scale = abs_rhs(m, K)[rows].max(0)             # term scale of these rows
+            assert (np.abs(F - want64).max(0) / scale).max() <= 4e-6, which
 
 
 def test_padded_weight_columns_are_never_read(plain):
