@@ -40,3 +40,34 @@ def test_init_argument_checks_fail_before_device_work():
     assert lib.swe_cuda_init(8, 1, 1, 4, 2, 0, 1, 1, 0.0, 1.0, *ptrs) == 1
     # null array
     assert lib.swe_cuda_init(8, 1, 1, 2, 2, 0, 1, 1, 0.0, 1.0, *([None] + ptrs[1:])) == 1
+
+
+def test_header_compiles_as_c_and_links(tmp_path):
+    """The reference's host is C99: include/swe_b200.h must compile as C with warnings
+    as errors, and a C program must link against the library and call it (a call that
+    fails before any device work, so no GPU is needed)."""
+    import os
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.dirname(capi.LIB_PATH)
+    src = tmp_path / "use_swe.c"
+    src.write_text(
+        '#include <stdio.h>\n'
+        '#include "swe_b200.h"\n'
+        'int main(void) {\n'
+        '    int st = swe_cuda_step(1);          /* before swe_cuda_init: a state error */\n'
+        '    const char* msg = swe_cuda_last_error();\n'
+        '    printf("%d %s\\n", st, msg);\n'
+        '    return (st == SWE_ERR_STATE && swe_b200_kernel_launches() >= 0) ? 0 : 1;\n'
+        '}\n')
+    exe = tmp_path / "use_swe"
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(root, "include"),
+                    str(src), "-L", libdir, "-lswe_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.startswith("2 ") and "swe_cuda_init" in out.stdout
