@@ -36,6 +36,9 @@ def build(with_reference: bool | None = None) -> None:
     if with_reference is None:
         with_reference = os.path.isdir(os.path.join(ref_root, "swe_code"))
     targets = ["port"] + (["ref"] if with_reference else [])
+    lib = os.path.join(os.path.dirname(HERE), "rbf-fd-swe_b200", "lib", "libswe_b200.so")
+    if with_reference and os.path.exists(lib):
+        targets.append("host")          # the reference's main program driving the library
     subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={ref_root}", "-j8", *targets], check=True)
 
 
