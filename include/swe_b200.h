@@ -134,7 +134,11 @@ int swe_cuda_last_timings(double* out);
 void* swe_cuda_stream(void);
 
 /* FP64 (mass, energy) of the device state with equal node areas 4*pi/n:
- * mass = sum A (h + gh0 - ghm), energy = sum A (0.5 (h+gh0-ghm)|u|^2 + 0.5 (h+gh0)^2). */
+ * mass = sum A (h + gh0 - ghm), energy = sum A (0.5 (h+gh0-ghm)|u|^2 + 0.5 (h+gh0)^2).
+ * Also the NaN/Inf watchdog (the reference's only such check is the NaN test in
+ * verify_output, main.c:451): the sums are written either way, and the call
+ * returns SWE_ERR_NONFINITE when either is NaN or Inf, i.e. when any value of
+ * the state is. */
 int swe_cuda_invariants(double* mass_energy);
 
 /* Frees all device memory and the stream. */
@@ -231,7 +235,9 @@ int swe_ens_use_variant(int tile_nodes, int members_per_cta);
  * exact TF32, |x - hi - lo| <= 2^-22 |x|), 1 = split BF16 (2^-17), both with
  * FP32 accumulation and the same FP64 h accumulation. */
 int swe_ens_set_precision(int precision);
-/* FP64 (mass, energy) per member, [members][2], definitions as swe_cuda_invariants. */
+/* FP64 (mass, energy) per member, [members][2], definitions as swe_cuda_invariants;
+ * SWE_ERR_NONFINITE (message naming the first such member) when a member's sums
+ * are NaN or Inf. */
 int swe_ens_invariants(double* mass_energy);
 int swe_ens_sync(void);
 int swe_ens_set_timing(int enabled);

@@ -608,6 +608,12 @@ int swe_ens_invariants(double* out) {
     SWE_CUDA_TRY(cudaStreamSynchronize(E.stream));
     const double area = 4.0 * 3.14159265358979323846 / (double)E.n;
     for (int t = 0; t < 2 * E.members; ++t) out[t] *= area;
+    // NaN/Inf watchdog per member: one non-finite value in a member's state makes its sums non-finite
+    for (int b = 0; b < E.members; ++b)
+        if (!std::isfinite(out[2 * b]) || !std::isfinite(out[2 * b + 1])) {
+            set_error("swe_ens_invariants: member %d's state holds NaN or Inf", b);
+            return SWE_ERR_NONFINITE;
+        }
     return SWE_OK;
 }
 

@@ -734,6 +734,11 @@ int swe_cuda_invariants(double* me) {
     const double area = 4.0 * 3.14159265358979323846 / (double)P.n;
     me[0] *= area;
     me[1] *= area;
+    // NaN/Inf watchdog: one non-finite value anywhere in H makes a sum non-finite
+    if (!std::isfinite(me[0]) || !std::isfinite(me[1])) {
+        set_error("swe_cuda_invariants: the state holds NaN or Inf (mass %g, energy %g)", me[0], me[1]);
+        return SWE_ERR_NONFINITE;
+    }
     return SWE_OK;
 }
 

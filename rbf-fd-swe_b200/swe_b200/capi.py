@@ -233,6 +233,7 @@ class Plain:
                 "tune_us": {"pipelined": out[2] / 1e3, "register": out[3] / 1e3, "lane": out[5] / 1e3}}
 
     def invariants(self) -> np.ndarray:
+        """FP64 (mass, energy); raises SweError (SWE_ERR_NONFINITE) when the state holds NaN/Inf."""
         out = np.zeros(2)
         check("swe_cuda_invariants", self.lib.swe_cuda_invariants(_p(out)))
         return out
@@ -320,6 +321,8 @@ class Ensemble:
                 "precision": self.PRECISIONS[int(out[4])]}
 
     def invariants(self) -> np.ndarray:
+        """FP64 (mass, energy) per member; raises SweError (SWE_ERR_NONFINITE) naming the first
+        member whose state holds NaN/Inf."""
         out = np.zeros((self.members, 2))
         check("swe_ens_invariants", self.lib.swe_ens_invariants(_p(out)))
         return out

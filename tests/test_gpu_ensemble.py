@@ -123,6 +123,21 @@ def test_ensemble_invariants_fp64(ens, model_l4):
     assert np.allclose(got, want, rtol=1e-6)
 
 
+def test_invariants_watchdog_names_the_non_finite_member(ens, model_l4):
+    m = model_l4
+    ens.init(m, 32)
+    H0 = _members(m, 32)
+    H0[5].reshape(-1, 4)[17, 3] = np.nan
+    ens.set_state(H0)
+    ens.step(1)
+    with pytest.raises(capi.SweError, match="member 5") as e:
+        ens.invariants()
+    assert e.value.status == 7
+    ens.set_state(_members(m, 32))
+    ens.step(1)
+    assert np.isfinite(ens.invariants()).all()
+
+
 def test_rejects_bad_member_count(ens, model_l4):
     with pytest.raises(capi.SweError):
         ens.init(model_l4, 48)

@@ -216,6 +216,25 @@ def test_out_of_range_index_is_rejected(plain):
     assert rel_err(plain.eval_rhs(m.H_init), oracle.Port(m, "fp64").eval_rhs(m.H_init)).max() <= 1e-12
 
 
+def test_invariants_watchdog_reports_non_finite_state(plain, grid_l4):
+    """A NaN in the state (here one node's h in the initial state) makes the FP64
+    conservation sums non-finite; swe_cuda_invariants reports SWE_ERR_NONFINITE and
+    the library stays usable."""
+    _, d = grid_l4
+    m = swe_input.to_model(d)
+    plain.init_model(m, "fp64")
+    H = m.H_init.copy().reshape(-1, 4)
+    H[17, 3] = np.nan
+    plain.set_state(H)
+    plain.step(2)
+    with pytest.raises(capi.SweError, match="NaN or Inf") as e:
+        plain.invariants()
+    assert e.value.status == 7
+    plain.set_state(m.H_init)
+    plain.step(2)
+    assert np.isfinite(plain.invariants()).all()
+
+
 def test_invariants_match_oracle(plain, grid_l4):
     _, d = grid_l4
     m = swe_input.to_model(d)
