@@ -282,6 +282,14 @@ class Ensemble:
         check("swe_ens_get_state", self.lib.swe_ens_get_state(_p(H)))
         return H
 
+    def set_state_ptr(self, addr: int) -> None:
+        """[members][n][4] FP64 from a host address (pinned for full PCIe speed); asynchronous."""
+        check("swe_ens_set_state", self.lib.swe_ens_set_state(addr))
+
+    def get_state_ptr(self, addr: int) -> None:
+        """[members][n][4] FP64 to a host address; synchronises."""
+        check("swe_ens_get_state", self.lib.swe_ens_get_state(addr))
+
     def eval_rhs(self, K: np.ndarray) -> np.ndarray:
         K = np.ascontiguousarray(K, dtype=np.float64).reshape(self.members, self.n, 4)
         F = np.empty_like(K)
