@@ -93,3 +93,29 @@ def test_plain_kernel_names_match_selection_codes():
                 assert bench.PLAIN_KERNELS[name] == capi.Plain.lane_shape(lanes, ctas, pf), name
     codes = [v for v in bench.PLAIN_KERNELS.values() if v is not None]
     assert len(codes) == len(set(codes)) and max(codes) == 23 and min(codes) == 1
+
+
+def test_reference_arm_line_on_rank0(capsys, monkeypatch):
+    """bench.py --impl reference on rank 0: one JSON line with the contract's keys, the
+    reference's own CPU code timed on the host cores, and vs_baseline against the
+    reference's recorded rate for this workload."""
+    import json
+    import types
+
+    sys.path.insert(0, ROOT)
+    import bench
+    import oracle
+
+    if not oracle.reference_available("fp64", "cfdl"):
+        pytest.skip("the reference was not built here")
+    monkeypatch.setenv("RANK", "0")
+    args = types.SimpleNamespace(gpus=1, steps=1, warmup=1)
+    bench.run_reference(args, 6, "fp64", "plain_fp64_n40962")
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    for key in ("metric", "value", "unit", "impl", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+    assert abs(line["vs_baseline"] - line["value"] / bench.RECORDED_RATE["plain_fp64_n40962"][0]) < 1e-12
