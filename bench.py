@@ -20,13 +20,24 @@ nothing else, so step time / 4) against the measured HBM copy bandwidth.  Multi-
 are independent replicas (the path does not shard across GPUs here): every
 rank steps its own state, time is the max over ranks, value is the sum.
 
+The default run also carries the targets quoted for the larger workloads, in
+`targets`: the plain FP64 form at N=163842 and N=655362 (data far beyond L2, so
+their roofline is an HBM roofline) and the 64-member 3xTF32 batched form at
+N=163842 (member-steps/s, its ratio to the plain FP64 form on the same grid, and
+the h error of all 64 members after 1000 steps against the plain FP64 GPU run).
+The default workload's own data (57 MB of algorithmic bytes per stage) fits the
+126 MB L2, so its roofline is labelled L2-resident.
+
 --impl reference times the reference's own CPU code (oracle/_ref, built from
 the reference's sources; the oracle port if that is absent) on the host cores
-with OpenMP, on the same workload.
+with OpenMP, on the same workload.  Both arms read one input file: the
+workload's grid is generated once (seeded, CPU generator) into the reference's
+binary format and reused by the other arm; its SHA-256 prefix is in `config`.
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -81,6 +92,8 @@ PLAIN_KERNELS = {"auto": None, "register": 1, "pipelined64": 2, "pipelined32": 3
                  "lane1d": 18, "lane2d": 19, "lane4d": 20, "lane1dpf": 21, "lane2dpf": 22, "lane4dpf": 23}
 L2_FLUSH_BYTES = 256 << 20
 L2_NOTE = "flushed between timed steps: 256 MB write, then 256 MB read (cold, clean L2 at each step)"
+L2_NOTE_BOTH = ("GPU arm: L2 flushed between timed steps (256 MB write, then 256 MB read: cold, clean L2 at "
+                "each step); CPU arm: no flush")
 # DRAM bytes (read + write) per launch of the dominant kernel, from ncu captures of the same
 # command (dram__bytes_read.sum + dram__bytes_write.sum, averaged over the captured launches);
 # the profile summaries under profiles/ give the commands.
@@ -258,53 +271,101 @@ def build_workload(level: int, prec: str, device: str):
     return d, m, pm
 
 
-def cpu_baseline_sample(d, prec: str, target_s: float = 15.0):
-    """The reference's own CPU code (oracle/_ref) on a bounded number of steps."""
+def workload_input(level: int):
+    """(path, SweInput, sha256 prefix) of the workload's input file, which both arms read.
+    The first arm to run generates it (seeded, CPU generator) in the reference's binary
+    format; later runs on the same host read it back."""
+    from swe_b200 import gen, swe_input
+
+    ddir = os.environ.get("SWE_BENCH_DATA") or os.path.join(tempfile.gettempdir(), "swe_b200_bench")
+    os.makedirs(ddir, exist_ok=True)
+    path = os.path.join(ddir, f"icos{10 * 4 ** level + 2}_seed1.bin")
+    t0 = time.time()
+    try:
+        d = swe_input.read_input(path)
+        how = "read"
+    except (OSError, ValueError):
+        d = gen.generate(level, seed=1, device="cpu")
+        swe_input.write_input(path, d)
+        how = "generated"
+    h = hashlib.sha256()
+    with open(path, "rb") as fh:
+        for block in iter(lambda: fh.read(1 << 24), b""):
+            h.update(block)
+    log(f"[bench] input {path} {how} in {time.time() - t0:.1f}s")
+    return path, d, h.hexdigest()[:16]
+
+
+def plain_config(wl: str, desc: str, d, sha: str) -> dict:
+    """The workload's config, the same dict in both arms."""
+    return {"workload": wl, "description": desc, "nodes": d.N, "nnbr": d.Nnbr, "dt": d.dt, "layout": "CFDL",
+            "rcm": True, "input": f"icos{d.N}_seed1.bin sha256:{sha}", "l2": L2_NOTE_BOTH}
+
+
+def cpu_baseline_sample(path: str, d, prec: str, target_s: float = 12.0):
+    """The reference's own CPU code (oracle/_ref) on a bounded number of steps, on every
+    CPU this process may use (affinity set and cgroup quota), and on one thread beside
+    it.  Rates are whole RK_substep loops (RHS and combine), 4 N steps / seconds; the
+    reference's own Eval_Rhs timer (profiling.c:118-126) gives eval_rhs_value."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from swe_b200 import swe_input
 
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    cpu = oracle.usable_cpus()
+    threads = int(os.environ.get("OMP_NUM_THREADS", cpu["threads"]))
+    os.environ["OMP_NUM_THREADS"] = str(threads)
     os.environ.setdefault("OMP_PROC_BIND", "close")
     os.environ.setdefault("OMP_SCHEDULE", "static")
-    tmp = tempfile.mkdtemp(prefix="swe_bench_")
-    path = os.path.join(tmp, f"icos{d.N}.bin")
-    swe_input.write_input(path, d)
+
+    def sized(run_one, budget):
+        t1 = run_one(1)[0]                        # warm-up step, also sizes the sample
+        steps = max(1, min(200, int(budget / max(t1, 1e-4))))
+        t, t_rhs = run_one(steps)
+        return steps, t, t_rhs
+
     if oracle.reference_available(prec, "cfdl"):
         ref = oracle.Ref(path, prec, "cfdl", use_rcm=1)
-        H = ref.H_init()
-        H, t1, _ = ref.run(H, 1)                    # warm-up step, also sizes the sample
-        steps = max(1, min(200, int(target_s / max(t1, 1e-4))))
-        H, t, t_rhs = ref.run(H, steps)
-        kind = "reference"
-        sample = f"{steps} RK4 steps of the reference's RK_substep (OpenMP, {cores} threads, CFDL, RCM) on N={d.N}"
+        H0 = ref.H_init()
+
+        def run_one(k):
+            _, t, t_rhs = ref.run(H0, k)
+            return t, t_rhs
+        kind, what = "reference", "the reference's RK_substep (CFDL, RCM)"
     else:
         m = swe_input.to_model(d)
         port = oracle.Port(m, prec)
-        t0 = time.time()
-        port.run(m.H_init, 1)
-        t1 = time.time() - t0
-        steps = max(1, min(200, int(target_s / max(t1, 1e-4))))
-        t0 = time.time()
-        port.run(m.H_init, steps)
-        t = time.time() - t0
-        kind = "port"
-        sample = f"{steps} RK4 steps of the C port (OpenMP, {cores} threads) on N={d.N}"
-    os.remove(path)
-    return {"value": 4.0 * d.N * steps / t, "unit": "node-stage updates/s", "cores": cores,
-            "kind": kind, "sample": sample, "seconds": round(t, 3)}
+
+        def run_one(k):
+            t0 = time.perf_counter()
+            port.run(m.H_init, k)
+            t = time.perf_counter() - t0
+            return t, None
+        kind, what = "port", "the oracle's C restatement"
+    oracle.set_thread_count(threads)
+    steps, t, t_rhs = sized(run_one, target_s)
+    oracle.set_thread_count(1)
+    steps1, t1, _ = sized(run_one, target_s / 3)
+    oracle.set_thread_count(threads)
+    rate = 4.0 * d.N * steps / t
+    one = 4.0 * d.N * steps1 / t1
+    return {"value": rate, "unit": "node-stage updates/s", "cores": threads, "kind": kind,
+            "sample": f"{steps} RK4 steps of {what}, OpenMP on {threads} threads, on N={d.N} "
+                      f"(one-thread figure: {steps1} steps)",
+            "seconds": round(t, 3),
+            "eval_rhs_value": (4.0 * d.N * steps / t_rhs) if t_rhs else None,
+            "one_thread_value": one, "speedup_vs_one_thread": rate / one,
+            "cpu": {"model": cpu["model"], "threads_used": threads, "affinity_cpus": cpu["affinity"],
+                    "cgroup_quota_cpus": cpu["cgroup_quota_cpus"], "os_cpu_count": cpu["cpu_count"],
+                    "omp": {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OMP_PROC_BIND", "OMP_SCHEDULE")}}}
 
 
-def run_reference(args, level, prec, wl):
+def run_reference(args, level, prec, wl, desc):
     """--impl reference: the reference's own CPU implementation, rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from swe_b200 import gen
-
-    d = gen.generate(level, seed=1, device="cpu")
-    base = cpu_baseline_sample(d, prec, target_s=max(5.0, 2.0 * args.steps))
+    path, d, sha = workload_input(level)
+    base = cpu_baseline_sample(path, d, prec, target_s=max(5.0, 0.6 * args.steps))
     line = {
         "metric": "node-stage updates/s (RK4 + RBF-FD stage, plain form)",
         "value": base["value"], "unit": "node-stage updates/s", "impl": "reference",
@@ -312,7 +373,8 @@ def run_reference(args, level, prec, wl):
         "ms_per_step": 1e3 * 4.0 * d.N / base["value"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": vs_recorded(wl, base["value"])[0], "vs_baseline_source": vs_recorded(wl, base["value"])[1],
         "dtype": "f64" if prec == "fp64" else "f32", "data": "synthetic",
-        "config": {"workload": wl, "nodes": d.N, "nnbr": 31, "dt": d.dt, "layout": "CFDL", "rcm": True},
+        "config": plain_config(wl, desc, d, sha),
+        "parallelism": f"OpenMP x{base['cores']} on the host (rank 0 only)",
         "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": "node-stage updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -320,145 +382,212 @@ def run_reference(args, level, prec, wl):
     print(json.dumps(line), flush=True)
 
 
-def run_ensemble(args, level, desc, members=64, precision="tf32x3"):
-    """member-steps/s of the batched form (3xTF32 or split BF16), next to the plain FP64
-    form on the same grid, with the h error of a few members against the plain FP64 run."""
+def timed_steps(step, stream, steps: int, flush) -> list:
+    """Seconds of each of `steps` calls of step(), CUDA events on the library's stream,
+    L2 flushed (untimed) before each."""
+    import torch
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    sync_ranks()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for s in range(steps):
+            flush()
+            starts[s].record(stream)
+            step()
+            stops[s].record(stream)
+    torch.cuda.synchronize()
+    sync_ranks()
+    return [a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops)]
+
+
+def sample_clocks(local: int, run, keep_busy):
+    """run() inside an nvidia-smi sampler; keep_busy() repeats untimed work until 3 samples
+    cover the region.  Returns (run's result, clock summary)."""
+    with ClockSampler(local) as clocks:
+        clocks.wait_for(1, 5.0)
+        first = clocks.count()
+        out = run()
+        clocks.wait_for(first + 3, 5.0, keep_busy=keep_busy)
+    return out, clocks.summary(first)
+
+
+def plain_target(wl: str, local: int, steps: int, warmup: int, flush, world: int) -> dict:
+    """One plain workload, timed like the headline line (per-step events, L2 flushed between
+    steps); an HBM roofline where the data is far beyond L2."""
+    import torch
+
+    from swe_b200 import capi
+
+    level, prec, desc = WORKLOADS[wl]
+    d, m, pm = build_workload(level, prec, device=f"cuda:{local}")
+    N = d.N
+    plain = capi.Plain()
+    plain.init_model(pm, prec)
+    plain.set_state(pm.H_init.astype(np.float64 if prec == "fp64" else np.float32))
+    for _ in range(warmup):
+        plain.step(1)
+    plain.sync()
+    stream = torch.cuda.ExternalStream(plain.stream())
+
+    def busy():
+        for _ in range(20):
+            plain.step(1)
+        plain.sync()
+    t, clocks = sample_clocks(local, lambda: timed_steps(lambda: plain.step(1), stream, steps, flush), busy)
+    t_total = max_over_ranks(sum(t), f"cuda:{local}")
+    t_kernel = t_total / (4 * steps)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = ALG_BYTES[prec] * N / t_kernel / 1e9
+    kinfo = plain.kernel_info()
+    plain.finalize()
+    return {"workload": wl, "description": desc, "value": 4.0 * N * steps * world / t_total,
+            "unit": "node-stage updates/s", "member_steps_per_s": steps * world / t_total,
+            "steps": steps, "ms_per_step": 1e3 * t_total / steps, "dtype": "f64" if prec == "fp64" else "f32",
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(wl),
+                         "peak_source": peak_kind, "kernel": "swe::stage_lane_kernel" if kinfo["in_use"] == "lane"
+                         else kinfo["in_use"], "kernel_us": round(t_kernel * 1e6, 2),
+                         "alg_bytes_per_node_stage": ALG_BYTES[prec], "kernel_choice": kinfo},
+            "clocks": clocks}
+
+
+def ensemble_target(wl: str, local: int, steps: int, warmup: int, flush, world: int, err_steps: int = 1000,
+                    err_members: int = 64, members: int = 64, plain_rate: float | None = None,
+                    with_e2e: bool = False) -> dict:
+    """member-steps/s of the batched form (3xTF32 or split BF16), its ratio to the plain FP64
+    form on the same grid (timed the same way: per-step events, L2 flushed between steps),
+    and the per-field error of `err_members` members after `err_steps` steps against the
+    plain FP64 GPU run of the same member (u, v, w on the velocity scale, h on max|h|)."""
     import torch
 
     from swe_b200 import capi, gen
 
-    rank, local, world = world_info()
-    torch.cuda.set_device(local)
-    init_replicas()
+    level, precision, desc = WORKLOADS[wl]
     d, m, pm = build_workload(level, "fp64", device=f"cuda:{local}")
     N = d.N
     H0 = np.stack([gen.perturb_h(m.H_init, 1000 + b) for b in range(members)])
     ens = capi.Ensemble()
-    capi.check("swe_cuda_select_device", ens.lib.swe_cuda_select_device(local))
     ens.init(m, members)
     ens.set_precision(precision)
     ens.set_state(H0)
     tune_ms = ens.tune().tolist()
     cfg = ens.config()
-    stream = torch.cuda.ExternalStream(ens.stream())
-    flush = L2Flush(f"cuda:{local}")
-    for _ in range(args.warmup):
+    ens.set_state(H0)
+    for _ in range(warmup):
         ens.step(1)
     ens.sync()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stream = torch.cuda.ExternalStream(ens.stream())
     launches0 = capi.kernel_launches()
-    with ClockSampler(local) as clocks:
-        clocks.wait_for(1, 5.0)
-        first = clocks.count()
-        sync_ranks()
-        torch.cuda.synchronize()
-        torch.cuda.profiler.start()
-        with torch.cuda.stream(stream):
-            for s in range(args.steps):
-                flush()
-                starts[s].record(stream)
-                ens.step(1)
-                stops[s].record(stream)
-        torch.cuda.synchronize()
-        torch.cuda.profiler.stop()
-        sync_ranks()
-        launches = capi.kernel_launches() - launches0
-        t_total = sum(a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops))
 
-        def busy():
-            for _ in range(20):
-                ens.step(1)
-            ens.sync()
-        clocks.wait_for(first + 3, 5.0, keep_busy=busy)
-    ens.sync()
-    t_total = max_over_ranks(t_total, f"cuda:{local}")
-    member_steps = members * args.steps * world / t_total
-    t_stage = t_total / (4 * args.steps)
+    def busy():
+        for _ in range(5):
+            ens.step(1)
+        ens.sync()
+    t, clocks = sample_clocks(local, lambda: timed_steps(lambda: ens.step(1), stream, steps, flush), busy)
+    launches = capi.kernel_launches() - launches0
+    t_total = max_over_ranks(sum(t), f"cuda:{local}")
+    member_steps = members * steps * world / t_total
+    t_stage = t_total / (4 * steps)
     ens_bytes = ENS_SHARED_BYTES + members * ENS_MEMBER_BYTES
     peak, peak_kind = measured_peak_hbm()
     achieved = ens_bytes * N / t_stage / 1e9
 
-    # e2e through the C ABI with pinned host buffers: host state in, one step, host state out
-    H_pin = torch.from_numpy(np.ascontiguousarray(H0, dtype=np.float64).reshape(-1)).pin_memory()
-    H_back = torch.empty_like(H_pin).pin_memory()
-    e2e_steps = max(3, args.steps // 4)
-    ens.set_state_ptr(H_pin.data_ptr())
-    ens.step(1)
-    ens.get_state_ptr(H_back.data_ptr())
-    sync_ranks()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    e2e = None
+    if with_e2e:
+        # through the C ABI with pinned host buffers: host state in, one step, host state out
+        H_pin = torch.from_numpy(np.ascontiguousarray(H0, dtype=np.float64).reshape(-1)).pin_memory()
+        H_back = torch.empty_like(H_pin).pin_memory()
+        e2e_steps = max(3, steps // 4)
         ens.set_state_ptr(H_pin.data_ptr())
         ens.step(1)
-        ens.get_state_ptr(H_back.data_ptr())       # synchronises
-    t_e2e = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
-    Hout = H_back.numpy().reshape(members, -1, 4)
-    nbytes = H_pin.numel() * H_pin.element_size()
+        ens.get_state_ptr(H_back.data_ptr())
+        sync_ranks()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ens.set_state_ptr(H_pin.data_ptr())
+            ens.step(1)
+            ens.get_state_ptr(H_back.data_ptr())       # synchronises
+        t_e2e = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
+        nbytes = H_pin.numel() * H_pin.element_size()
+        e2e = {"value": members * e2e_steps * world / t_e2e, "unit": "member-steps/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
 
-    # plain FP64 on the same grid: member-steps/s = steps/s of one state
     plain = capi.Plain()
-    plain.init_model(pm, "fp64")
-    plain.set_state(pm.H_init)
-    for _ in range(3):
-        plain.step(1)
-    plain.sync()
-    # timed as the ensemble steps are: one step per pair of events, L2 flushed between
-    pstream = torch.cuda.ExternalStream(plain.stream())
-    p_starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    p_stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    with torch.cuda.stream(pstream):
-        for s in range(args.steps):
-            flush()
-            p_starts[s].record(pstream)
+    if plain_rate is None:
+        # plain FP64 on the same grid (RCM order, the drop-in's own order): member-steps/s =
+        # steps/s of one state
+        plain.init_model(pm, "fp64")
+        plain.set_state(pm.H_init)
+        for _ in range(3):
             plain.step(1)
-            p_stops[s].record(pstream)
-    torch.cuda.synchronize()
-    plain_steps = args.steps / sum(a.elapsed_time(b) * 1e-3 for a, b in zip(p_starts, p_stops))
+        plain.sync()
+        pt = timed_steps(lambda: plain.step(1), torch.cuda.ExternalStream(plain.stream()), steps, flush)
+        plain_rate = steps / max_over_ranks(sum(pt), f"cuda:{local}")
 
-    # h error after err_steps steps against the plain FP64 GPU run of the same members
-    # (natural node order, as the ensemble exchanges states)
+    # error after err_steps steps against the plain FP64 GPU run of the same members
+    # (natural node order, as the batched form exchanges states)
     plain.init_model(m, "fp64")
-    err_members = list(range(0, members, max(1, members // args.err_members)))[: args.err_members]
+    err_idx = list(range(0, members, max(1, members // err_members)))[:err_members]
     ens.set_state(H0)
-    ens.step(args.err_steps)
+    ens.step(err_steps)
     Hens = ens.get_state()
     errs = []
-    for b in err_members:
+    for b in err_idx:
         plain.set_state(H0[b])
-        plain.step(args.err_steps)
+        plain.step(err_steps)
         Hp = plain.get_state().reshape(-1, 4)
-        # max-norm error per field; u, v, w relative to the velocity scale max|(u,v,w)|
-        # (w starts at zero), h relative to max|h|
-        scale = np.array([np.abs(Hp[:, :3]).max()] * 3 + [np.abs(Hp[:, 3]).max()])
+        vel = np.abs(Hp[:, :3]).max()
+        scale = np.array([vel, vel, vel, np.abs(Hp[:, 3]).max()])
         errs.append(np.abs(Hens[b] - Hp).max(0) / scale)
     errs = np.array(errs)
     plain.finalize()
     ens.finalize()
+    return {"workload": wl, "description": desc, "value": member_steps, "unit": "member-steps/s",
+            "steps": steps, "ms_per_step": 1e3 * t_total / steps,
+            "dtype": f"{precision} (fp32 state, fp64 h accumulation)", "members": members,
+            "kernel_variant": cfg, "tune_ms_per_step": tune_ms,
+            "plain_fp64_member_steps_per_s": plain_rate, "ratio_vs_plain_fp64": member_steps / plain_rate,
+            "h_err_vs_fp64": {"steps": err_steps, "members": len(err_idx),
+                              "reference": "plain FP64 GPU run of the same member (itself within 1e-12 of the "
+                                           "oracle in the GPU tests)",
+                              "max_norm_rel_per_field_max": errs.max(0).tolist(),
+                              "h_max": float(errs[:, 3].max()), "h_median": float(np.median(errs[:, 3])),
+                              "h_worst_member": int(err_idx[int(errs[:, 3].argmax())])},
+            "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(wl),
+                         "peak_source": peak_kind, "kernel": "swe::ens_stage_kernel",
+                         "kernel_us": round(t_stage * 1e6, 2), "alg_bytes_per_node_stage": ens_bytes},
+            "clocks": clocks, "state_finite": bool(np.isfinite(Hens).all())}
+
+
+def run_ensemble(args, desc):
+    """--workload ens_*: the batched form as the line's own metric."""
+    import torch
+
+    rank, local, world = world_info()
+    torch.cuda.set_device(local)
+    init_replicas()
+    from swe_b200 import capi
+    capi.check("swe_cuda_select_device", capi.load().swe_cuda_select_device(local))
+    flush = L2Flush(f"cuda:{local}")
+    r = ensemble_target(args.workload, local, args.steps, args.warmup, flush, world, err_steps=args.err_steps,
+                        err_members=args.err_members, with_e2e=True)
     if rank == 0:
         line = {
-            "metric": f"member-steps/s (batched ensemble, {'3xTF32' if precision == 'tf32x3' else 'split BF16'} "
+            "metric": f"member-steps/s (batched ensemble, {'3xTF32' if 'tf32' in args.workload else 'split BF16'} "
                       "tcgen05) and ratio to plain FP64",
-            "value": member_steps, "unit": "member-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": f"{precision} (fp32 state, fp64 h accumulation)",
+            "value": r["value"], "unit": "member-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": r["dtype"],
             "data": "synthetic (seeded icosahedral grid, PHS RBF-FD weights, TC5 ICs, per-member 1e-3 h noise)",
-            "config": {"workload": args.workload, "description": desc, "nodes": N, "members": members,
-                       "dt": d.dt, "kernel_variant": cfg, "tune_ms_per_step": tune_ms,
-                       "l2": L2_NOTE},
-            "plain_fp64_member_steps_per_s": plain_steps,
-            "ratio_vs_plain_fp64": member_steps / plain_steps,
-            "h_err_vs_fp64": {"steps": args.err_steps, "members": err_members,
-                              "max_norm_rel_per_field_max": errs.max(0).tolist()},
-            "e2e": {"value": members * e2e_steps * world / t_e2e, "unit": "member-steps/s",
-                    "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
-            "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(args.workload), "peak_source": peak_kind,
-                         "kernel": "swe::ens_stage_kernel", "kernel_us": round(t_stage * 1e6, 2),
-                         "alg_bytes_per_node_stage": ens_bytes},
-            "clocks": clocks.summary(first),
-            "state_finite": bool(np.isfinite(Hout).all()),
+            "config": {"workload": args.workload, "description": desc, "members": r["members"],
+                       "kernel_variant": r["kernel_variant"], "l2": L2_NOTE},
+            "parallelism": f"replicas x{world}",
+            **{k: r[k] for k in ("plain_fp64_member_steps_per_s", "ratio_vs_plain_fp64", "h_err_vs_fp64", "e2e",
+                                 "gpu_launches", "roofline", "clocks", "state_finite", "tune_ms_per_step")},
         }
         print(json.dumps(line), flush=True)
     finish_replicas()
@@ -542,8 +671,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain_fp64_n40962", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--err-steps", type=int, default=100)
-    ap.add_argument("--err-members", type=int, default=4)
+    ap.add_argument("--no-targets", action="store_true",
+                    help="skip the nested lines of the larger workloads in the default run")
+    ap.add_argument("--target-steps", type=int, default=10, help="timed steps of each nested line")
+    ap.add_argument("--err-steps", type=int, default=1000)
+    ap.add_argument("--err-members", type=int, default=64)
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--seed", type=int, default=2026)
@@ -555,22 +687,30 @@ def main():
     args.warmup = max(args.warmup, 3)
     level, prec, desc = WORKLOADS[args.workload]
     if args.impl == "reference":
-        return run_reference(args, level if level else 6, "fp64" if prec in ("tf32x3", "bf16x3", "serve") else prec,
-                             args.workload)
+        rlevel = level if level else 6
+        rprec = "fp64" if prec in ("tf32x3", "bf16x3", "serve") else prec
+        return run_reference(args, rlevel, rprec, args.workload, desc)
     if prec in ("tf32x3", "bf16x3"):
-        return run_ensemble(args, level, desc, precision=prec)
+        return run_ensemble(args, desc)
     if prec == "serve":
         return run_serving(args, desc)
 
     import torch
 
-    from swe_b200 import capi
+    from swe_b200 import capi, layout, swe_input
 
     rank, local, world = world_info()
     torch.cuda.set_device(local)
     init_replicas()
 
-    d, m, pm = build_workload(level, prec, device=f"cuda:{local}")
+    if level <= 6:
+        # the input file the reference arm reads too
+        path, d, sha = workload_input(level)
+        m = swe_input.to_model(d)
+        pm, _ = layout.prepare(m, use_rcm=True, simd_length=32)
+    else:
+        path, sha = None, None
+        d, m, pm = build_workload(level, prec, device=f"cuda:{local}")
     N = d.N
     dt_np = np.float64 if prec == "fp64" else np.float32
     plain = capi.Plain()
@@ -581,36 +721,24 @@ def main():
     stream = torch.cuda.ExternalStream(plain.stream())
     flush = L2Flush(f"cuda:{local}")
 
-    plain.set_state(pm.H_init)
+    plain.set_state(pm.H_init.astype(dt_np))
     for _ in range(args.warmup):
         plain.step(1)
     plain.sync()
 
     # ---- device-resident timed region -------------------------------------------------
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     launches0 = capi.kernel_launches()
-    sync_ranks()
-    torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         clocks.wait_for(1, 5.0)
         first_sample = clocks.count()
         torch.cuda.profiler.start()                 # a profiler run with --profile-from-start off sees this loop only
-        with torch.cuda.stream(stream):
-            for s in range(args.steps):
-                flush()                       # L2 flush between timed steps (not timed)
-                starts[s].record(stream)
-                plain.step(1)
-                stops[s].record(stream)
-        torch.cuda.synchronize()
+        t_steps = timed_steps(lambda: plain.step(1), stream, args.steps, flush)
         torch.cuda.profiler.stop()
-        sync_ranks()
         launches = capi.kernel_launches() - launches0
-        t_steps = [a.elapsed_time(b) * 1e-3 for a, b in zip(starts, stops)]
         t_total = float(sum(t_steps))
 
-        # ---- per-stage kernel durations for the roofline (same stream, events), right
-        # after the timed steps and at the same clocks --------------------------------------
+        # ---- per-stage kernel durations (same stream, events), right after the timed
+        # steps and at the same clocks -------------------------------------------------------
         plain.set_timing(True)
         with torch.cuda.stream(stream):
             for s in range(max(3, args.steps // 4)):
@@ -659,22 +787,51 @@ def main():
     t_isolated = k_time / max(k_launches, 1)
     achieved = ALG_BYTES[prec] * N / t_kernel / 1e9
     kinfo = plain.kernel_info()
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(args.workload), "peak_source": peak_kind,
+    alg_per_launch = ALG_BYTES[prec] * N
+    traffic = TRAFFIC_BYTES.get(args.workload)
+    # data that fits the 126 MB L2 (with the flush's lines and headroom) is served from L2
+    # for most of each step: its roofline is not an HBM roofline
+    l2_resident = alg_per_launch < 100e6
+    roofline = {"bound": "l2-resident" if l2_resident else "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                 "kernel": {"pipelined": "swe::stage_tma_kernel", "register": "swe::stage_kernel",
                            "lane": "swe::stage_lane_kernel"}[kinfo["in_use"]],
                 "kernel_us": round(t_kernel * 1e6, 2), "kernel_us_isolated": round(t_isolated * 1e6, 2),
-                "alg_bytes_per_node_stage": ALG_BYTES[prec],
+                "alg_bytes_per_node_stage": ALG_BYTES[prec], "alg_bytes_per_launch": alg_per_launch,
                 "kernel_choice": kinfo}
+    if l2_resident:
+        roofline["note"] = (f"{alg_per_launch / 1e6:.1f} MB of algorithmic bytes per launch fit the 126 MB L2: "
+                            "'achieved' counts them over the stage time and 'frac' divides that by the measured "
+                            "HBM copy peak, an effective-bandwidth figure, not an HBM fraction; the HBM rooflines "
+                            "are the targets' lines (N=163842 and N=655362)")
+        if traffic:
+            roofline["dram_achieved"] = round(traffic / t_kernel / 1e9, 1)
+            roofline["dram_frac"] = round(traffic / t_kernel / 1e9 / peak, 4)
+    plain.finalize()
+
+    targets = None
+    if args.workload == "plain_fp64_n40962" and not args.no_targets:
+        targets = {}
+        for wl in ("plain_fp64_n163842", "plain_fp64_n655362"):
+            targets[wl] = plain_target(wl, local, args.target_steps, args.warmup, flush, world)
+        targets["ens_tf32_n163842_b64"] = ensemble_target(
+            "ens_tf32_n163842_b64", local, args.target_steps, args.warmup, flush, world,
+            err_steps=args.err_steps, err_members=args.err_members,
+            plain_rate=targets["plain_fp64_n163842"]["member_steps_per_s"] / world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline_sample(d, prec)
+            if path is None:
+                path, d, _ = workload_input(level)
+            cpu = cpu_baseline_sample(path, d, prec)
         except Exception as e:            # reported, not fatal
             cpu = {"value": None, "unit": "node-stage updates/s", "error": str(e)[:200]}
 
     if rank == 0:
+        config = plain_config(args.workload, desc, d, sha) if sha else \
+            {"workload": args.workload, "description": desc, "nodes": N, "nnbr": d.Nnbr, "dt": d.dt,
+             "layout": "CFDL", "rcm": True, "input": "generated on the GPU (seed 1)", "l2": L2_NOTE}
         line = {
             "metric": "node-stage updates/s (RK4 + RBF-FD stage, plain form)",
             "value": value, "unit": "node-stage updates/s", "n_gpus": world, "steps": args.steps,
@@ -683,9 +840,8 @@ def main():
             "vs_baseline_source": vs_recorded(args.workload, value)[1],
             "dtype": "f64" if prec == "fp64" else "f32",
             "data": "synthetic (seeded icosahedral grid, PHS RBF-FD weights, TC5 Gaussian-mountain ICs)",
-            "config": {"workload": args.workload, "description": desc, "nodes": N, "nnbr": 31, "dt": d.dt,
-                       "layout": "CFDL", "rcm": True, "parallelism": f"replicas x{world}",
-                       "l2": L2_NOTE},
+            "config": config,
+            "parallelism": f"replicas x{world}",
             "e2e": {"value": e2e, "unit": "node-stage updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
             "gpu_launches": int(launches),
@@ -694,8 +850,9 @@ def main():
             "clocks": clocks.summary(first_sample),
             "state_finite": finite,
         }
+        if targets is not None:
+            line["targets"] = targets
         print(json.dumps(line), flush=True)
-    plain.finalize()
     finish_replicas()
 
 

@@ -73,8 +73,10 @@ int swe_cuda_init(int fsize, int layout, int simd_length,
                   const int* idx, const void* Dx, const void* Dy, const void* Dz, const void* L);
 
 /* State transfer, H of patch_size*4 values in the init layout (SVM_LIN_ID).
- * set_state also resets the RK registers (K <- H), as the reference's time
- * loop does at the start of each attempt (main.c:297, :308-314). */
+ * set_state writes H only.  The RK registers need no reset: the reference's
+ * time loop copies H into K at the start of each attempt (main.c:297,
+ * :308-314), and here stage 0 of every step reads H and writes K and D before
+ * any later stage reads them, so K and D never carry values across set_state. */
 int swe_cuda_set_state(const void* H);
 int swe_cuda_get_state(void* H);
 
@@ -261,9 +263,21 @@ int swe_ens_finalize(void);
  * the FP64 plain-form arithmetic.  swe_srv_poll returns 0 while queued or
  * running, 1 when done, 2 when cancelled (times[2] = seconds from submission
  * to admission and to completion, -1 until known); swe_srv_fetch copies the
- * final states and forgets the request.  swe_srv_stats fills out[9] =
+ * final states and forgets the request.  swe_srv_stats fills out[10] =
  * {kernel launches, admitted, completed, arena bytes in use, peak bytes in
- * use, budget, work items done, queued requests, running requests}. */
+ * use, budget, work items done, queued requests, running requests,
+ * dependency-wait failures}.
+ *
+ * Failure path.  Every wait of the persistent kernel is bounded.  A work item
+ * waits for its request's previous stage at most the dependency limit (10 s,
+ * swe_srv_set_dep_limit changes it; 1 ms .. 1 h).  When a wait runs out the
+ * kernel stops claiming work and ends; every request whose work was queued
+ * then fails (swe_srv_poll returns -SWE_ERR_TIMEOUT naming it), while queued
+ * and later requests run normally on a relaunched kernel.
+ * swe_srv_test_withhold(request, stage_index) is a test hook: the first work
+ * item of that stage (step * 4 + stage) of that request (of the next request
+ * submitted, when request < 0) is never queued, so the next stage's wait runs
+ * out. */
 int swe_srv_start(double budget_bytes, int max_requests);
 int swe_srv_add_grid(int n, int nnbr, double gh0, double dt, const int* idx,
                      const double* Dx, const double* Dy, const double* Dz, const double* L,
@@ -276,6 +290,8 @@ int swe_srv_fetch(int request, double* H);
 int swe_srv_cancel(int request);
 int swe_srv_stats(double* out);
 int swe_srv_stop(void);
+int swe_srv_set_dep_limit(double seconds);
+int swe_srv_test_withhold(int request, int stage_index);
 
 /* ---------------------------------------------------------------------------
  * Plain form without device allocation
@@ -297,7 +313,13 @@ int swe_srv_stop(void);
  * stream capture.  Calls share the array: calls that overlap on the GPU race
  * and must be serialised by the caller.  Kernels go to `stream` (a
  * cudaStream_t, NULL for the default stream); the call returns once they are
- * enqueued. */
+ * enqueued.  Every idx entry must lie in 0..n-1.  The kernels check each one
+ * as they gather: an entry outside that range is never dereferenced (the node's
+ * own row is read in its place, so that call's results are wrong) and the
+ * first one is recorded.  A call with nsteps = 0 steps nothing: it waits for
+ * `stream` and returns SWE_ERR_INDEX, naming the recorded (node, slot, value)
+ * in swe_cuda_last_error(), if any earlier call met such an entry (clearing
+ * the record), else SWE_OK. */
 #define SWE_NOALLOC_SCRATCH_BYTES (4u << 20)
 int swe_cuda_step_noalloc(int fsize, int n, int nnbr, double gh0, double dt, const int* idx,
                           const void* Dx, const void* Dy, const void* Dz, const void* L,

@@ -30,9 +30,54 @@ LAYOUTS = ("default", "cfdl", "sfdl", "cfdl_sfdl")
 LAYOUT_FLAGS = {"default": 0, "cfdl": 1, "sfdl": 2, "cfdl_sfdl": 3}
 
 
+def usable_cpus() -> dict:
+    """The CPUs this process may really use: its affinity set, capped by a cgroup CPU
+    quota (cgroup v2 cpu.max, else v1 cfs_quota_us / cfs_period_us) rounded down, at
+    least 1.  os.cpu_count() counts the machine's CPUs and ignores both, and a static
+    OpenMP schedule over more threads than the quota allows waits at every barrier
+    for threads that are not running."""
+    try:
+        affinity = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        affinity = os.cpu_count() or 1
+    quota = None
+    try:
+        q, period = open("/sys/fs/cgroup/cpu.max").read().split()[:2]
+        if q != "max":
+            quota = int(q) / int(period)
+    except (OSError, ValueError):
+        try:
+            q = int(open("/sys/fs/cgroup/cpu/cpu.cfs_quota_us").read())
+            period = int(open("/sys/fs/cgroup/cpu/cpu.cfs_period_us").read())
+            if q > 0:
+                quota = q / period
+        except (OSError, ValueError):
+            pass
+    threads = affinity if quota is None else max(1, min(affinity, int(quota)))
+    model = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"threads": threads, "affinity": affinity, "cpu_count": os.cpu_count(),
+            "cgroup_quota_cpus": quota, "model": model}
+
+
+def set_thread_count(n: int) -> None:
+    """OpenMP threads for later parallel regions of the calling thread (libgomp, which
+    the oracle and reference libraries link)."""
+    ctypes.CDLL("libgomp.so.1").omp_set_num_threads(int(n))
+
+
 def build(with_reference: bool | None = None) -> None:
     """Build the port (always) and the reference libraries (when the reference is present)."""
-    ref_root = os.environ.get("SWE_REFERENCE_DIR", "/root/reference")
+    # the reference project root: SWE_REFERENCE_DIR, else a checkout named `reference`
+    # beside this repository
+    ref_root = os.environ.get("SWE_REFERENCE_DIR",
+                              os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
     if with_reference is None:
         with_reference = os.path.isdir(os.path.join(ref_root, "swe_code"))
     targets = ["port"] + (["ref"] if with_reference else [])

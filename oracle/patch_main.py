@@ -1,5 +1,5 @@
 """Test infrastructure (oracle): the reference's own main program with the
-SWE_USE_CUDA switch that INTEGRATION.md describes, for an end-to-end check that
+SWE_USE_CUDA switch (the additions listed below), for an end-to-end check that
 the C host drives libswe_b200.so unchanged otherwise.
 
     python patch_main.py <reference>/swe_code/main/main.c _ref/main_cuda.c

@@ -122,11 +122,34 @@ class HistoryWriter {
             slots_[si].busy = true;
         }
         Slot& s = slots_[si];
-        SWE_TRY(fill(s.dbuf));
-        SWE_CUDA_TRY(cudaEventRecord(s.filled, compute));
-        SWE_CUDA_TRY(cudaStreamWaitEvent(copy_, s.filled, 0));
-        SWE_CUDA_TRY(cudaMemcpyAsync(s.hbuf, s.dbuf, rec_bytes_, cudaMemcpyDeviceToHost, copy_));
-        SWE_CUDA_TRY(cudaEventRecord(s.copied, copy_));
+        // a failure after the slot was taken gives the slot back and marks the writer
+        // failed, so that later snapshots report the error instead of waiting for a
+        // slot that would never be freed
+        int st = fill(s.dbuf);
+        cudaError_t ce = cudaSuccess;
+        const char* what = "filling a snapshot failed";
+        if (st == SWE_OK) {
+            if ((ce = cudaEventRecord(s.filled, compute)) != cudaSuccess ||
+                (ce = cudaStreamWaitEvent(copy_, s.filled, 0)) != cudaSuccess ||
+                (ce = cudaMemcpyAsync(s.hbuf, s.dbuf, rec_bytes_, cudaMemcpyDeviceToHost, copy_)) != cudaSuccess ||
+                (ce = cudaEventRecord(s.copied, copy_)) != cudaSuccess) {
+                st = SWE_ERR_CUDA;
+                what = cudaGetErrorString(ce);
+            }
+        }
+        if (st != SWE_OK) {
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                s.busy = false;
+                if (!failed_) {
+                    failed_ = true;
+                    err_ = what;
+                }
+            }
+            cv_.notify_all();
+            if (ce != cudaSuccess) set_error("history writer: %s", what);
+            return st;
+        }
         {
             std::lock_guard<std::mutex> lk(mu_);
             queue_.push_back({si, step});
@@ -144,8 +167,13 @@ class HistoryWriter {
         }
         cv_.notify_all();
         if (writer_.joinable()) writer_.join();
-        const bool failed = failed_;
-        const std::string err = err_;
+        bool failed;
+        std::string err;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            failed = failed_;
+            err = err_;
+        }
         const bool closed_ok = std::fclose(fp_) == 0;
         fp_ = nullptr;
         for (Slot& s : slots_) {
@@ -194,7 +222,12 @@ class HistoryWriter {
             Slot& s = slots_[j.slot];
             bool ok = cudaEventSynchronize(s.copied) == cudaSuccess;
             std::string why = ok ? "" : "a snapshot copy failed";
-            if (ok && !failed_) {
+            bool failed_before;
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                failed_before = failed_;
+            }
+            if (ok && !failed_before) {
                 const int64_t step = j.step;
                 const double t = (double)j.step * dt_;
                 ok = std::fwrite(&step, 8, 1, fp_) == 1 && std::fwrite(&t, 8, 1, fp_) == 1 &&

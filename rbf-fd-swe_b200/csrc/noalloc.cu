@@ -17,6 +17,14 @@
 // The kernels are the fused stage kernel's math (stage_kernel.cuh) reading the
 // caller's row-major arrays directly instead of the packed device layout that
 // swe_cuda_init builds, so no packing buffer is needed either.
+//
+// The other entry points check every stencil index while packing it; here the
+// indices are read straight from the caller's device array, so the kernel
+// checks them as it gathers.  An index outside 0..n-1 is never dereferenced:
+// the gather reads the node's own row instead (so that call's results are
+// wrong), and the first such (node, slot, value) is kept in g_noalloc_bad.  A
+// call with nsteps = 0 waits for `stream`, reports a kept record as
+// SWE_ERR_INDEX and clears it.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -31,6 +39,20 @@ constexpr size_t kNoallocScratchBytes = (size_t)4 << 20;
 static_assert(kNoallocScratchBytes == SWE_NOALLOC_SCRATCH_BYTES, "header and file disagree");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+// First out-of-range stencil index met by a kernel: {seen, node, slot, value}.
+// Zero at load; cleared by the nsteps = 0 call that reports it.
+static __device__ int g_noalloc_bad[4];
+
+__device__ __forceinline__ int checked_neighbour(int v, int n, long node, int slot) {
+    if ((unsigned)v < (unsigned)n) return v;
+    if (atomicCAS(&g_noalloc_bad[0], 0, 1) == 0) {
+        g_noalloc_bad[1] = (int)node;
+        g_noalloc_bad[2] = slot;
+        g_noalloc_bad[3] = v;
+    }
+    return (int)node;
+}
 
 // Device addresses of the scratch array, one per device, filled by the first
 // call on that device (cudaGetSymbolAddress with that device current).  In
@@ -75,7 +97,7 @@ __global__ void __launch_bounds__(kStageThreads) rowmajor_stage_kernel(const Row
                 const long e = ii * a.nnbr + j;
                 const T w[4] = {__ldg(a.Dx + e), __ldg(a.Dy + e), __ldg(a.Dz + e), __ldg(a.L + e)};
                 T kv[4];
-                Quad<T>::load_row(a.Kin + 4L * __ldg(a.idx + e), kv);
+                Quad<T>::load_row(a.Kin + 4L * checked_neighbour(__ldg(a.idx + e), a.n, ii, j), kv);
 #pragma unroll
                 for (int op = 0; op < 4; ++op)
 #pragma unroll
@@ -150,6 +172,20 @@ int scratch_for_current_device(void** out) {
     return SWE_OK;
 }
 
+// nsteps = 0: wait for the caller's stream, then report (and clear) the first
+// out-of-range stencil index any earlier call met.
+int report_bad_index(cudaStream_t stream) {
+    SWE_CUDA_TRY(cudaStreamSynchronize(stream));
+    int bad[4] = {0, 0, 0, 0};
+    SWE_CUDA_TRY(cudaMemcpyFromSymbol(bad, g_noalloc_bad, sizeof(bad)));
+    if (!bad[0]) return SWE_OK;
+    const int zero[4] = {0, 0, 0, 0};
+    SWE_CUDA_TRY(cudaMemcpyToSymbol(g_noalloc_bad, zero, sizeof(zero)));
+    set_error("swe_cuda_step_noalloc: an earlier call met idx[node %d][nbr %d] = %d outside 0..n-1; it read the "
+              "node's own row there, so its results are wrong", bad[1], bad[2], bad[3]);
+    return SWE_ERR_INDEX;
+}
+
 template <typename T>
 int run_noalloc(int n, int nnbr, double gh0, double dt, const int* idx, const void* Dx, const void* Dy,
                 const void* Dz, const void* L, const void* x, const void* y, const void* z, const void* f,
@@ -212,6 +248,7 @@ extern "C" int swe_cuda_step_noalloc(int fsize, int n, int nnbr, double gh0, dou
         return SWE_ERR_ARG;
     }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (nsteps == 0) return report_bad_index(s);
     return fsize == 8 ? run_noalloc<double>(n, nnbr, gh0, dt, idx, Dx, Dy, Dz, L, x, y, z, f, ghm, p_u, p_v, p_w,
                                             gradghm, H, nsteps, s)
                       : run_noalloc<float>(n, nnbr, gh0, dt, idx, Dx, Dy, Dz, L, x, y, z, f, ghm, p_u, p_v, p_w,

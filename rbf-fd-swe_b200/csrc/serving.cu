@@ -73,6 +73,7 @@ struct alignas(16) ReqDesc {   // device table entry of an admitted request
 
 struct Shared {          // host-mapped block the kernel writes (posted stores only)
     volatile int error;            // kernel-side error code
+    volatile int error_request;    // request whose dependency wait ran out (error 2)
     volatile long long progress;   // items completed (approximate mirror)
 };
 
@@ -80,12 +81,13 @@ struct DevCtl {          // device-resident control words the host sets by async
     long long tail;      // items published by the host
     int stop;            // host asks the kernel to exit
     int pad;
+    unsigned long long dep_ns;   // dependency wait limit
 };
 
 constexpr int kThreads = kStageThreads;         // 8 warps x 4 nodes
 static_assert(sizeof(ReqDesc) % 16 == 0 && sizeof(ReqDesc) / 16 <= kStageThreads, "descriptor copy");
 constexpr unsigned long long kIdleNs = 20ull * 1000 * 1000;          // idle exit after 20 ms
-constexpr unsigned long long kDepNs = 10ull * 1000 * 1000 * 1000;    // dependency wait limit 10 s
+constexpr unsigned long long kDepNs = 10ull * 1000 * 1000 * 1000;    // default dependency wait limit 10 s
 
 __device__ __forceinline__ unsigned long long globaltimer() {
     unsigned long long t;
@@ -226,15 +228,16 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
         if (threadIdx.x == 0) {
             s_ok = 1;
             const int need = it.q * r.per_stage;
+            const unsigned long long limit = *(volatile const unsigned long long*)&dctl->dep_ns;
             const unsigned long long t0 = globaltimer();
             // plain loads (served by L2, no atomic serialisation against the
             // increments on the critical path) with exponential backoff
             unsigned ns = 64;
             while (*(volatile const int*)(done + it.slot) < need) {
                 if (*(volatile const int*)&dctl->stop) { s_ok = 0; break; }
-                if (globaltimer() - t0 > kDepNs) {
+                if (globaltimer() - t0 > limit) {
                     s_ok = 0;
-                    atomicExch(kerr, 2);
+                    if (atomicExch(kerr, 2) == 0) ctl->error_request = r.id;
                     ctl->error = 2;
                     break;
                 }
@@ -298,6 +301,7 @@ struct Request {
     int next_step = 0;                   // steps appended so far
     long long appended = 0;              // items appended so far
     enum State { PENDING, UPLOADING, RUNNING, DRAINING, DONE, CANCELLED, FAILED } state = PENDING;
+    long long withhold_q = -1;           // test hook: stage index whose first item is never queued
     double t_submit = 0, t_admit = 0, t_done = 0;
     bool cancel_req = false;
 };
@@ -336,6 +340,8 @@ struct Server {
     std::deque<int> pending;
     std::vector<int> active;                      // slots order for round-robin
     int next_id = 0;
+    long long failures = 0;                       // dependency-wait failures recovered from
+    long long withhold_next_q = -1;               // test hook armed for the next submission
     cudaStream_t kstream = nullptr, cstream = nullptr, pstream = nullptr;
     long long launches = 0, admitted = 0, completed = 0;
     std::thread worker;
@@ -441,6 +447,10 @@ struct Server {
             const int q = r.next_step * 4 + st;
             for (int c = 0; c < nch; ++c)
                 for (int mb = 0; mb < r.members; ++mb) {
+                    if (q == r.withhold_q && c == 0 && mb == 0) {    // test hook: never queued
+                        ++r.appended;
+                        continue;
+                    }
                     Item& it = ring_h[tail % ring_cap];
                     it.slot = r.slot;
                     it.q = q;
@@ -531,8 +541,47 @@ struct Server {
         published = tail;
     }
 
+    // A dependency wait ran out (error 2): the kernel stops claiming work, and it
+    // ends once its other waits, bounded by the same limit, have ended.  Items it
+    // skipped are lost, so every request whose work was queued (RUNNING) fails;
+    // uploads in flight, drains and pending requests carry on.  The queue and its
+    // counters start again from zero, and the next pass relaunches the kernel.
+    void recover_from_dependency_timeout() {
+        for (size_t a = 0; a < active.size();) {
+            Request& r = requests[active[a]];
+            if (r.state == Request::RUNNING) {
+                retire(r, Request::FAILED);
+                active.erase(active.begin() + a);
+            } else {
+                ++a;
+            }
+        }
+        tail = published = 0;
+        hctl->tail = 0;
+        cudaMemcpyAsync(&dctl->tail, &hctl->tail, sizeof(long long), cudaMemcpyHostToDevice, cstream);
+        cudaMemsetAsync(head, 0, sizeof(unsigned long long), cstream);
+        cudaMemsetAsync(items_done, 0, sizeof(unsigned long long), cstream);
+        cudaMemsetAsync(kerr, 0, sizeof(int), cstream);
+        if (cudaStreamSynchronize(cstream) != cudaSuccess) {
+            fatal = "serving: reset after a dependency timeout failed";
+            return;
+        }
+        ctl->progress = 0;
+        ctl->error = 0;
+        ++failures;
+    }
+
     // one scheduler pass (called with mu held)
     void pass() {
+        if (ctl->error) {
+            if (ctl->error != 2) {
+                fatal = "serving kernel error";
+                return;
+            }
+            if (kernel_running()) return;
+            recover_from_dependency_timeout();
+            if (!fatal.empty()) return;
+        }
         // uploads done -> running; kernel done -> draining; drained -> done
         for (size_t a = 0; a < active.size();) {
             Request& r = requests[active[a]];
@@ -581,10 +630,7 @@ struct Server {
         }
         if (appended) publish();
         const bool work = tail > (long long)ctl->progress || !active.empty();
-        if (ctl->error) {
-            fatal = ctl->error == 2 ? "serving kernel: a dependency wait ran out" : "serving kernel error";
-            return;
-        }
+        if (ctl->error) return;                  // handled by the next pass
         const bool was_running = kernel_running();
         if (work && !was_running) launch_kernel();
         if (trace) {
@@ -657,7 +703,8 @@ int swe_srv_start(double budget_bytes, int max_requests) {
     if ((e = cudaMalloc(&S->dctl, sizeof(DevCtl))) != cudaSuccess) return fail("cudaMalloc ctl");
     if ((e = cudaMalloc(&S->kerr, sizeof(int))) != cudaSuccess) return fail("cudaMalloc err");
     memset(S->hctl, 0, sizeof(DevCtl));
-    cudaMemset(S->dctl, 0, sizeof(DevCtl));
+    S->hctl->dep_ns = kDepNs;
+    cudaMemcpy(S->dctl, S->hctl, sizeof(DevCtl), cudaMemcpyHostToDevice);
     cudaMemset(S->kerr, 0, sizeof(int));
     if ((e = cudaHostAlloc(&S->flags, sizeof(int) * max_requests, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc flags");
     if ((e = cudaHostAlloc(&S->mdone, sizeof(int) * max_requests, cudaHostAllocMapped)) != cudaSuccess) return fail("cudaHostAlloc mdone");
@@ -748,6 +795,8 @@ int swe_srv_submit(int grid, int members, int nsteps, const double* H0) {
         return -SWE_ERR_CUDA;
     }
     r.t_submit = now_s();
+    r.withhold_q = S.withhold_next_q;
+    S.withhold_next_q = -1;
     S.requests[r.id] = std::move(r);
     S.pending.push_back(S.requests.rbegin()->first);
     return S.requests.rbegin()->first;
@@ -768,8 +817,46 @@ int swe_srv_poll(int id, double* times) {
     switch (r.state) {
         case Request::DONE: return 1;
         case Request::CANCELLED: return 2;
+        case Request::FAILED:
+            set_error("swe_srv_poll: request %d failed: a dependency wait in the serving kernel ran out", id);
+            return -SWE_ERR_TIMEOUT;
         default: return 0;
     }
+}
+
+int swe_srv_set_dep_limit(double seconds) {
+    if (!g_srv) { set_error("swe_srv_set_dep_limit: server not started"); return SWE_ERR_STATE; }
+    if (!(seconds >= 1e-3 && seconds <= 3600.0)) {
+        set_error("swe_srv_set_dep_limit: limit %g s outside 1 ms .. 1 h", seconds);
+        return SWE_ERR_ARG;
+    }
+    Server& S = *g_srv;
+    std::lock_guard<std::mutex> lock(S.mu);
+    S.hctl->dep_ns = (unsigned long long)(seconds * 1e9);
+    SWE_CUDA_TRY(cudaMemcpyAsync(&S.dctl->dep_ns, &S.hctl->dep_ns, sizeof(unsigned long long),
+                                 cudaMemcpyHostToDevice, S.cstream));
+    SWE_CUDA_TRY(cudaStreamSynchronize(S.cstream));
+    return SWE_OK;
+}
+
+int swe_srv_test_withhold(int id, int stage_index) {
+    if (!g_srv) { set_error("swe_srv_test_withhold: server not started"); return SWE_ERR_STATE; }
+    Server& S = *g_srv;
+    std::lock_guard<std::mutex> lock(S.mu);
+    if (id < 0) {                       // arm the hook for the next submission
+        if (stage_index < 0) { set_error("swe_srv_test_withhold: negative stage index"); return SWE_ERR_ARG; }
+        S.withhold_next_q = stage_index;
+        return SWE_OK;
+    }
+    auto it = S.requests.find(id);
+    if (it == S.requests.end()) { set_error("swe_srv_test_withhold: unknown request %d", id); return SWE_ERR_ARG; }
+    Request& r = it->second;
+    if (stage_index < 4 * r.next_step || stage_index >= 4 * r.nsteps) {
+        set_error("swe_srv_test_withhold: stage index %d already queued or past the request's end", stage_index);
+        return SWE_ERR_ARG;
+    }
+    r.withhold_q = stage_index;
+    return SWE_OK;
 }
 
 int swe_srv_fetch(int id, double* H) {
@@ -825,6 +912,7 @@ int swe_srv_stats(double* out) {
     out[6] = (double)S.ctl->progress;
     out[7] = (double)S.pending.size();
     out[8] = (double)S.active.size();
+    out[9] = (double)S.failures;
     return SWE_OK;
 }
 

@@ -22,6 +22,18 @@ SWE_LAYOUT_SFDL = 2
 STATUS = {0: "SWE_OK", 1: "SWE_ERR_ARG", 2: "SWE_ERR_STATE", 3: "SWE_ERR_CUDA", 4: "SWE_ERR_NOMEM",
           5: "SWE_ERR_INDEX", 6: "SWE_ERR_TIMEOUT", 7: "SWE_ERR_NONFINITE", 8: "SWE_ERR_CANCELLED"}
 
+
+
+def _header_define(name: str) -> int:
+    m = re.search(r"#define\s+%s\s+\((\d+)u\s*<<\s*(\d+)\)" % name, open(HEADER).read())
+    if not m:
+        raise RuntimeError(f"{name} not found in {HEADER}")
+    return int(m.group(1)) << int(m.group(2))
+
+
+# bytes of the static device array swe_cuda_step_noalloc keeps K and D in
+NOALLOC_SCRATCH_BYTES = _header_define("SWE_NOALLOC_SCRATCH_BYTES")
+
 _lib = None
 
 
@@ -82,6 +94,8 @@ def load() -> ctypes.CDLL:
     lib.swe_srv_submit.argtypes = [i, i, i, vp]
     lib.swe_srv_poll.argtypes = [i, vp]
     lib.swe_srv_fetch.argtypes = [i, vp]
+    lib.swe_srv_set_dep_limit.argtypes = [d]
+    lib.swe_srv_test_withhold.argtypes = [i, i]
     lib.swe_srv_cancel.argtypes = [i]
     lib.swe_srv_stats.argtypes = [vp]
     _lib = lib
@@ -354,7 +368,7 @@ class Server:
     """The serving form (swe_srv_*): continuous batching of forecast requests."""
 
     STAT_NAMES = ("kernel_launches", "admitted", "completed", "bytes_in_use", "peak_bytes", "budget",
-                  "items_done", "queued", "running")
+                  "items_done", "queued", "running", "dependency_failures")
 
     def __init__(self, budget_bytes: float, max_requests: int = 256):
         self.lib = load()
@@ -400,8 +414,18 @@ class Server:
     def cancel(self, rid: int) -> None:
         check("swe_srv_cancel", self.lib.swe_srv_cancel(rid))
 
+    def set_dep_limit(self, seconds: float) -> None:
+        """Limit of a work item's wait for its request's previous stage."""
+        check("swe_srv_set_dep_limit", self.lib.swe_srv_set_dep_limit(ctypes.c_double(seconds)))
+
+    def test_withhold(self, rid: int, stage_index: int) -> None:
+        """Test hook: the first work item of stage `stage_index` (step * 4 + stage) of
+        request `rid` (of the next request submitted, when rid < 0) is never queued, so
+        the following stage's wait runs out."""
+        check("swe_srv_test_withhold", self.lib.swe_srv_test_withhold(int(rid), int(stage_index)))
+
     def stats(self) -> dict:
-        out = np.zeros(9)
+        out = np.zeros(10)
         check("swe_srv_stats", self.lib.swe_srv_stats(_p(out)))
         return dict(zip(self.STAT_NAMES, out.tolist()))
 

@@ -235,7 +235,8 @@ def perturb_h(H: np.ndarray, seed: int, noise: float = NOISE) -> np.ndarray:
 def generate(level: int, seed: int = 0, dt: float | None = None, device: str = "cpu",
              gamma_coef: float = GAMMA_COEF, native: bool | None = None,
              idx: np.ndarray | None = None, nnbr: int = NNBR) -> SweInput:
-    """A complete input (H_100 left zero; oracle/fill_fc.py fills it).
+    """A complete input.  H_100 is left zero: the generator has no reference run to
+    take it from (the tests fill it with the oracle's 100-step state where they need it).
 
     On a CUDA device the stencils and weights come from the library's GPU kernels
     (native, the default there); on the CPU from scipy and torch.  `idx` (0-based

@@ -13,6 +13,13 @@ for sub in ("rbf-fd-swe_b200", "oracle"):
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
+# The oracle's OpenMP loops get the CPUs this process may use (affinity and cgroup
+# quota), set before any oracle library loads.
+import oracle as _oracle  # noqa: E402
+
+os.environ.setdefault("OMP_NUM_THREADS", str(_oracle.usable_cpus()["threads"]))
+os.environ.setdefault("OMP_SCHEDULE", "static")
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
@@ -35,16 +42,18 @@ def pytest_collection_modifyitems(config, items):
 _grid_cache = {}
 
 
-def generated_input(level: int, seed: int = 1, fill_fc: bool = False, nnbr: int = 31):
-    """(path, SweInput) of a generated grid, written once per session under a temp dir."""
+def generated_input(level: int, seed: int = 1, fill_fc: bool = False, nnbr: int = 31, device: str = "cpu"):
+    """(path, SweInput) of a generated grid, written once per session under a temp dir.
+    device="cuda" makes the stencils and weights with the library's GPU generator (the
+    large grids); the oracle and the library then read the same arrays either way."""
     import tempfile
 
     from swe_b200 import gen, swe_input
 
-    key = (level, seed, fill_fc, nnbr)
+    key = (level, seed, fill_fc, nnbr, device)
     if key in _grid_cache:
         return _grid_cache[key]
-    d = gen.generate(level, seed=seed, nnbr=nnbr)
+    d = gen.generate(level, seed=seed, nnbr=nnbr, device=device)
     if fill_fc:
         import oracle
 
@@ -83,13 +92,27 @@ def rel_err(a, b):
     return np.abs(a - b).max(axis=0) / np.maximum(np.abs(b).max(axis=0), 1e-300)
 
 
-def abs_rhs(model, K):
+def scaled_err(a, b):
+    """Per-field max-norm error of [.., 4] states, u, v, w over the velocity scale
+    max|(u, v, w)| of b (w starts at zero in the test cases) and h over max|h|."""
+    a = np.asarray(a, dtype=np.float64).reshape(-1, 4)
+    b = np.asarray(b, dtype=np.float64).reshape(-1, 4)
+    vel = max(np.abs(b[:, :3]).max(), 1e-300)
+    scale = np.array([vel, vel, vel, max(np.abs(b[:, 3]).max(), 1e-300)])
+    return np.abs(a - b).max(axis=0) / scale
+
+
+def abs_rhs(model, K, chunk: int = 65536):
     """eval_RHS_swe (rk4_rbffd_swe.c:285-353) evaluated on absolute values with every
     subtraction turned into an addition: the running-error scale of each F entry."""
     Kf = np.abs(np.asarray(K, dtype=np.float64).reshape(-1, 4))
-    G = Kf[model.idx]                                             # [N, n, 4]
-    dX = [(np.abs(D)[:, :, None] * G).sum(1) for D in (model.Dx, model.Dy, model.Dz)]
-    LX = (np.abs(model.L)[:, :, None] * G).sum(1)
+    dX = [np.empty((model.N, 4)) for _ in range(3)]
+    LX = np.empty((model.N, 4))
+    for r0 in range(0, model.N, chunk):                           # [chunk, n, 4] gathers
+        rows = slice(r0, min(model.N, r0 + chunk))
+        G = Kf[model.idx[rows]]
+        for D, out in zip((model.Dx, model.Dy, model.Dz, model.L), dX + [LX]):
+            out[rows] = (np.abs(D[rows])[:, :, None] * G).sum(1)
     u, v, w, h = Kf[:, 0], Kf[:, 1], Kf[:, 2], Kf[:, 3]
     f, x, y, z = np.abs(model.f), np.abs(model.x), np.abs(model.y), np.abs(model.z)
     adv = [u * dX[0][:, c] + v * dX[1][:, c] + w * dX[2][:, c] for c in range(3)]

@@ -36,7 +36,7 @@ def _rank_main(rank, world, port, out):
         res["rate"] = bench.job_rate(100.0, 1.0 + rank)            # 100 units per rank
         if rank != 0:
             # the reference arm does no work on ranks other than 0
-            res["ref"] = bench.run_reference(None, 6, "fp64", "plain_fp64_n40962")
+            res["ref"] = bench.run_reference(None, 6, "fp64", "plain_fp64_n40962", "")
         bench.sync_ranks()
         bench.finish_replicas()
     except Exception as e:                                            # reported to the parent
@@ -110,8 +110,15 @@ def test_reference_arm_line_on_rank0(capsys, monkeypatch):
         pytest.skip("the reference was not built here")
     monkeypatch.setenv("RANK", "0")
     args = types.SimpleNamespace(gpus=1, steps=1, warmup=1)
-    bench.run_reference(args, 6, "fp64", "plain_fp64_n40962")
+    desc = bench.WORKLOADS["plain_fp64_n40962"][2]
+    bench.run_reference(args, 6, "fp64", "plain_fp64_n40962", desc)
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    # both arms read one input file and print one config dict
+    _, d, sha = bench.workload_input(6)
+    assert line["config"] == bench.plain_config("plain_fp64_n40962", desc, d, sha)
+    cpu = line["cpu_baseline"]
+    assert cpu["cores"] == cpu["cpu"]["threads_used"] >= 1 and cpu["one_thread_value"] > 0
+    assert cpu["cpu"]["affinity_cpus"] >= cpu["cores"] or os.environ.get("OMP_NUM_THREADS")
     for key in ("metric", "value", "unit", "impl", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
                 "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert key in line, key

@@ -71,3 +71,24 @@ def test_header_compiles_as_c_and_links(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.startswith("2 ") and "swe_cuda_init" in out.stdout
+
+
+def test_noalloc_argument_checks_fail_before_device_work():
+    """swe_cuda_step_noalloc checks its arguments before any CUDA call: a bad fsize,
+    stencil width, step count, node count or null pointer is rejected with
+    SWE_ERR_ARG.  The dummy pointers are never dereferenced."""
+    lib = capi.load()
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    lib.swe_cuda_step_noalloc.argtypes = [i, i, i, d, d] + [vp] * 15 + [i, vp]
+    dummy = [ctypes.c_void_p(16)] * 15
+    limit = capi.NOALLOC_SCRATCH_BYTES // (12 * 8)
+    assert lib.swe_cuda_step_noalloc(3, 100, 31, 0.0, 1.0, *dummy, 1, None) == 1
+    assert lib.swe_cuda_step_noalloc(8, 100, 33, 0.0, 1.0, *dummy, 1, None) == 1
+    assert b"nnbr" in lib.swe_cuda_last_error()
+    assert lib.swe_cuda_step_noalloc(8, 100, 31, 0.0, 1.0, *dummy, -1, None) == 1
+    assert lib.swe_cuda_step_noalloc(8, 0, 31, 0.0, 1.0, *dummy, 1, None) == 1
+    assert lib.swe_cuda_step_noalloc(8, limit + 1, 31, 0.0, 1.0, *dummy, 1, None) == 1
+    assert b"static scratch" in lib.swe_cuda_last_error()
+    assert lib.swe_cuda_step_noalloc(4, 2 * limit + 2, 31, 0.0, 1.0, *dummy, 1, None) == 1
+    assert lib.swe_cuda_step_noalloc(8, 100, 31, 0.0, 1.0, *([None] + dummy[1:]), 1, None) == 1
+    assert b"null" in lib.swe_cuda_last_error()

@@ -153,3 +153,22 @@ def test_short_stencils(ens):
     port = oracle.Port(m, "fp64")
     worst = max(cond_err(F[b], port.eval_rhs(K[b]), m, K[b]) for b in (0, 13, 31))
     assert worst <= COND_BOUND["tf32x3"], worst
+
+
+def test_pinned_state_round_trip_equals_pageable(ens, model_l4):
+    """set_state_ptr / get_state_ptr with pinned host buffers (the bench's e2e path) give
+    the same bits as set_state / get_state with pageable arrays."""
+    import torch
+
+    m = model_l4
+    ens.init(m, 32)
+    H0 = _members(m, 32)
+    ens.set_state(H0)
+    ens.step(3)
+    want = ens.get_state()
+    H_pin = torch.from_numpy(np.ascontiguousarray(H0).reshape(-1)).pin_memory()
+    H_back = torch.empty_like(H_pin).pin_memory()
+    ens.set_state_ptr(H_pin.data_ptr())
+    ens.step(3)
+    ens.get_state_ptr(H_back.data_ptr())
+    assert np.array_equal(H_back.numpy().reshape(want.shape), want)

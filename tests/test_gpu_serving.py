@@ -5,11 +5,16 @@
   drop-in form's result for the same state (FP64 arithmetic in both);
 * admission never lets the arena exceed the HBM budget, and requests that do
   not fit wait until earlier ones finish;
-* cancellation retires a request without results.
+* cancellation retires a request without results;
+* every served member equals the FP64 oracle's run of the same state and step
+  count (rk4_rbffd_swe.c:30-72) within 1e-12 relative per field;
+* a dependency wait that runs out (a work item withheld by the test hook) fails
+  the request with SWE_ERR_TIMEOUT, and the server then completes a clean request.
 """
 import numpy as np
 import pytest
 
+import oracle
 from conftest import generated_input, rel_err
 from swe_b200 import capi, gen, swe_input
 
@@ -102,3 +107,52 @@ def test_rejects_oversized_request(models):
         assert e.value.status == 4
     finally:
         srv.stop()
+
+
+def test_served_members_match_oracle(models):
+    """Requests of two grids, several member counts and lengths, overlapping on the
+    device; every member of every result against the oracle's own RK4 run."""
+    m3, m4 = models[3], models[4]
+    plan = [(m4, 3, 40, 11), (m3, 2, 60, 21), (m4, 1, 15, 31), (m3, 5, 25, 41), (m4, 4, 30, 51)]
+    srv = capi.Server(2 << 30)
+    try:
+        gids = {id(m4): srv.add_grid(m4), id(m3): srv.add_grid(m3)}
+        states = [_states(m, mb, seed) for m, mb, st, seed in plan]
+        rids = [srv.submit(gids[id(m)], H0, st) for (m, mb, st, seed), H0 in zip(plan, states)]
+        srv.wait(rids)
+        outs = [srv.fetch(r) for r in rids]
+    finally:
+        srv.stop()
+    ports = {id(m4): oracle.Port(m4, "fp64"), id(m3): oracle.Port(m3, "fp64")}
+    for (m, mb, st, seed), H0, out in zip(plan, states, outs):
+        for b in range(mb):
+            want = ports[id(m)].run(H0[b], st)
+            assert rel_err(out[b], want).max() <= 1e-12, (m.N, mb, st, b)
+
+
+def test_dependency_timeout_fails_request_then_server_recovers(models):
+    """The test hook withholds one work item of stage 5 (step 1, stage 1); the items
+    of stage 6 wait for it until the 0.2 s limit runs out.  The request fails with
+    SWE_ERR_TIMEOUT, the server counts the failure, and a clean request submitted
+    afterwards completes and matches the oracle."""
+    m3 = models[3]
+    srv = capi.Server(1 << 30)
+    try:
+        g = srv.add_grid(m3)
+        srv.set_dep_limit(0.2)
+        srv.test_withhold(-1, 5)            # armed for the next submission
+        bad = srv.submit(g, _states(m3, 1, 3), 6)
+        with pytest.raises(capi.SweError, match="dependency wait") as e:
+            srv.wait([bad], timeout=60.0)
+        assert e.value.status == 6
+        assert srv.stats()["dependency_failures"] == 1
+        H0 = _states(m3, 2, 9)
+        good = srv.submit(g, H0, 12)
+        res = srv.wait([good], timeout=60.0)
+        assert res[good][0] == 1
+        out = srv.fetch(good)
+    finally:
+        srv.stop()
+    port = oracle.Port(m3, "fp64")
+    for b in range(2):
+        assert rel_err(out[b], port.run(H0[b], 12)).max() <= 1e-12

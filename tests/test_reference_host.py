@@ -1,5 +1,5 @@
-"""The reference's own main program, built with the SWE_USE_CUDA switch of
-INTEGRATION.md (oracle/patch_main.py, `make -C oracle host`), on its shipped
+"""The reference's own main program, built with a SWE_USE_CUDA switch beside its
+SWE_USE_OCL one (oracle/patch_main.py, `make -C oracle host`), on its shipped
 N=2562 input: 100 RK4 steps per attempt and the reference's own verify_output
 against H_100 (main.c:439-477, FP64 tolerance 1e-9).
 
