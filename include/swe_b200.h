@@ -336,6 +336,19 @@ int swe_cuda_step_noalloc(int fsize, int n, int nnbr, double gh0, double dt, con
  * idx is [n][nnbr], 0-based, self first. */
 int swe_host_rcm_mapping(int n, int nnbr, const int* idx, int* mapping);
 
+/* Reverse Cuthill-McKee-style order computed on the current device, for callers
+ * that need a bandwidth-reducing order fast (serving admission of new grids, large
+ * N): breadth-first from node 0 one level at a time, in parallel within a level;
+ * each level sorted by (position of the node's first parent in the order, stencil
+ * slot); reversed at the end.  It replaces the ordering step of rcm_mapping
+ * (swe_code/rcm/rcm.c:9-62) but not its exact permutation: the reference sorts each
+ * node's children by their count of still-unmapped neighbours, a sequential
+ * dependency.  Its bandwidth, as print_max_bandwidth (rcm.c:68-96) measures it, is
+ * of the same size.  mapping[new] = old; idx [n][nnbr] host array, 0-based, self
+ * first; needs 0 < n < 2^24 and breadth-first levels of at most 16384 nodes
+ * (SWE_ERR_ARG otherwise, or for a disconnected stencil graph). */
+int swe_dev_rcm_mapping(int n, int nnbr, const int* idx, int* mapping);
+
 /* Number of kernels this library has launched since load (all forms). */
 long long swe_b200_kernel_launches(void);
 

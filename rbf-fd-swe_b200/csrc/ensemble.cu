@@ -387,6 +387,10 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
         set_error("swe_ens_init: null array");
         return SWE_ERR_ARG;
     }
+    if ((double)n * 4 * members >= 4294967296.0) {
+        set_error("swe_ens_init: %d nodes x %d members exceed the 2^32 state values a stage indexes", n, members);
+        return SWE_ERR_ARG;
+    }
     for (long e = 0; e < (long)n * nnbr; ++e)
         if (idx[e] < 0 || idx[e] >= n) { set_error("swe_ens_init: idx[%ld] = %d out of range", e, idx[e]); return SWE_ERR_INDEX; }
     Ensemble& E = g_ens;
@@ -408,17 +412,29 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     for (int i = 0; i < n; ++i) inv[E.perm_h[i]] = i;
     for (long i = 0; i < n; ++i)
         for (int j = 0; j < nnbr; ++j) ridx[i * nnbr + j] = inv[idx[(long)E.perm_h[i] * nnbr + j]];
-    // static data in FP32, curve order; operator row sums in FP64 of the FP32 weights
-    std::vector<float> w((size_t)n * 32 * 4, 0.f), pt((size_t)n * kPointStride, 0.f), rs((size_t)n * 4);
+    // Static data in FP32, curve order.  The operator row sums that add the centre
+    // back (c * sum_k W) are summed from the FP64 weights: the weights themselves are
+    // rounded to FP32, which moves each row sum by up to 2^-24 sum_k |W|, and a row sum
+    // taken from the rounded weights would add that error times the full state value
+    // c at every node and stage.  With the FP64 sums only the centred part sum_k W (X -
+    // c), which is small, sees the rounded weights; the operators' annihilation of
+    // constants holds to FP64 accuracy (the h error of the batched form after 1000
+    // steps drops several-fold).
+    // W covers whole tiles: the nodes past n in the last tile have zero weights (their
+    // rows of the tile map name no stencil slot, so the A converters read slot 32)
+    const size_t wnodes = (size_t)(n + kEnsTileNodes - 1) / kEnsTileNodes * kEnsTileNodes;
+    std::vector<float> w(wnodes * kEnsSlots * 4, 0.f), pt((size_t)n * kPointStride, 0.f), rs((size_t)n * 4);
     std::vector<double> X((size_t)n * 3);
     for (long i = 0; i < n; ++i) {
         const long o = E.perm_h[i];
         double sum[4] = {0, 0, 0, 0};
         for (int j = 0; j < nnbr; ++j) {
-            float* q = &w[((size_t)i * 32 + j) * 4];
-            q[0] = (float)Dx[o * nnbr + j]; q[1] = (float)Dy[o * nnbr + j];
-            q[2] = (float)Dz[o * nnbr + j]; q[3] = (float)L[o * nnbr + j];
-            for (int op = 0; op < 4; ++op) sum[op] += (double)q[op];
+            float* q = &w[((size_t)i * kEnsSlots + j) * 4];
+            const double wd[4] = {Dx[o * nnbr + j], Dy[o * nnbr + j], Dz[o * nnbr + j], L[o * nnbr + j]};
+            for (int op = 0; op < 4; ++op) {
+                q[op] = (float)wd[op];
+                sum[op] += wd[op];
+            }
         }
         for (int op = 0; op < 4; ++op) rs[i * 4 + op] = (float)sum[op];
         float* r = &pt[(size_t)i * kPointStride];
@@ -431,7 +447,6 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
         X[3 * i] = x[o]; X[3 * i + 1] = y[o]; X[3 * i + 2] = z[o];
     }
     const TileTables tb = build_tiles(n, nnbr, ridx, X);
-
     E.ntiles = tb.ntiles;
     E.max_rows = tb.max_rows;
     SWE_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));

@@ -25,15 +25,26 @@ _ROW_FIELDS = ("x", "y", "z", "f", "ghm", "p_u", "p_v", "p_w", "gradghm", "Dx", 
                "H_init", "H_100")
 
 
-def rcm_mapping(model: SweModel) -> np.ndarray:
-    """mapping[new] = old, identical to the reference's rcm_mapping."""
+def rcm_mapping(model: SweModel, device: bool = False) -> np.ndarray:
+    """mapping[new] = old.  device=False: identical to the reference's rcm_mapping (the
+    library's host restatement).  device=True: the breadth-first level order built on
+    the GPU (swe_dev_rcm_mapping), of the same bandwidth but not the same permutation."""
     lib = capi.load()
-    lib.swe_host_rcm_mapping.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    fn = lib.swe_dev_rcm_mapping if device else lib.swe_host_rcm_mapping
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     idx = np.ascontiguousarray(model.idx, dtype=np.int32)
     out = np.empty(model.N, dtype=np.int32)
-    capi.check("swe_host_rcm_mapping", lib.swe_host_rcm_mapping(model.N, model.Nnbr, idx.ctypes.data,
-                                                                 out.ctypes.data))
+    name = "swe_dev_rcm_mapping" if device else "swe_host_rcm_mapping"
+    capi.check(name, fn(model.N, model.Nnbr, idx.ctypes.data, out.ctypes.data))
     return out
+
+
+def bandwidth(idx: np.ndarray) -> tuple[int, float]:
+    """(max, mean) over nodes of max - min stencil index, as the reference's
+    print_max_bandwidth (rcm/rcm.c:68-96) reports it for a reordered idx."""
+    idx = np.asarray(idx)
+    bw = idx.max(1) - idx.min(1)
+    return int(bw.max()), float(bw.mean())
 
 
 def reorder(model: SweModel, mapping: np.ndarray) -> SweModel:
@@ -57,9 +68,12 @@ def pad(model: SweModel, simd_length: int) -> SweModel:
     return dataclasses.replace(model, N=Np, **kw)
 
 
-def prepare(model: SweModel, use_rcm: bool = True, simd_length: int = 32) -> tuple[SweModel, np.ndarray]:
+def prepare(model: SweModel, use_rcm: bool = True, simd_length: int = 32,
+            device_order: bool = False) -> tuple[SweModel, np.ndarray]:
     """The reference's host pipeline for one serial patch (main.c:107-140): optional
-    RCM, then padding.  Returns (patch model, mapping[new] = old over real nodes)."""
-    mapping = rcm_mapping(model) if use_rcm else np.arange(model.N, dtype=np.int32)
+    RCM, then padding.  Returns (patch model, mapping[new] = old over real nodes).
+    device_order=True orders by the GPU's breadth-first level order instead of the
+    reference's exact RCM permutation."""
+    mapping = rcm_mapping(model, device_order) if use_rcm else np.arange(model.N, dtype=np.int32)
     m = reorder(model, mapping) if use_rcm else model
     return pad(m, simd_length), mapping

@@ -92,3 +92,16 @@ def test_noalloc_argument_checks_fail_before_device_work():
     assert lib.swe_cuda_step_noalloc(4, 2 * limit + 2, 31, 0.0, 1.0, *dummy, 1, None) == 1
     assert lib.swe_cuda_step_noalloc(8, 100, 31, 0.0, 1.0, *([None] + dummy[1:]), 1, None) == 1
     assert b"null" in lib.swe_cuda_last_error()
+
+
+def test_device_order_argument_checks_fail_before_device_work():
+    lib = capi.load()
+    lib.swe_dev_rcm_mapping.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    idx = np.zeros((4, 3), dtype=np.int32)
+    out = np.zeros(4, dtype=np.int32)
+    assert lib.swe_dev_rcm_mapping(0, 3, idx.ctypes.data, out.ctypes.data) == 1
+    assert lib.swe_dev_rcm_mapping(4, 1, idx.ctypes.data, out.ctypes.data) == 1
+    assert lib.swe_dev_rcm_mapping(4, 3, None, out.ctypes.data) == 1
+    idx[2, 1] = 9
+    assert lib.swe_dev_rcm_mapping(4, 3, idx.ctypes.data, out.ctypes.data) == 5      # SWE_ERR_INDEX
+    assert b"outside" in lib.swe_cuda_last_error()

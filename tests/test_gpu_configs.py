@@ -89,8 +89,9 @@ def test_n40962_1000_steps_every_reference_layout(plain, rcm):
 @pytest.fixture(scope="module")
 def model_l8():
     _, d = generated_input(8, device="cuda")
+    assert d.N == 655362
+    # RCM order, padded to a multiple of 32 nodes by replicating the last one (layout.c)
     m, _ = layout.prepare(swe_input.to_model(d), use_rcm=True, simd_length=32)
-    assert m.N == 655362
     return m
 
 

@@ -127,3 +127,19 @@ def test_port_matches_reference_1000_steps_n40962():
     H = oracle.Port(pm, "fp64").run(pm.H_init, 1000)
     err = rel_err(H, H_ref)
     assert err.max() <= 1e-13, err
+
+
+def test_levelset_statement_bandwidth_matches_reference_rcm():
+    """The plain-Python statement of the device order, on the golden N=162 grid and a
+    generated N=2562 grid: a permutation whose bandwidth (rcm.c:68-96) is within 5 % of
+    the reference's RCM order (the library's host restatement, identical to rcm.c)."""
+    from conftest import generated_input
+    from levelset_order import levelset_mapping
+    from swe_b200 import layout
+
+    for m in (swe_input.load_model(GOLDEN_BIN), swe_input.to_model(generated_input(4)[1])):
+        ls = levelset_mapping(m.idx)
+        assert np.array_equal(np.sort(ls), np.arange(m.N))
+        bw_ls = layout.bandwidth(layout.reorder(m, ls).idx)
+        bw_ref = layout.bandwidth(layout.reorder(m, layout.rcm_mapping(m)).idx)
+        assert bw_ls[0] <= 1.05 * bw_ref[0] and bw_ls[1] <= 1.05 * bw_ref[1], (m.N, bw_ls, bw_ref)
