@@ -305,58 +305,42 @@ def plain_config(wl: str, desc: str, d, sha: str) -> dict:
 def cpu_baseline_sample(path: str, d, prec: str, target_s: float = 12.0):
     """The reference's own CPU code (oracle/_ref) on a bounded number of steps, on every
     CPU this process may use (affinity set and cgroup quota), and on one thread beside
-    it.  Rates are whole RK_substep loops (RHS and combine), 4 N steps / seconds; the
-    reference's own Eval_Rhs timer (profiling.c:118-126) gives eval_rhs_value."""
+    it.  Each sample runs in a process of its own (oracle/cpu_baseline.py) that holds
+    no GPU context or PyTorch thread pool, so the OpenMP team has the host cores to
+    itself.  Rates are whole RK_substep loops (RHS and combine), 4 N steps / seconds;
+    the reference's own Eval_Rhs timer (profiling.c:118-126) gives eval_rhs_value."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    from swe_b200 import swe_input
 
     cpu = oracle.usable_cpus()
     threads = int(os.environ.get("OMP_NUM_THREADS", cpu["threads"]))
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    os.environ.setdefault("OMP_PROC_BIND", "close")
-    os.environ.setdefault("OMP_SCHEDULE", "static")
+    script = os.path.join(ROOT, "oracle", "cpu_baseline.py")
 
-    def sized(run_one, budget):
-        t1 = run_one(1)[0]                        # warm-up step, also sizes the sample
-        steps = max(1, min(200, int(budget / max(t1, 1e-4))))
-        t, t_rhs = run_one(steps)
-        return steps, t, t_rhs
+    def sample(nthreads: int, budget: float) -> dict:
+        env = dict(os.environ, OMP_NUM_THREADS=str(nthreads), OMP_SCHEDULE="static")
+        env.setdefault("OMP_PROC_BIND", "close")
+        out = subprocess.run([sys.executable, script, path, prec, str(budget)], env=env, capture_output=True,
+                             text=True, timeout=max(120.0, 20 * budget))
+        if out.returncode != 0:
+            raise RuntimeError(f"cpu_baseline.py failed: {out.stderr[-300:]}")
+        return json.loads(out.stdout.strip().splitlines()[-1])
 
-    if oracle.reference_available(prec, "cfdl"):
-        ref = oracle.Ref(path, prec, "cfdl", use_rcm=1)
-        H0 = ref.H_init()
-
-        def run_one(k):
-            _, t, t_rhs = ref.run(H0, k)
-            return t, t_rhs
-        kind, what = "reference", "the reference's RK_substep (CFDL, RCM)"
-    else:
-        m = swe_input.to_model(d)
-        port = oracle.Port(m, prec)
-
-        def run_one(k):
-            t0 = time.perf_counter()
-            port.run(m.H_init, k)
-            t = time.perf_counter() - t0
-            return t, None
-        kind, what = "port", "the oracle's C restatement"
-    oracle.set_thread_count(threads)
-    steps, t, t_rhs = sized(run_one, target_s)
-    oracle.set_thread_count(1)
-    steps1, t1, _ = sized(run_one, target_s / 3)
-    oracle.set_thread_count(threads)
-    rate = 4.0 * d.N * steps / t
-    one = 4.0 * d.N * steps1 / t1
-    return {"value": rate, "unit": "node-stage updates/s", "cores": threads, "kind": kind,
-            "sample": f"{steps} RK4 steps of {what}, OpenMP on {threads} threads, on N={d.N} "
-                      f"(one-thread figure: {steps1} steps)",
-            "seconds": round(t, 3),
-            "eval_rhs_value": (4.0 * d.N * steps / t_rhs) if t_rhs else None,
-            "one_thread_value": one, "speedup_vs_one_thread": rate / one,
+    full = sample(threads, target_s)
+    one = sample(1, target_s / 3)
+    rate = 4.0 * d.N * full["steps"] / full["seconds"]
+    one_rate = 4.0 * d.N * one["steps"] / one["seconds"]
+    what = "the reference's RK_substep (CFDL, RCM)" if full["kind"] == "reference" else "the oracle's C restatement"
+    return {"value": rate, "unit": "node-stage updates/s", "cores": threads, "kind": full["kind"],
+            "sample": f"{full['steps']} RK4 steps of {what}, OpenMP on {threads} threads, on N={d.N}, in a process "
+                      f"of its own (one-thread figure: {one['steps']} steps)",
+            "seconds": round(full["seconds"], 3),
+            "eval_rhs_value": (4.0 * d.N * full["steps"] / full["eval_rhs_seconds"]) if full["eval_rhs_seconds"]
+            else None,
+            "one_thread_value": one_rate, "speedup_vs_one_thread": rate / one_rate,
             "cpu": {"model": cpu["model"], "threads_used": threads, "affinity_cpus": cpu["affinity"],
                     "cgroup_quota_cpus": cpu["cgroup_quota_cpus"], "os_cpu_count": cpu["cpu_count"],
-                    "omp": {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OMP_PROC_BIND", "OMP_SCHEDULE")}}}
+                    "omp": {"OMP_NUM_THREADS": str(threads), "OMP_PROC_BIND": os.environ.get("OMP_PROC_BIND", "close"),
+                            "OMP_SCHEDULE": "static"}}}
 
 
 def run_reference(args, level, prec, wl, desc):
@@ -595,7 +579,7 @@ def run_ensemble(args, desc):
 
 def run_serving(args, desc):
     """Seeded Poisson stream of forecast requests through the serving form."""
-    from swe_b200 import capi, gen, swe_input
+    from swe_b200 import capi, gen, layout, swe_input
 
     rank, local, world = world_info()
     import torch
@@ -605,10 +589,18 @@ def run_serving(args, desc):
     levels = [4, 5, 6, 7]
     models = {}
     t0 = time.time()
+    order_s = {}
     for lv in levels:
         d = gen.generate(lv, seed=1, device=f"cuda:{local}")
-        models[lv] = swe_input.to_model(d)
-    log(f"[bench] serving grids generated in {time.time() - t0:.1f}s")
+        m = swe_input.to_model(d)
+        if args.serve_order == "device":
+            # registered in the device's breadth-first level order (bandwidth-reducing, like
+            # the reference's RCM), which keeps each work item's gathers local
+            t1 = time.time()
+            m = layout.reorder(m, layout.rcm_mapping(m, device=True))
+            order_s[lv] = time.time() - t1
+        models[lv] = m
+    log(f"[bench] serving grids generated in {time.time() - t0:.1f}s (ordering {order_s})")
     srv = capi.Server(args.budget_gb * 1e9, max_requests=512)
     capi.check("swe_cuda_select_device", srv.lib.swe_cuda_select_device(local))
     gids = {lv: srv.add_grid(models[lv]) for lv in levels}
@@ -649,7 +641,9 @@ def run_serving(args, desc):
             "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded request stream",
             "config": {"workload": args.workload, "description": desc, "requests": nreq,
-                       "arrival_rate_per_s": args.rate, "seed": args.seed, "budget_bytes": args.budget_gb * 1e9},
+                       "arrival_rate_per_s": args.rate, "seed": args.seed, "budget_bytes": args.budget_gb * 1e9,
+                       "grid_order": args.serve_order},
+            "grid_order_seconds": order_s,
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max())},
             "admission_wait_s": {"p50": float(np.percentile(wait_admit, 50)),
@@ -680,6 +674,8 @@ def main():
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--budget-gb", type=float, default=80.0)
+    ap.add_argument("--serve-order", default="device", choices=["device", "natural"],
+                    help="node order the serving grids are registered in")
     ap.add_argument("--plain-kernel", default="auto", choices=sorted(PLAIN_KERNELS),
                     help="plain stage kernel: auto = the one swe_cuda_init timed fastest; the others pin a kernel "
                          "and shape (for profiling runs, where the init-time timing is not representative)")

@@ -10,13 +10,6 @@
 //           (|x - hi - lo| <= 2^-17 |x|), one k-step of K = 16 per chunk;
 //           half the shared-memory bytes of Tf32x3 and twice the tensor rate.
 //
-// Two kinds of converter threads fill a chunk:
-//   * B threads (4 * MPC of them) gather the chunk's neighbour rows of the
-//     member-fields they own, centre and split them into the state operand;
-//   * A threads (kEnsAThreads) gather the weights of the chunk's rows through
-//     the per-tile map of chunk rows to stencil slots and split them into the
-//     weight operand.
-//
 // Padding rows of a tile's neighbour list name the tile's centring node, so their
 // centred values are exactly zero (their weights are zero as well).
 //
@@ -36,8 +29,6 @@ namespace swe {
 
 constexpr int kEnsTileNodes = 32;   // nodes per tile (M = 4 operators x 32 nodes)
 constexpr int kEnsKc = 16;          // neighbour rows per pipeline chunk
-constexpr int kEnsSlots = 33;       // weight slots per node: 32 stencil slots + a zero one
-constexpr int kEnsAThreads = 128;   // A (weight) converter threads
 
 enum EnsPrecision { kTf32x3 = 0, kBf16x3 = 1 };
 
@@ -57,68 +48,82 @@ __device__ __forceinline__ uint32_t bf16x2_split(float a, float b, uint32_t& lo)
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// Stencil slot of chunk row i from a map word (4 rows per word, 255 = not in the
-// stencil).  The zero slot stands for "not in the stencil", so every row's weights
-// are one unconditional load.
-__device__ __forceinline__ uint32_t slot_of(uint32_t word, int i) {
-    return min((word >> (8 * i)) & 0xffu, (uint32_t)(kEnsSlots - 1));
-}
-
 template <int MPC, int PREC>
 struct Operands;
 
 // --------------------------------------------------------------------------------------
-// 3xTF32.  B thread: member-fields 4q..4q+3 of rows 4kg..4kg+3.  A thread: node t, rows
-// 4akg..4akg+3, all four operators.
+// 3xTF32.  B thread: member-fields 4q..4q+3 of rows 4kg..4kg+3; A thread: node t, rows
+// 4akg..4akg+3, operator pairs opp0 .. opp0 + kOpp - 1.
 // --------------------------------------------------------------------------------------
 template <int MPC>
 struct Operands<MPC, kTf32x3> {
     static constexpr int kN = 4 * MPC;
-    static constexpr int kBThreads = 4 * MPC;
+    static constexpr int kConvThreads = 4 * MPC;
+    static constexpr int kOpp = 256 / kConvThreads;
     static constexpr int kSboA = (kEnsKc / 4) * 128;
     static constexpr int kSboB = (kEnsKc / 4) * 128 + 16;
     static constexpr int kAHalf = (128 / 8) * kSboA;
     static constexpr int kBHalf = (kN / 8) * kSboB;
     static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
     static constexpr int kStages = 3;
+    static_assert(kOpp == 1 || kOpp == 2, "A build covers 32 nodes x 4 row groups x 2 operator pairs");
 
-    struct BThread {
-        int quad, kg;
-        __device__ explicit BThread(int ct) : quad(ct % MPC), kg(ct / MPC) {}
+    struct Thread {
+        int quad, kg, at, akg, opp0;
+        __device__ explicit Thread(int ct)
+            : quad(ct % MPC), kg(ct / MPC), at(ct & 31), akg((ct >> 5) & 3), opp0((ct >> 7) * kOpp) {}
         __device__ int col() const { return 4 * quad; }
     };
-    struct BFetch {
+    struct Fetch {
         int4 idx = make_int4(-1, -1, -1, -1);
-    };
-    struct BSet {
-        float4 x[4];          // 4 gathered rows x 4 member-fields
-        float4 cen;           // centre state of the same member-fields
-    };
-    struct AThread {
-        int at, akg;
-        __device__ explicit AThread(int ct) : at(ct & 31), akg(ct >> 5) {}
-    };
-    struct AFetch {
         uint32_t jj = 0xffffffffu;
     };
-    struct ASet {
-        float4 w[4];          // (Dx, Dy, Dz, L) of the 4 chunk rows
+    struct Set {
+        float4 x[4];          // 4 gathered rows x 4 member-fields
+        float4 cen;           // centre state of the same member-fields
+        float2 w[kOpp][4];    // weights of the operator pairs for the 4 chunk rows
     };
 
-    __device__ static void fetch_bidx(const int* rows, int gc, const BThread& th, BFetch& f) {
+    __device__ static void fetch_idx(const int* rows, const uint32_t* jmap, int gc, const Thread& th, Fetch& f) {
         f.idx = __ldg(reinterpret_cast<const int4*>(rows + gc * kEnsKc + 4 * th.kg));
+        f.jj = __ldg(jmap + (gc * 4 + th.akg) * 32 + th.at);
     }
-    __device__ static void fetch_b(const float* Kin, int mf, unsigned col, const float* cen_row, const BFetch& f,
-                                   BSet& o, const BSet& prev) {
+    __device__ static void fetch_ops(const float* Kin, int mf, long col, const float4* W, long node, const float* cen_row,
+                                     const Thread& th, const Fetch& f, Set& o, const Set& prev) {
         const int r[4] = {f.idx.x, f.idx.y, f.idx.z, f.idx.w};
 #pragma unroll
-        for (int i = 0; i < 4; ++i) o.x[i] = ldg_f4(Kin + ((unsigned)r[i] * (unsigned)mf + col));
+        for (int i = 0; i < 4; ++i) o.x[i] = ldg_f4(Kin + (long)r[i] * mf + col);
         o.cen = cen_row ? ldg_f4(cen_row + col) : prev.cen;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t j = (f.jj >> (8 * i)) & 0xffu;
+#pragma unroll
+            for (int q = 0; q < kOpp; ++q)
+                o.w[q][i] = j != 0xffu ? __ldg(reinterpret_cast<const float2*>(W + node * 32 + j) + th.opp0 + q)
+                                       : make_float2(0.f, 0.f);
+        }
     }
-    __device__ static void build_b(unsigned char* slot, const BThread& th, const BSet& o) {
+    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o) {
+        unsigned char* A_hi = slot;
+        unsigned char* A_lo = slot + kAHalf;
         unsigned char* B_hi = slot + 2 * kAHalf;
         unsigned char* B_lo = B_hi + kBHalf;
-        // each member-field's 4 rows are one 16-byte core row
+        // A: one 16-byte core row (4 chunk rows) of (operator, node) per operator handled
+#pragma unroll
+        for (int q = 0; q < kOpp; ++q)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = 32 * (2 * (th.opp0 + q) + h) + th.at;
+                float4 hi, lo;
+                tc::tf32_split_lo_fp32(h ? o.w[q][0].y : o.w[q][0].x, hi.x, lo.x);
+                tc::tf32_split_lo_fp32(h ? o.w[q][1].y : o.w[q][1].x, hi.y, lo.y);
+                tc::tf32_split_lo_fp32(h ? o.w[q][2].y : o.w[q][2].x, hi.z, lo.z);
+                tc::tf32_split_lo_fp32(h ? o.w[q][3].y : o.w[q][3].x, hi.w, lo.w);
+                const uint32_t off = (r >> 3) * kSboA + th.akg * 128 + (r & 7) * 16;
+                *reinterpret_cast<float4*>(A_hi + off) = hi;
+                *reinterpret_cast<float4*>(A_lo + off) = lo;
+            }
+        // B: each member-field's 4 rows are one 16-byte core row
         const float xv[4][4] = {{o.x[0].x, o.x[0].y, o.x[0].z, o.x[0].w},
                                 {o.x[1].x, o.x[1].y, o.x[1].z, o.x[1].w},
                                 {o.x[2].x, o.x[2].y, o.x[2].z, o.x[2].w},
@@ -140,36 +145,6 @@ struct Operands<MPC, kTf32x3> {
             *reinterpret_cast<float4*>(B_lo + off) = lo;
         }
     }
-    __device__ static void fetch_aidx(const uint32_t* jmap, int gc, const AThread& th, AFetch& f) {
-        f.jj = __ldg(jmap + (gc * 4 + th.akg) * 32 + th.at);
-    }
-    // W: [node][33 slots] of (Dx, Dy, Dz, L); slot 32 is zero.
-    __device__ static void fetch_a(const float4* W, unsigned node, const AThread&, const AFetch& f, ASet& o) {
-        const float4* wn = W + node * (unsigned)kEnsSlots;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) o.w[i] = __ldg(wn + slot_of(f.jj, i));
-    }
-    __device__ static void build_a(unsigned char* slot, const AThread& th, const ASet& o) {
-        unsigned char* A_hi = slot;
-        unsigned char* A_lo = slot + kAHalf;
-        // one 16-byte core row (4 chunk rows) of (operator, node) per operator
-        const float wv[4][4] = {{o.w[0].x, o.w[0].y, o.w[0].z, o.w[0].w},
-                                {o.w[1].x, o.w[1].y, o.w[1].z, o.w[1].w},
-                                {o.w[2].x, o.w[2].y, o.w[2].z, o.w[2].w},
-                                {o.w[3].x, o.w[3].y, o.w[3].z, o.w[3].w}};
-#pragma unroll
-        for (int op = 0; op < 4; ++op) {
-            const int r = 32 * op + th.at;
-            float4 hi, lo;
-            tc::tf32_split_lo_fp32(wv[0][op], hi.x, lo.x);
-            tc::tf32_split_lo_fp32(wv[1][op], hi.y, lo.y);
-            tc::tf32_split_lo_fp32(wv[2][op], hi.z, lo.z);
-            tc::tf32_split_lo_fp32(wv[3][op], hi.w, lo.w);
-            const uint32_t off = (r >> 3) * kSboA + th.akg * 128 + (r & 7) * 16;
-            *reinterpret_cast<float4*>(A_hi + off) = hi;
-            *reinterpret_cast<float4*>(A_lo + off) = lo;
-        }
-    }
     // The chunk's products A_hi B_hi + A_hi B_lo + A_lo B_hi into accumulator d.
     __device__ static void issue(uint32_t slot, uint32_t d, bool first) {
         constexpr uint32_t idesc = tc::idesc_tf32(128, kN);
@@ -188,60 +163,90 @@ struct Operands<MPC, kTf32x3> {
 };
 
 // --------------------------------------------------------------------------------------
-// split BF16.  B thread: member-fields 2p, 2p+1 of rows 8kh..8kh+7.  A thread: node t,
-// rows 8akh..8akh+7, operators 2 opp and 2 opp + 1.
+// split BF16.  B thread: member-fields 2p, 2p+1 of rows 8kh..8kh+7; A thread: node t,
+// rows 8akh..8akh+7, operators op0 .. op0 + kOps - 1.
 // --------------------------------------------------------------------------------------
 template <int MPC>
 struct Operands<MPC, kBf16x3> {
     static constexpr int kN = 4 * MPC;
-    static constexpr int kBThreads = 4 * MPC;
+    static constexpr int kConvThreads = 4 * MPC;
+    static constexpr int kOps = 256 / kConvThreads;
     static constexpr int kSboA = (kEnsKc / 8) * 128;
     static constexpr int kSboB = (kEnsKc / 8) * 128 + 16;
     static constexpr int kAHalf = (128 / 8) * kSboA;
     static constexpr int kBHalf = (kN / 8) * kSboB;
     static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
     static constexpr int kStages = 5;
+    static_assert(kOps == 1 || kOps == 2, "A build covers 32 nodes x 2 row halves x 4 operators");
 
-    struct BThread {
-        int p, kh;
-        __device__ explicit BThread(int ct) : p(ct % (kN / 2)), kh(ct / (kN / 2)) {}
+    struct Thread {
+        int p, kh, at, akh, op0;
+        __device__ explicit Thread(int ct)
+            : p(ct % (kN / 2)), kh(ct / (kN / 2)), at(ct & 31), akh((ct >> 5) & 1), op0((ct >> 6) * kOps) {}
         __device__ int col() const { return 2 * p; }
     };
-    struct BFetch {
+    struct Fetch {
         int4 idx[2] = {make_int4(-1, -1, -1, -1), make_int4(-1, -1, -1, -1)};
-    };
-    struct BSet {
-        float2 x[8];          // 8 gathered rows x 2 member-fields
-        float2 cen;
-    };
-    struct AThread {
-        int at, akh, opp;
-        __device__ explicit AThread(int ct) : at(ct & 31), akh((ct >> 5) & 1), opp(ct >> 6) {}
-    };
-    struct AFetch {
         uint32_t jj[2] = {0xffffffffu, 0xffffffffu};
     };
-    struct ASet {
-        float2 w[8];          // operators 2 opp, 2 opp + 1 of the 8 chunk rows
+    // weights of the thread's operators for the 8 chunk rows: one operator, or the pair op0, op0 + 1
+    using WT = typename std::conditional<kOps == 1, float, float2>::type;
+    struct Set {
+        float2 x[8];          // 8 gathered rows x 2 member-fields
+        float2 cen;
+        WT w[8];
     };
 
-    __device__ static void fetch_bidx(const int* rows, int gc, const BThread& th, BFetch& f) {
+    __device__ static void fetch_idx(const int* rows, const uint32_t* jmap, int gc, const Thread& th, Fetch& f) {
         const int4* r = reinterpret_cast<const int4*>(rows + gc * kEnsKc + 8 * th.kh);
         f.idx[0] = __ldg(r);
         f.idx[1] = __ldg(r + 1);
+        f.jj[0] = __ldg(jmap + (gc * 4 + 2 * th.akh) * 32 + th.at);
+        f.jj[1] = __ldg(jmap + (gc * 4 + 2 * th.akh + 1) * 32 + th.at);
     }
-    __device__ static void fetch_b(const float* Kin, int mf, unsigned col, const float* cen_row, const BFetch& f,
-                                   BSet& o, const BSet& prev) {
+    __device__ static void fetch_ops(const float* Kin, int mf, long col, const float4* W, long node, const float* cen_row,
+                                     const Thread& th, const Fetch& f, Set& o, const Set& prev) {
         const int r[8] = {f.idx[0].x, f.idx[0].y, f.idx[0].z, f.idx[0].w,
                           f.idx[1].x, f.idx[1].y, f.idx[1].z, f.idx[1].w};
 #pragma unroll
-        for (int i = 0; i < 8; ++i) o.x[i] = ldg_f2(Kin + ((unsigned)r[i] * (unsigned)mf + col));
+        for (int i = 0; i < 8; ++i) o.x[i] = ldg_f2(Kin + (long)r[i] * mf + col);
         o.cen = cen_row ? ldg_f2(cen_row + col) : prev.cen;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t j = (f.jj[i >> 2] >> (8 * (i & 3))) & 0xffu;
+            if constexpr (kOps == 1)
+                o.w[i] = j != 0xffu ? __ldg(reinterpret_cast<const float*>(W + node * 32 + j) + th.op0) : 0.f;
+            else
+                o.w[i] = j != 0xffu ? __ldg(reinterpret_cast<const float2*>(W + node * 32 + j) + (th.op0 >> 1))
+                                    : make_float2(0.f, 0.f);
+        }
     }
-    __device__ static void build_b(unsigned char* slot, const BThread& th, const BSet& o) {
+    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o) {
+        unsigned char* A_hi = slot;
+        unsigned char* A_lo = slot + kAHalf;
         unsigned char* B_hi = slot + 2 * kAHalf;
         unsigned char* B_lo = B_hi + kBHalf;
-        // each member-field's 8 rows are one 16-byte core row
+        // A: one 16-byte core row (8 chunk rows) of (operator, node) per operator handled
+#pragma unroll
+        for (int q = 0; q < kOps; ++q) {
+            const int op = th.op0 + q;
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if constexpr (kOps == 1) v[i] = o.w[i];
+                else v[i] = (op & 1) ? o.w[i].y : o.w[i].x;
+            }
+            uint4 hi, lo;
+            hi.x = bf16x2_split(v[0], v[1], lo.x);
+            hi.y = bf16x2_split(v[2], v[3], lo.y);
+            hi.z = bf16x2_split(v[4], v[5], lo.z);
+            hi.w = bf16x2_split(v[6], v[7], lo.w);
+            const int r = 32 * op + th.at;
+            const uint32_t off = (r >> 3) * kSboA + th.akh * 128 + (r & 7) * 16;
+            *reinterpret_cast<uint4*>(A_hi + off) = hi;
+            *reinterpret_cast<uint4*>(A_lo + off) = lo;
+        }
+        // B: each member-field's 8 rows are one 16-byte core row
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const float c = j ? o.cen.y : o.cen.x;
@@ -257,38 +262,6 @@ struct Operands<MPC, kBf16x3> {
             const uint32_t off = (nrow >> 3) * kSboB + th.kh * 128 + (nrow & 7) * 16;
             *reinterpret_cast<uint4*>(B_hi + off) = hi;
             *reinterpret_cast<uint4*>(B_lo + off) = lo;
-        }
-    }
-    __device__ static void fetch_aidx(const uint32_t* jmap, int gc, const AThread& th, AFetch& f) {
-        f.jj[0] = __ldg(jmap + (gc * 4 + 2 * th.akh) * 32 + th.at);
-        f.jj[1] = __ldg(jmap + (gc * 4 + 2 * th.akh + 1) * 32 + th.at);
-    }
-    // W: [node][33 slots] of (Dx, Dy, Dz, L); slot 32 is zero.  The thread's operator
-    // pair is the float2 2 opp / 2 + {0, 1} of a slot's float4.
-    __device__ static void fetch_a(const float4* W, unsigned node, const AThread& th, const AFetch& f, ASet& o) {
-        const float2* wn = reinterpret_cast<const float2*>(W + node * (unsigned)kEnsSlots) + th.opp;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) o.w[i] = __ldg(wn + 2 * slot_of(f.jj[i >> 2], i & 3));
-    }
-    __device__ static void build_a(unsigned char* slot, const AThread& th, const ASet& o) {
-        unsigned char* A_hi = slot;
-        unsigned char* A_lo = slot + kAHalf;
-        // one 16-byte core row (8 chunk rows) of (operator, node) per operator
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int op = 2 * th.opp + h;
-            float v[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = h ? o.w[i].y : o.w[i].x;
-            uint4 hi, lo;
-            hi.x = bf16x2_split(v[0], v[1], lo.x);
-            hi.y = bf16x2_split(v[2], v[3], lo.y);
-            hi.z = bf16x2_split(v[4], v[5], lo.z);
-            hi.w = bf16x2_split(v[6], v[7], lo.w);
-            const int r = 32 * op + th.at;
-            const uint32_t off = (r >> 3) * kSboA + th.akh * 128 + (r & 7) * 16;
-            *reinterpret_cast<uint4*>(A_hi + off) = hi;
-            *reinterpret_cast<uint4*>(A_lo + off) = lo;
         }
     }
     __device__ static void issue(uint32_t slot, uint32_t d, bool first) {

@@ -420,16 +420,13 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     // c), which is small, sees the rounded weights; the operators' annihilation of
     // constants holds to FP64 accuracy (the h error of the batched form after 1000
     // steps drops several-fold).
-    // W covers whole tiles: the nodes past n in the last tile have zero weights (their
-    // rows of the tile map name no stencil slot, so the A converters read slot 32)
-    const size_t wnodes = (size_t)(n + kEnsTileNodes - 1) / kEnsTileNodes * kEnsTileNodes;
-    std::vector<float> w(wnodes * kEnsSlots * 4, 0.f), pt((size_t)n * kPointStride, 0.f), rs((size_t)n * 4);
+    std::vector<float> w((size_t)n * 32 * 4, 0.f), pt((size_t)n * kPointStride, 0.f), rs((size_t)n * 4);
     std::vector<double> X((size_t)n * 3);
     for (long i = 0; i < n; ++i) {
         const long o = E.perm_h[i];
         double sum[4] = {0, 0, 0, 0};
         for (int j = 0; j < nnbr; ++j) {
-            float* q = &w[((size_t)i * kEnsSlots + j) * 4];
+            float* q = &w[((size_t)i * 32 + j) * 4];
             const double wd[4] = {Dx[o * nnbr + j], Dy[o * nnbr + j], Dz[o * nnbr + j], L[o * nnbr + j]};
             for (int op = 0; op < 4; ++op) {
                 q[op] = (float)wd[op];

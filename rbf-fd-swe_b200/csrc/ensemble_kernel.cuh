@@ -59,13 +59,11 @@ template <int MPC, int PREC>
 struct EnsCfg {
     using Op = ens::Operands<MPC, PREC>;
     static constexpr int kN = 4 * MPC;                     // MMA N: member-fields per CTA
-    static constexpr int kBWarps = MPC / 8;                // 4 * MPC state (B) converter threads
-    static constexpr int kAWarps = kEnsAThreads / 32;      // weight (A) converters; the first issues the MMAs
-    static constexpr int kAWarp0 = kBWarps;
-    static constexpr int kMmaWarp = kAWarp0;
-    static constexpr int kConvWarps = kBWarps + kAWarps;
-    static constexpr int kEpiWarp0 = kConvWarps;
-    static constexpr int kThreads = 32 * (kConvWarps + kEnsEpiWarps);
+    static constexpr int kConvWarps = MPC / 8;             // 4 * MPC converter threads
+    static constexpr int kConvThreads = 32 * kConvWarps;
+    static constexpr int kMmaWarp = kConvWarps;
+    static constexpr int kEpiWarp0 = kConvWarps + 1;
+    static constexpr int kThreads = 32 * (kConvWarps + 1 + kEnsEpiWarps);
     static constexpr int kStages = Op::kStages;            // ring slots
     static constexpr int kStageBytes = Op::kStageBytes;
     static constexpr int kXchStride = 36;                  // floats per (op, node) row; 9 x 16 B
@@ -75,8 +73,7 @@ struct EnsCfg {
     static constexpr int kTileBuf = (kTbCen + kN * 4 + 127) / 128 * 128;
     static constexpr int kSmem = kStages * kStageBytes + 2 * kXchGroupFloats * 4 + 2 * kTileBuf;
     static constexpr int kTmemCols = (2 * kN <= 256) ? 256 : 512;
-    static_assert(32 * kBWarps == Op::kBThreads, "state converter thread count");
-    static_assert(kEpiWarp0 % 4 == 0, "epilogue warps start on a TMEM lane quarter");
+    static_assert(kConvThreads == Op::kConvThreads, "converter thread count");
     static_assert(kN % 64 == 0, "epilogue column chunks");
 };
 
@@ -89,7 +86,7 @@ struct EnsArgs {
     const int* row_off;    // [ntiles + 1] offsets into rows, multiples of kEnsKc
     const int* rows;       // unique neighbour rows of each tile, ascending; padded with the centring node
     const uint32_t* jmap;  // [chunk][row group][node t]: stencil slot of each of the 4 rows, 255 = none
-    const float4* W;       // [n][33] (Dx, Dy, Dz, L) per stencil slot; slot 32 (and any slot >= nnbr) zero
+    const float4* W;       // [n][32] (Dx, Dy, Dz, L) per stencil slot
     const int* centre;     // [ntiles] node whose state centres the tile
     const float4* PT;      // [n][5] pointwise record (20 floats)
     const float4* RS;      // [n] row sums of the four operators
@@ -182,10 +179,10 @@ __device__ __forceinline__ Cursor next_cursor(Cursor p, const EnsArgs& a, int ha
     return p;
 }
 
-// Streamed operands of one epilogue chunk: one node, two adjacent members per thread.
+// Streamed operands of one epilogue chunk (two (node, member) pairs per thread).
 struct EpiSet {
     float4 own[2], h32[2], d32[2];
-    double2 hh, dh;
+    double hh[2], dh[2];
 };
 
 }  // namespace ens
@@ -226,30 +223,30 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
     tc::fence_after_sync();
     const uint32_t tmem = tmem_s;
 
-    if (warp < C::kBWarps) {
-        // ========================= state (B) converters =========================
-        const typename Op::BThread th(threadIdx.x);
+    if (warp < C::kConvWarps) {
+        // =============================== converters ===============================
+        const typename Op::Thread th(threadIdx.x);
         ens::Cursor cur = ens::first_cursor(a, halves);
-        typename Op::BFetch fx;        // indices of the step after the current one
-        typename Op::BSet sa, sb;      // operands of the current / next step (ping-pong)
-        auto fetch_ops = [&](const ens::Cursor& p, const typename Op::BFetch& f, typename Op::BSet& o,
-                             const typename Op::BSet& prev, int u_prev) {
+        typename Op::Fetch fx;         // indices of the step after the current one
+        typename Op::Set sa, sb;       // operands of the current / next step (ping-pong)
+        auto fetch_ops = [&](const ens::Cursor& p, const typename Op::Fetch& f, typename Op::Set& o,
+                             const typename Op::Set& prev, int u_prev) {
             if (!p.valid) return;
             const int tile = p.u / halves;
-            const unsigned col = (unsigned)((p.u % halves) * C::kN + th.col());
-            const float* cen_row = p.u != u_prev ? a.Kin + (size_t)__ldg(a.centre + tile) * a.mf : nullptr;
-            Op::fetch_b(a.Kin, a.mf, col, cen_row, f, o, prev);
+            const long col = (long)(p.u % halves) * C::kN + th.col();
+            const float* cen_row = p.u != u_prev ? a.Kin + (long)__ldg(a.centre + tile) * a.mf : nullptr;
+            Op::fetch_ops(a.Kin, a.mf, col, a.W, (long)tile * kEnsTileNodes + th.at, cen_row, th, f, o, prev);
         };
         int g = 0;
-        auto step = [&](typename Op::BSet& o, typename Op::BSet& nx, int u_cur) -> bool {
+        auto step = [&](typename Op::Set& o, typename Op::Set& nx, int u_cur) -> bool {
             // look ahead: operands of the next step, indices of the one after
             ens::Cursor nxt = ens::next_cursor(cur, a, halves);
             fetch_ops(nxt, fx, nx, o, u_cur);
             ens::Cursor nxt2 = ens::next_cursor(nxt, a, halves);
-            if (nxt2.valid) Op::fetch_bidx(a.rows, nxt2.gc, th, fx);
+            if (nxt2.valid) Op::fetch_idx(a.rows, a.jmap, nxt2.gc, th, fx);
             const int s = g % C::kStages;
             if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) return false;
-            Op::build_b(smem + s * C::kStageBytes, th, o);
+            Op::build(smem + s * C::kStageBytes, th, o);
             tc::fence_async_smem();
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&full_bar[s]);
@@ -258,11 +255,11 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
             return true;
         };
         if (cur.valid) {
-            typename Op::BFetch f0;
-            Op::fetch_bidx(a.rows, cur.gc, th, f0);
+            typename Op::Fetch f0;
+            Op::fetch_idx(a.rows, a.jmap, cur.gc, th, f0);
             fetch_ops(cur, f0, sa, sa, -1);
             const ens::Cursor n1 = ens::next_cursor(cur, a, halves);
-            if (n1.valid) Op::fetch_bidx(a.rows, n1.gc, th, fx);
+            if (n1.valid) Op::fetch_idx(a.rows, a.jmap, n1.gc, th, fx);
         }
         // two steps per trip so that the ping-pong sets never need copying
         while (cur.valid) {
@@ -272,72 +269,28 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
             u = cur.u;
             if (!step(sb, sa, u)) break;
         }
-    } else if (warp < C::kConvWarps) {
-        // ====================== weight (A) converters + MMA issuer ======================
-        // Lane 0 of the first A warp also issues each chunk's products once every
-        // converter has filled the slot (the A warps have the lighter share of the
-        // work, so this one can wait for the slot without holding anything up).
-        const typename Op::AThread th(threadIdx.x - 32 * C::kAWarp0);
-        const bool issuer = warp == C::kMmaWarp && lane == 0;
-        ens::Cursor cur = ens::first_cursor(a, halves);
-        typename Op::AFetch fx;
-        typename Op::ASet sa, sb;
-        auto fetch_ops = [&](const ens::Cursor& p, const typename Op::AFetch& f, typename Op::ASet& o) {
-            if (!p.valid) return;
-            Op::fetch_a(a.W, (unsigned)((p.u / halves) * kEnsTileNodes + th.at), th, f, o);
-        };
-        int g = 0, it = 0;
-        bool ok = true;
-        auto step = [&](typename Op::ASet& o, typename Op::ASet& nx) -> bool {
-            ens::Cursor nxt = ens::next_cursor(cur, a, halves);
-            fetch_ops(nxt, fx, nx);
-            ens::Cursor nxt2 = ens::next_cursor(nxt, a, halves);
-            if (nxt2.valid) Op::fetch_aidx(a.jmap, nxt2.gc, th, fx);
-            const int s = g % C::kStages;
-            if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) return false;
-            Op::build_a(smem + s * C::kStageBytes, th, o);
-            tc::fence_async_smem();
-            __syncwarp();
-            if (lane == 0) ens::mbar_arrive(&full_bar[s]);
-            if (issuer) {
+    } else if (warp == C::kMmaWarp) {
+        // =============================== MMA issuer ===============================
+        if (lane == 0) {
+            int g = 0, it = 0;
+            bool ok = true;
+            for (int u = blockIdx.x; u < a.units && ok; u += gridDim.x, ++it) {
                 const int ab = it & 1;
-                const bool first = cur.gc == cur.gc0;
-                bool good = true;
-                if (first) {
-                    good = ens::wait(&acce_bar[ab], ((it >> 1) & 1) ^ 1, abort_v, a.err, 4);
+                if (!ens::wait(&acce_bar[ab], ((it >> 1) & 1) ^ 1, abort_v, a.err, 4)) { ok = false; break; }
+                tc::fence_after_sync();
+                const int tile = u / halves;
+                const int gc0 = __ldg(a.row_off + tile) / kEnsKc, gc1 = __ldg(a.row_off + tile + 1) / kEnsKc;
+                const uint32_t d = tmem + ab * C::kN;
+                for (int gc = gc0; gc < gc1; ++gc, ++g) {
+                    const int s = g % C::kStages;
+                    if (!ens::wait(&full_bar[s], (g / C::kStages) & 1, abort_v, a.err, 5)) { ok = false; break; }
                     tc::fence_after_sync();
-                }
-                if (good) good = ens::wait(&full_bar[s], (g / C::kStages) & 1, abort_v, a.err, 5);
-                if (good) {
-                    tc::fence_after_sync();
-                    Op::issue(tc::smem_u32(smem + s * C::kStageBytes), tmem + ab * C::kN, first);
+                    Op::issue(tc::smem_u32(smem + s * C::kStageBytes), d, gc == gc0);
                     tc::mma_commit(&empty_bar[s]);
-                    if (cur.gc + 1 == cur.gc_end) {
-                        tc::mma_commit(&accf_bar[ab]);
-                        ++it;
-                    }
                 }
-                ok = good;
+                if (!ok) break;
+                tc::mma_commit(&accf_bar[ab]);
             }
-            __syncwarp();
-            if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) return false;
-            ++g;
-            cur = nxt;
-            return true;
-        };
-        if (cur.valid) {
-            typename Op::AFetch f0;
-            Op::fetch_aidx(a.jmap, cur.gc, th, f0);
-            fetch_ops(cur, f0, sa);
-            const ens::Cursor n1 = ens::next_cursor(cur, a, halves);
-            if (n1.valid) Op::fetch_aidx(a.jmap, n1.gc, th, fx);
-        }
-        while (cur.valid) {
-            if (!step(sa, sb)) break;
-            if (!cur.valid) break;
-            if (!step(sb, sa)) break;
-        }
-        if (issuer) {
             // every MMA this thread issued has completed before tensor memory is freed
             // (this wait ignores the abort flag: it only ends when they have)
             tc::mma_commit(&fin_bar);
@@ -370,29 +323,26 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
             tc::bulk_g2s(tb + C::kTbCen, a.Kin + (long)__ldg(a.centre + tile) * a.mf + (u % halves) * C::kN,
                          C::kN * 4, &tile_bar[b]);
         };
-        // This thread's pairs in every chunk: node t = gt / 4 of the tile and the two
-        // adjacent members 2 (gt % 4), 2 (gt % 4) + 1 of the chunk's 8, so that the node's
-        // pointwise record and row sums are read once for both, and the FP64 h operands of
-        // the two members are one 16-byte access.
-        const int et_t = gt >> 2, et_bm = 2 * (gt & 3);
         // streamed per-(node, member) operands of one chunk for this thread's two pairs
         auto fetch = [&](int u, int ch, ens::EpiSet& o) {
             if (u >= a.units) return;
             const int tile = u / halves;
-            const int node = tile * kEnsTileNodes + et_t;
-            if (node >= a.n) return;
-            const int mfb = (u % halves) * C::kN + ch * 32 + 4 * et_bm;
-            const unsigned e4 = (unsigned)node * (unsigned)a.mf + (unsigned)mfb;
-            const unsigned eh = (unsigned)node * (unsigned)members + (unsigned)(mfb >> 2);
-            o.own[0] = ens::ldg_f4(a.Kin + e4);
-            o.own[1] = ens::ldg_f4(a.Kin + e4 + 4);
-            if (MODE != kEvalOnly) o.hh = __ldg(reinterpret_cast<const double2*>(a.Hh + eh));
-            if (kHD) {
-                o.h32[0] = ens::ldg_f4(a.H32 + e4);
-                o.h32[1] = ens::ldg_f4(a.H32 + e4 + 4);
-                o.d32[0] = ens::ldg_f4(a.D32 + e4);
-                o.d32[1] = ens::ldg_f4(a.D32 + e4 + 4);
-                o.dh = __ldg(reinterpret_cast<const double2*>(a.Dh + eh));
+            const int col0 = (u % halves) * C::kN;
+#pragma unroll
+            for (int pi = 0; pi < 2; ++pi) {
+                const int pr = gt + 128 * pi;
+                const long node = (long)tile * kEnsTileNodes + (pr >> 3);
+                if (node >= a.n) continue;
+                const int mfb = col0 + ch * 32 + 4 * (pr & 7);
+                const long e4 = node * a.mf + mfb;
+                const long eh = node * members + (mfb >> 2);
+                o.own[pi] = ens::ldg_f4(a.Kin + e4);
+                if (MODE != kEvalOnly) o.hh[pi] = __ldg(a.Hh + eh);
+                if (kHD) {
+                    o.h32[pi] = ens::ldg_f4(a.H32 + e4);
+                    o.d32[pi] = ens::ldg_f4(a.D32 + e4);
+                    o.dh[pi] = __ldg(a.Dh + eh);
+                }
             }
         };
         // one 32-column chunk: accumulator -> exchange -> (node, member) epilogue
@@ -416,79 +366,70 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
                 }
             }
             ens::named_sync(2 + grp, 128);
-            const int t = et_t;
-            const int node = tile * kEnsTileNodes + t;
-            if (node < a.n) {
-                const int mfb = col0 + ch * 32 + 4 * et_bm;      // first mf of the first member
-                const unsigned e4 = (unsigned)node * (unsigned)a.mf + (unsigned)mfb;
-                const unsigned eh = (unsigned)node * (unsigned)members + (unsigned)(mfb >> 2);
-                // the node's pointwise record and operator row sums, shared by both pairs
+#pragma unroll
+            for (int pi = 0; pi < 2; ++pi) {
+                const int pr = gt + 128 * pi;
+                const int t = pr >> 3, bm = pr & 7;
+                const long node = (long)tile * kEnsTileNodes + t;
+                if (node >= a.n) continue;
+                const int mfb = col0 + ch * 32 + 4 * bm;      // first mf of this member
+                const int member = mfb >> 2;
+                float S[16];
+#pragma unroll
+                for (int o2 = 0; o2 < 4; ++o2) {
+                    const float4 sv = *reinterpret_cast<const float4*>(xch + (o2 * 32 + t) * C::kXchStride + 4 * bm);
+                    S[4 * o2] = sv.x; S[4 * o2 + 1] = sv.y; S[4 * o2 + 2] = sv.z; S[4 * o2 + 3] = sv.w;
+                }
+                const float4 cen = *reinterpret_cast<const float4*>(tb + C::kTbCen / 4 + (mfb - col0));
+                const float4 rs4 = *reinterpret_cast<const float4*>(tb + C::kTbRs / 4 + 4 * t);
+                const float cf[4] = {cen.x, cen.y, cen.z, cen.w};
+                const float rs[4] = {rs4.x, rs4.y, rs4.z, rs4.w};
+#pragma unroll
+                for (int o2 = 0; o2 < 4; ++o2)
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) S[4 * o2 + f] = fmaf(cf[f], rs[o2], S[4 * o2 + f]);
+                const float q[4] = {o.own[pi].x, o.own[pi].y, o.own[pi].z, o.own[pi].w};
                 float pt[kPointStride];
 #pragma unroll
                 for (int pp = 0; pp < kPointStride / 4; ++pp) {
                     const float4 pv = *reinterpret_cast<const float4*>(tb + t * kPointStride + 4 * pp);
                     pt[4 * pp] = pv.x; pt[4 * pp + 1] = pv.y; pt[4 * pp + 2] = pv.z; pt[4 * pp + 3] = pv.w;
                 }
-                const float4 rs4 = *reinterpret_cast<const float4*>(tb + C::kTbRs / 4 + 4 * t);
-                const float rs[4] = {rs4.x, rs4.y, rs4.z, rs4.w};
-                const double hh2[2] = {o.hh.x, o.hh.y};
-                const double dh2[2] = {o.dh.x, o.dh.y};
-                double h_out[2], dh_out[2];
-#pragma unroll
-                for (int pi = 0; pi < 2; ++pi) {
-                    const int bm = et_bm + pi;
-                    float S[16];
-#pragma unroll
-                    for (int o2 = 0; o2 < 4; ++o2) {
-                        const float4 sv = *reinterpret_cast<const float4*>(xch + (o2 * 32 + t) * C::kXchStride + 4 * bm);
-                        S[4 * o2] = sv.x; S[4 * o2 + 1] = sv.y; S[4 * o2 + 2] = sv.z; S[4 * o2 + 3] = sv.w;
-                    }
-                    const float4 cen = *reinterpret_cast<const float4*>(tb + C::kTbCen / 4 + (mfb - col0) + 4 * pi);
-                    const float cf[4] = {cen.x, cen.y, cen.z, cen.w};
-#pragma unroll
-                    for (int o2 = 0; o2 < 4; ++o2)
-#pragma unroll
-                        for (int f = 0; f < 4; ++f) S[4 * o2 + f] = fmaf(cf[f], rs[o2], S[4 * o2 + f]);
-                    const float q[4] = {o.own[pi].x, o.own[pi].y, o.own[pi].z, o.own[pi].w};
-                    float F[4];
-                    pointwise_rhs<float>(S, q, pt, a.gh0, F);
-                    const unsigned e = e4 + 4 * pi;
-                    if (MODE == kEvalOnly) {
-                        *reinterpret_cast<float4*>(a.F + e) = make_float4(F[0], F[1], F[2], F[3]);
-                    } else if (MODE == kStage0) {
-                        // K = H + c F (q is the base state here); D = F
-                        const double fh = (double)F[3];
-                        *reinterpret_cast<float4*>(a.D32 + e) = make_float4(F[0], F[1], F[2], 0.f);
-                        dh_out[pi] = fh;
-                        *reinterpret_cast<float4*>(a.Kout + e) =
-                            make_float4(__fadd_rn(q[0], __fmul_rn(c32, F[0])), __fadd_rn(q[1], __fmul_rn(c32, F[1])),
-                                        __fadd_rn(q[2], __fmul_rn(c32, F[2])), __double2float_rn(hh2[pi] + a.c * fh));
-                    } else if (MODE == kStage1 || MODE == kStage2) {
-                        const double fh = (double)F[3];
-                        const float4 h4 = o.h32[pi], d4 = o.d32[pi];
-                        *reinterpret_cast<float4*>(a.D32 + e) =
-                            make_float4(__fadd_rn(d4.x, __fmul_rn(2.f, F[0])), __fadd_rn(d4.y, __fmul_rn(2.f, F[1])),
-                                        __fadd_rn(d4.z, __fmul_rn(2.f, F[2])), 0.f);
-                        dh_out[pi] = dh2[pi] + 2.0 * fh;
-                        *reinterpret_cast<float4*>(a.Kout + e) =
-                            make_float4(__fadd_rn(h4.x, __fmul_rn(c32, F[0])), __fadd_rn(h4.y, __fmul_rn(c32, F[1])),
-                                        __fadd_rn(h4.z, __fmul_rn(c32, F[2])), __double2float_rn(hh2[pi] + a.c * fh));
-                    } else {
-                        const float4 h4 = o.h32[pi], d4 = o.d32[pi];
-                        const float du = __fadd_rn(d4.x, F[0]), dv = __fadd_rn(d4.y, F[1]), dw = __fadd_rn(d4.z, F[2]);
-                        const double dh = dh2[pi] + (double)F[3];
-                        const double h = hh2[pi] + a.dt6 * dh;
-                        h_out[pi] = h;
-                        *reinterpret_cast<float4*>(a.H32 + e) =
-                            make_float4(__double2float_rn((double)h4.x + a.dt6 * (double)du),
-                                        __double2float_rn((double)h4.y + a.dt6 * (double)dv),
-                                        __double2float_rn((double)h4.z + a.dt6 * (double)dw), __double2float_rn(h));
-                    }
+                float F[4];
+                pointwise_rhs<float>(S, q, pt, a.gh0, F);
+                const long e4 = node * a.mf + mfb;
+                const long eh = node * members + member;
+                if (MODE == kEvalOnly) {
+                    *reinterpret_cast<float4*>(a.F + e4) = make_float4(F[0], F[1], F[2], F[3]);
+                } else if (MODE == kStage0) {
+                    // K = H + c F (q is the base state here); D = F
+                    const double fh = (double)F[3];
+                    *reinterpret_cast<float4*>(a.D32 + e4) = make_float4(F[0], F[1], F[2], 0.f);
+                    a.Dh[eh] = fh;
+                    *reinterpret_cast<float4*>(a.Kout + e4) =
+                        make_float4(__fadd_rn(q[0], __fmul_rn(c32, F[0])), __fadd_rn(q[1], __fmul_rn(c32, F[1])),
+                                    __fadd_rn(q[2], __fmul_rn(c32, F[2])), __double2float_rn(o.hh[pi] + a.c * fh));
+                } else if (MODE == kStage1 || MODE == kStage2) {
+                    const double fh = (double)F[3];
+                    const float4 h4 = o.h32[pi], d4 = o.d32[pi];
+                    *reinterpret_cast<float4*>(a.D32 + e4) =
+                        make_float4(__fadd_rn(d4.x, __fmul_rn(2.f, F[0])), __fadd_rn(d4.y, __fmul_rn(2.f, F[1])),
+                                    __fadd_rn(d4.z, __fmul_rn(2.f, F[2])), 0.f);
+                    a.Dh[eh] = o.dh[pi] + 2.0 * fh;
+                    *reinterpret_cast<float4*>(a.Kout + e4) =
+                        make_float4(__fadd_rn(h4.x, __fmul_rn(c32, F[0])), __fadd_rn(h4.y, __fmul_rn(c32, F[1])),
+                                    __fadd_rn(h4.z, __fmul_rn(c32, F[2])), __double2float_rn(o.hh[pi] + a.c * fh));
+                } else {
+                    const float4 h4 = o.h32[pi], d4 = o.d32[pi];
+                    const float du = __fadd_rn(d4.x, F[0]), dv = __fadd_rn(d4.y, F[1]), dw = __fadd_rn(d4.z, F[2]);
+                    const double dh = o.dh[pi] + (double)F[3];
+                    const double h = o.hh[pi] + a.dt6 * dh;
+                    a.Hh[eh] = h;
+                    *reinterpret_cast<float4*>(a.H32 + e4) =
+                        make_float4(__double2float_rn((double)h4.x + a.dt6 * (double)du),
+                                    __double2float_rn((double)h4.y + a.dt6 * (double)dv),
+                                    __double2float_rn((double)h4.z + a.dt6 * (double)dw), __double2float_rn(h));
                 }
-                if (MODE == kStage0 || MODE == kStage1 || MODE == kStage2)
-                    *reinterpret_cast<double2*>(a.Dh + eh) = make_double2(dh_out[0], dh_out[1]);
-                else if (MODE == kStage3)
-                    *reinterpret_cast<double2*>(a.Hh + eh) = make_double2(h_out[0], h_out[1]);
             }
             ens::named_sync(2 + grp, 128);
         };
