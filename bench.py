@@ -531,7 +531,9 @@ def ensemble_target(wl: str, local: int, steps: int, warmup: int, flush, world: 
     return {"workload": wl, "description": desc, "value": member_steps, "unit": "member-steps/s",
             "steps": steps, "ms_per_step": 1e3 * t_total / steps,
             "dtype": f"{precision} (fp32 state, fp64 h accumulation)", "members": members,
-            "kernel_variant": cfg, "tune_ms_per_step": tune_ms,
+            "kernel_variant": cfg,
+            "tune_ms_per_step": {f"tile{t}_mpc{mp}": (v if v > 0 else None)
+                                 for (t, mp), v in zip(capi.Ensemble.TUNE_VARIANTS, tune_ms)},
             "plain_fp64_member_steps_per_s": plain_rate, "ratio_vs_plain_fp64": member_steps / plain_rate,
             "h_err_vs_fp64": {"steps": err_steps, "members": len(err_idx),
                               "reference": "plain FP64 GPU run of the same member (itself within 1e-12 of the "

@@ -223,15 +223,16 @@ int swe_ens_eval_rhs(const double* K, double* F);
  * kernels); swe_ens_stage runs one stage, same semantics as RK_substep. */
 int swe_ens_step(int nsteps);
 int swe_ens_stage(int substep_id);
-/* Autotuner: times one RK4 step of every kernel variant (32 or 64 members per
- * CTA; tiles are 32 nodes) in the current precision on the live state,
- * restores the state and keeps the fastest.  ms_per_step[4] (may be NULL)
- * receives the timings ({32, 64} members per CTA, then two unused slots), -1
+/* Autotuner: times one RK4 step of every kernel variant -- tile shape (32-node
+ * tiles, M = 128, or 16-node tiles, M = 64; 3xTF32 only) x members per CTA (64
+ * or 32) -- in the current precision on the live state, restores the state and
+ * keeps the fastest.  ms_per_step[4] (may be NULL) receives the timings in the
+ * order (tile, members per CTA) = (32, 64), (32, 32), (16, 64), (16, 32), -1
  * where a variant does not apply.  config[5] = {tile nodes, members per CTA,
  * largest neighbour set of a tile, tiles, precision}. */
 int swe_ens_tune(double* ms_per_step);
 int swe_ens_config(int* config);
-/* Forces one variant (tile_nodes 32, members_per_cta 32 or 64). */
+/* Forces one variant (tile_nodes 32 or 16, members_per_cta 64 or 32). */
 int swe_ens_use_variant(int tile_nodes, int members_per_cta);
 /* Precision of the stencil products: 0 = 3xTF32 (default; hi and lo parts both
  * exact TF32, |x - hi - lo| <= 2^-22 |x|), 1 = split BF16 (2^-17), both with

@@ -27,7 +27,7 @@
 
 namespace swe {
 
-constexpr int kEnsTileNodes = 32;   // nodes per tile (M = 4 operators x 32 nodes)
+constexpr int kEnsTileNodes = 32;   // nodes per tile of the default shape (M = 4 operators x 32 nodes)
 constexpr int kEnsKc = 16;          // neighbour rows per pipeline chunk
 
 enum EnsPrecision { kTf32x3 = 0, kBf16x3 = 1 };
@@ -48,30 +48,35 @@ __device__ __forceinline__ uint32_t bf16x2_split(float a, float b, uint32_t& lo)
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-template <int MPC, int PREC>
+template <int T, int MPC, int PREC>
 struct Operands;
 
 // --------------------------------------------------------------------------------------
-// 3xTF32.  B thread: member-fields 4q..4q+3 of rows 4kg..4kg+3; A thread: node t, rows
-// 4akg..4akg+3, operator pairs opp0 .. opp0 + kOpp - 1.
+// 3xTF32, tiles of T = 32 or 16 nodes (M = 4T = 128 or 64).  B thread: member-fields
+// 4q..4q+3 of rows 4kg..4kg+3.  A thread: node t, rows 4akg..4akg+3, operators
+// op0 .. op0 + kOps - 1 (kOps = 16 T / converter threads: 1, 2 or 4).
 // --------------------------------------------------------------------------------------
-template <int MPC>
-struct Operands<MPC, kTf32x3> {
+template <int T, int MPC>
+struct Operands<T, MPC, kTf32x3> {
     static constexpr int kN = 4 * MPC;
+    static constexpr int kM = 4 * T;
     static constexpr int kConvThreads = 4 * MPC;
-    static constexpr int kOpp = 256 / kConvThreads;
+    static constexpr int kOps = 16 * T / kConvThreads;
     static constexpr int kSboA = (kEnsKc / 4) * 128;
     static constexpr int kSboB = (kEnsKc / 4) * 128 + 16;
-    static constexpr int kAHalf = (128 / 8) * kSboA;
+    static constexpr int kAHalf = (kM / 8) * kSboA;
     static constexpr int kBHalf = (kN / 8) * kSboB;
     static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
     static constexpr int kStages = 3;
-    static_assert(kOpp == 1 || kOpp == 2, "A build covers 32 nodes x 4 row groups x 2 operator pairs");
+    static_assert(T == 16 || T == 32, "tiles of 16 or 32 nodes");
+    static_assert(kOps == 1 || kOps == 2 || kOps == 4, "A build: T nodes x 4 row groups x 4 operators");
+    // the weights of the thread's operators: one, a pair or all four of (Dx, Dy, Dz, L)
+    using WT = typename std::conditional<kOps == 1, float, typename std::conditional<kOps == 2, float2, float4>::type>::type;
 
     struct Thread {
-        int quad, kg, at, akg, opp0;
+        int quad, kg, at, akg, op0;
         __device__ explicit Thread(int ct)
-            : quad(ct % MPC), kg(ct / MPC), at(ct & 31), akg((ct >> 5) & 3), opp0((ct >> 7) * kOpp) {}
+            : quad(ct % MPC), kg(ct / MPC), at(ct % T), akg((ct / T) & 3), op0((ct / (4 * T)) * kOps) {}
         __device__ int col() const { return 4 * quad; }
     };
     struct Fetch {
@@ -81,12 +86,18 @@ struct Operands<MPC, kTf32x3> {
     struct Set {
         float4 x[4];          // 4 gathered rows x 4 member-fields
         float4 cen;           // centre state of the same member-fields
-        float2 w[kOpp][4];    // weights of the operator pairs for the 4 chunk rows
+        WT w[4];              // weights of the thread's operators for the 4 chunk rows
     };
+
+    __device__ static float wget(const WT& w, int q) {
+        if constexpr (kOps == 1) return w;
+        else if constexpr (kOps == 2) return q ? w.y : w.x;
+        else return q == 0 ? w.x : q == 1 ? w.y : q == 2 ? w.z : w.w;
+    }
 
     __device__ static void fetch_idx(const int* rows, const uint32_t* jmap, int gc, const Thread& th, Fetch& f) {
         f.idx = __ldg(reinterpret_cast<const int4*>(rows + gc * kEnsKc + 4 * th.kg));
-        f.jj = __ldg(jmap + (gc * 4 + th.akg) * 32 + th.at);
+        f.jj = __ldg(jmap + (gc * 4 + th.akg) * T + th.at);
     }
     __device__ static void fetch_ops(const float* Kin, int mf, long col, const float4* W, long node, const float* cen_row,
                                      const Thread& th, const Fetch& f, Set& o, const Set& prev) {
@@ -97,10 +108,12 @@ struct Operands<MPC, kTf32x3> {
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const uint32_t j = (f.jj >> (8 * i)) & 0xffu;
-#pragma unroll
-            for (int q = 0; q < kOpp; ++q)
-                o.w[q][i] = j != 0xffu ? __ldg(reinterpret_cast<const float2*>(W + node * 32 + j) + th.opp0 + q)
-                                       : make_float2(0.f, 0.f);
+            if constexpr (kOps == 4) {
+                o.w[i] = j != 0xffu ? __ldg(W + node * 32 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                const WT* wp = reinterpret_cast<const WT*>(W + node * 32 + j) + th.op0 / kOps;
+                o.w[i] = j != 0xffu ? __ldg(wp) : WT{};
+            }
         }
     }
     __device__ static void build(unsigned char* slot, const Thread& th, const Set& o) {
@@ -110,19 +123,17 @@ struct Operands<MPC, kTf32x3> {
         unsigned char* B_lo = B_hi + kBHalf;
         // A: one 16-byte core row (4 chunk rows) of (operator, node) per operator handled
 #pragma unroll
-        for (int q = 0; q < kOpp; ++q)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = 32 * (2 * (th.opp0 + q) + h) + th.at;
-                float4 hi, lo;
-                tc::tf32_split_lo_fp32(h ? o.w[q][0].y : o.w[q][0].x, hi.x, lo.x);
-                tc::tf32_split_lo_fp32(h ? o.w[q][1].y : o.w[q][1].x, hi.y, lo.y);
-                tc::tf32_split_lo_fp32(h ? o.w[q][2].y : o.w[q][2].x, hi.z, lo.z);
-                tc::tf32_split_lo_fp32(h ? o.w[q][3].y : o.w[q][3].x, hi.w, lo.w);
-                const uint32_t off = (r >> 3) * kSboA + th.akg * 128 + (r & 7) * 16;
-                *reinterpret_cast<float4*>(A_hi + off) = hi;
-                *reinterpret_cast<float4*>(A_lo + off) = lo;
-            }
+        for (int q = 0; q < kOps; ++q) {
+            const int r = T * (th.op0 + q) + th.at;
+            float4 hi, lo;
+            tc::tf32_split_lo_fp32(wget(o.w[0], q), hi.x, lo.x);
+            tc::tf32_split_lo_fp32(wget(o.w[1], q), hi.y, lo.y);
+            tc::tf32_split_lo_fp32(wget(o.w[2], q), hi.z, lo.z);
+            tc::tf32_split_lo_fp32(wget(o.w[3], q), hi.w, lo.w);
+            const uint32_t off = (r >> 3) * kSboA + th.akg * 128 + (r & 7) * 16;
+            *reinterpret_cast<float4*>(A_hi + off) = hi;
+            *reinterpret_cast<float4*>(A_lo + off) = lo;
+        }
         // B: each member-field's 4 rows are one 16-byte core row
         const float xv[4][4] = {{o.x[0].x, o.x[0].y, o.x[0].z, o.x[0].w},
                                 {o.x[1].x, o.x[1].y, o.x[1].z, o.x[1].w},
@@ -147,7 +158,7 @@ struct Operands<MPC, kTf32x3> {
     }
     // The chunk's products A_hi B_hi + A_hi B_lo + A_lo B_hi into accumulator d.
     __device__ static void issue(uint32_t slot, uint32_t d, bool first) {
-        constexpr uint32_t idesc = tc::idesc_tf32(128, kN);
+        constexpr uint32_t idesc = tc::idesc_tf32(kM, kN);
         const uint32_t a_hi = slot, a_lo = slot + kAHalf, b_hi = slot + 2 * kAHalf, b_lo = b_hi + kBHalf;
 #pragma unroll
         for (int ks = 0; ks < kEnsKc / 8; ++ks) {
@@ -163,11 +174,11 @@ struct Operands<MPC, kTf32x3> {
 };
 
 // --------------------------------------------------------------------------------------
-// split BF16.  B thread: member-fields 2p, 2p+1 of rows 8kh..8kh+7; A thread: node t,
-// rows 8akh..8akh+7, operators op0 .. op0 + kOps - 1.
+// split BF16, tiles of 32 nodes.  B thread: member-fields 2p, 2p+1 of rows 8kh..8kh+7;
+// A thread: node t, rows 8akh..8akh+7, operators op0 .. op0 + kOps - 1.
 // --------------------------------------------------------------------------------------
 template <int MPC>
-struct Operands<MPC, kBf16x3> {
+struct Operands<32, MPC, kBf16x3> {
     static constexpr int kN = 4 * MPC;
     static constexpr int kConvThreads = 4 * MPC;
     static constexpr int kOps = 256 / kConvThreads;

@@ -77,15 +77,15 @@ struct TileTables {
     std::vector<uint32_t> jmap;   // [chunk][row group][node t] 4 stencil slots (255 = none)
 };
 
-TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std::vector<double>& X) {
+TileTables build_tiles(int T, int n, int nnbr, const std::vector<int>& ridx, const std::vector<double>& X) {
     TileTables tb;
-    tb.ntiles = (n + kEnsTileNodes - 1) / kEnsTileNodes;
+    tb.ntiles = (n + T - 1) / T;
     tb.row_off.assign(tb.ntiles + 1, 0);
     tb.centre.assign(tb.ntiles, 0);
     std::vector<int> u;
     std::vector<uint8_t> slot;   // [t][k] stencil slot of row k in node t's stencil
     for (int tile = 0; tile < tb.ntiles; ++tile) {
-        const int n0 = tile * kEnsTileNodes, n1 = std::min(n, n0 + kEnsTileNodes);
+        const int n0 = tile * T, n1 = std::min(n, n0 + T);
         u.clear();
         for (int i = n0; i < n1; ++i)
             for (int j = 0; j < nnbr; ++j) u.push_back(ridx[(size_t)i * nnbr + j]);
@@ -98,7 +98,7 @@ TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std:
         const size_t pad0 = tb.rows.size() + u.size();
         for (int k = 0; k < kpad; ++k) tb.rows.push_back(k < (int)u.size() ? u[k] : -1);
         tb.row_off[tile + 1] = (int)tb.rows.size();
-        slot.assign((size_t)kEnsTileNodes * kpad, 0xff);
+        slot.assign((size_t)T * kpad, 0xff);
         for (int i = n0; i < n1; ++i)
             for (int j = 0; j < nnbr; ++j) {
                 const int k = (int)(std::lower_bound(u.begin(), u.end(), ridx[(size_t)i * nnbr + j]) - u.begin());
@@ -106,7 +106,7 @@ TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std:
             }
         for (int c = 0; c < nch; ++c)
             for (int g = 0; g < 4; ++g)
-                for (int t = 0; t < kEnsTileNodes; ++t) {
+                for (int t = 0; t < T; ++t) {
                     uint32_t v = 0;
                     for (int i = 0; i < 4; ++i) v |= (uint32_t)slot[(size_t)t * kpad + c * kEnsKc + 4 * g + i] << (8 * i);
                     tb.jmap.push_back(v);
@@ -127,10 +127,22 @@ TileTables build_tiles(int n, int nnbr, const std::vector<int>& ridx, const std:
     return tb;
 }
 
+// A kernel variant: tile shape (nodes per tile) and members per CTA.
 struct Variant {
+    int tile = 32;
     int mpc = 32;
     bool usable = false;
 };
+
+// Device copies of one tile shape's tables.
+struct DevTables {
+    int ntiles = 0, max_rows = 0;
+    int *row_off = nullptr, *rows = nullptr, *centre = nullptr;
+    uint32_t* jmap = nullptr;
+};
+constexpr int kEnsShapes = 2;          // tiles of 32 and 16 nodes
+constexpr int kEnsShapeNodes[kEnsShapes] = {32, 16};
+constexpr int kEnsVariants = 4;        // (32, 64), (32, 32), (16, 64), (16, 32)
 
 __global__ void ens_invariants_kernel(const float* __restrict__ H32, const double* __restrict__ Hh,
                                       const float4* __restrict__ PT, int n, int members, double gh0,
@@ -194,12 +206,10 @@ struct Ensemble {
     float* bkH32 = nullptr;
     double* bkHh = nullptr;
     int* err = nullptr;
-    // tile tables
-    int ntiles = 0, max_rows = 0;
-    int *row_off = nullptr, *rows = nullptr, *centre = nullptr;
-    uint32_t* jmap = nullptr;
+    // tile tables, one set per tile shape (32 and 16 nodes)
+    DevTables tabs[kEnsShapes];
     float4* W = nullptr;
-    Variant var[2];       // members per CTA: 32, 64
+    Variant var[kEnsVariants];   // (tile nodes, members per CTA): (32, 64), (32, 32), (16, 64), (16, 32)
     int chosen = -1;
     int prec = kTf32x3;
     cudaStream_t stream = nullptr;
@@ -207,37 +217,42 @@ struct Ensemble {
     bool timing = false;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     bool timed = false;
-    double tune_ms[2] = {-1, -1};
+    double tune_ms[kEnsVariants] = {-1, -1, -1, -1};
+
+    static int shape_of(int tile) { return tile == 32 ? 0 : 1; }
 
     void release() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
-        void* ps[] = {perm, PT, RS, H32, D32, Ka, Kb, F, Kx, Hh, Dh, io, inv, bkH32, bkHh, err,
-                      row_off, rows, centre, jmap, W};
+        void* ps[] = {perm, PT, RS, H32, D32, Ka, Kb, F, Kx, Hh, Dh, io, inv, bkH32, bkHh, err, W};
         for (void* p : ps) if (p) cudaFree(p);
+        for (DevTables& t : tabs) {
+            void* tp[] = {t.row_off, t.rows, t.centre, t.jmap};
+            for (void* p : tp) if (p) cudaFree(p);
+            t = DevTables{};
+        }
         perm = nullptr; PT = nullptr; RS = nullptr; H32 = D32 = Ka = Kb = F = Kx = nullptr;
         Hh = Dh = io = inv = nullptr; bkH32 = nullptr; bkHh = nullptr; err = nullptr;
-        row_off = rows = centre = nullptr;
-        jmap = nullptr;
         W = nullptr;
         for (auto& v : var) v = Variant{};
         for (auto& e : ev) { if (e) cudaEventDestroy(e); e = nullptr; }
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
         chosen = -1;
-        tune_ms[0] = tune_ms[1] = -1;
+        for (double& t : tune_ms) t = -1;
         ready = false;
     }
 
-    EnsArgs args(int mode, int mpc) const {
+    EnsArgs args(int mode, int tile, int mpc) const {
+        const DevTables& tb = tabs[shape_of(tile)];
         EnsArgs a{};
         a.n = n;
-        a.ntiles = ntiles;
+        a.ntiles = tb.ntiles;
         a.members = members;
-        a.units = ntiles * (members / mpc);
+        a.units = tb.ntiles * (members / mpc);
         a.mf = mf;
-        a.row_off = row_off; a.rows = rows; a.jmap = jmap; a.W = W;
-        a.centre = centre;
+        a.row_off = tb.row_off; a.rows = tb.rows; a.jmap = tb.jmap; a.W = W;
+        a.centre = tb.centre;
         a.PT = PT;
         a.RS = RS;
         a.H32 = H32; a.Hh = Hh; a.D32 = D32; a.Dh = Dh; a.F = F;
@@ -254,39 +269,46 @@ struct Ensemble {
         return a;
     }
 
-    template <int MPC, int PREC>
+    template <int T, int MPC, int PREC>
     void launch_v(int mode) {
-        using C = EnsCfg<MPC, PREC>;
-        const EnsArgs a = args(mode, MPC);
+        using C = EnsCfg<T, MPC, PREC>;
+        const EnsArgs a = args(mode, T, MPC);
         const int grid = std::min(a.units, nsm);
         switch (mode) {
-            case 0: ens_stage_kernel<MPC, kStage0, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
-            case 1: ens_stage_kernel<MPC, kStage1, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
-            case 2: ens_stage_kernel<MPC, kStage2, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
-            case 3: ens_stage_kernel<MPC, kStage3, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
-            default: ens_stage_kernel<MPC, kEvalOnly, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 0: ens_stage_kernel<T, MPC, kStage0, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 1: ens_stage_kernel<T, MPC, kStage1, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 2: ens_stage_kernel<T, MPC, kStage2, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            case 3: ens_stage_kernel<T, MPC, kStage3, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
+            default: ens_stage_kernel<T, MPC, kEvalOnly, PREC><<<grid, C::kThreads, C::kSmem, stream>>>(a); break;
         }
     }
 
+    // split BF16 has 32-node tiles only: usable() keeps it off the 16-node variants
+    bool usable(int vi) const { return var[vi].usable && (prec == kTf32x3 || var[vi].tile == 32); }
+
     void launch(int vi, int mode) {
+        const Variant& v = var[vi];
         if (prec == kBf16x3) {
-            if (var[vi].mpc == 64) launch_v<64, kBf16x3>(mode);
-            else launch_v<32, kBf16x3>(mode);
+            if (v.mpc == 64) launch_v<32, 64, kBf16x3>(mode);
+            else launch_v<32, 32, kBf16x3>(mode);
+        } else if (v.tile == 32) {
+            if (v.mpc == 64) launch_v<32, 64, kTf32x3>(mode);
+            else launch_v<32, 32, kTf32x3>(mode);
         } else {
-            if (var[vi].mpc == 64) launch_v<64, kTf32x3>(mode);
-            else launch_v<32, kTf32x3>(mode);
+            if (v.mpc == 64) launch_v<16, 64, kTf32x3>(mode);
+            else launch_v<16, 32, kTf32x3>(mode);
         }
         count_launch();
     }
 
-    template <int MPC, int PREC>
+    template <int T, int MPC, int PREC>
     static int set_attrs() {
-        const int sm = EnsCfg<MPC, PREC>::kSmem;
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage0, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage1, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage2, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kStage3, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<MPC, kEvalOnly, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        const int sm = EnsCfg<T, MPC, PREC>::kSmem;
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, MPC, kStage0, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, MPC, kStage1, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, MPC, kStage2, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, MPC, kStage3, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        SWE_CUDA_TRY(cudaFuncSetAttribute(ens_stage_kernel<T, MPC, kEvalOnly, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
         return SWE_OK;
     }
 
@@ -339,9 +361,9 @@ int tune(Ensemble& E) {
     SWE_CUDA_TRY(cudaEventCreate(&e1));
     float best = 1e30f;
     int best_i = -1;
-    for (int vi = 0; vi < 2; ++vi) {
+    for (int vi = 0; vi < kEnsVariants; ++vi) {
         E.tune_ms[vi] = -1.0;
-        if (!E.var[vi].usable) continue;
+        if (!E.usable(vi)) continue;
         for (int w = 0; w < 2; ++w)
             for (int s = 0; s < 4; ++s) E.launch(vi, s);
         SWE_CUDA_TRY(cudaEventRecord(e0, E.stream));
@@ -443,9 +465,8 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
         }
         X[3 * i] = x[o]; X[3 * i + 1] = y[o]; X[3 * i + 2] = z[o];
     }
-    const TileTables tb = build_tiles(n, nnbr, ridx, X);
-    E.ntiles = tb.ntiles;
-    E.max_rows = tb.max_rows;
+    TileTables tbs[kEnsShapes];
+    for (int sh = 0; sh < kEnsShapes; ++sh) tbs[sh] = build_tiles(kEnsShapeNodes[sh], n, nnbr, ridx, X);
     SWE_CUDA_TRY(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
     const size_t s32 = (size_t)n * E.mf * sizeof(float), s64 = (size_t)n * members * sizeof(double);
     auto upload = [](auto** dst, const auto& vec) -> int {
@@ -457,10 +478,15 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     SWE_TRY(upload(&E.perm, E.perm_h));
     SWE_TRY(upload(reinterpret_cast<float**>(&E.PT), pt));
     SWE_TRY(upload(reinterpret_cast<float**>(&E.RS), rs));
-    SWE_TRY(upload(&E.row_off, tb.row_off));
-    SWE_TRY(upload(&E.rows, tb.rows));
-    SWE_TRY(upload(&E.jmap, tb.jmap));
-    SWE_TRY(upload(&E.centre, tb.centre));
+    for (int sh = 0; sh < kEnsShapes; ++sh) {
+        DevTables& d = E.tabs[sh];
+        d.ntiles = tbs[sh].ntiles;
+        d.max_rows = tbs[sh].max_rows;
+        SWE_TRY(upload(&d.row_off, tbs[sh].row_off));
+        SWE_TRY(upload(&d.rows, tbs[sh].rows));
+        SWE_TRY(upload(&d.jmap, tbs[sh].jmap));
+        SWE_TRY(upload(&d.centre, tbs[sh].centre));
+    }
     SWE_TRY(upload(reinterpret_cast<float**>(&E.W), w));
     for (float** p : {&E.H32, &E.D32, &E.Ka, &E.Kb, &E.F, &E.Kx, &E.bkH32}) SWE_CUDA_TRY(cudaMalloc(p, s32));
     for (double** p : {&E.Hh, &E.Dh, &E.bkHh}) SWE_CUDA_TRY(cudaMalloc(p, s64));
@@ -470,18 +496,22 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     SWE_CUDA_TRY(cudaMemset(E.err, 0, sizeof(int)));
     for (float* p : {E.H32, E.D32, E.Ka, E.Kb, E.F, E.Kx}) SWE_CUDA_TRY(cudaMemset(p, 0, s32));
     for (double* p : {E.Hh, E.Dh}) SWE_CUDA_TRY(cudaMemset(p, 0, s64));
-    E.var[0].mpc = 32;
-    E.var[0].usable = true;
-    E.var[1].mpc = 64;
-    E.var[1].usable = members % 64 == 0;
-    SWE_TRY((Ensemble::set_attrs<32, kTf32x3>()));
-    SWE_TRY((Ensemble::set_attrs<64, kTf32x3>()));
-    SWE_TRY((Ensemble::set_attrs<32, kBf16x3>()));
-    SWE_TRY((Ensemble::set_attrs<64, kBf16x3>()));
+    const int shapes[kEnsVariants][2] = {{32, 64}, {32, 32}, {16, 64}, {16, 32}};
+    for (int vi = 0; vi < kEnsVariants; ++vi) {
+        E.var[vi].tile = shapes[vi][0];
+        E.var[vi].mpc = shapes[vi][1];
+        E.var[vi].usable = members % shapes[vi][1] == 0;
+    }
+    SWE_TRY((Ensemble::set_attrs<32, 32, kTf32x3>()));
+    SWE_TRY((Ensemble::set_attrs<32, 64, kTf32x3>()));
+    SWE_TRY((Ensemble::set_attrs<16, 32, kTf32x3>()));
+    SWE_TRY((Ensemble::set_attrs<16, 64, kTf32x3>()));
+    SWE_TRY((Ensemble::set_attrs<32, 32, kBf16x3>()));
+    SWE_TRY((Ensemble::set_attrs<32, 64, kBf16x3>()));
     E.prec = kTf32x3;
     E.ready = true;
-    // default choice until tuned: all members in one CTA
-    E.chosen = E.var[1].usable ? 1 : 0;
+    // default choice until tuned: 32-node tiles, all members in one CTA
+    E.chosen = E.var[0].usable ? 0 : 1;
     return E.build_graph();
 }
 
@@ -553,43 +583,49 @@ int swe_ens_stage(int substep_id) {
 int swe_ens_tune(double* ms_per_step) {
     SWE_TRY(ens_ready());
     SWE_TRY(tune(g_ens));
-    if (ms_per_step) {
-        ms_per_step[0] = g_ens.tune_ms[0];
-        ms_per_step[1] = g_ens.tune_ms[1];
-        ms_per_step[2] = ms_per_step[3] = -1.0;
-    }
+    if (ms_per_step)
+        for (int vi = 0; vi < kEnsVariants; ++vi) ms_per_step[vi] = g_ens.tune_ms[vi];
     return SWE_OK;
 }
 
 int swe_ens_use_variant(int tile_nodes, int members_per_cta) {
     SWE_TRY(ens_ready());
-    if (tile_nodes != kEnsTileNodes) {
-        set_error("swe_ens_use_variant: tiles have %d nodes, got %d", kEnsTileNodes, tile_nodes);
+    if (tile_nodes != 32 && tile_nodes != 16) {
+        set_error("swe_ens_use_variant: tiles have 32 or 16 nodes, got %d", tile_nodes);
         return SWE_ERR_ARG;
     }
-    for (int vi = 0; vi < 2; ++vi) {
-        const Variant& v = g_ens.var[vi];
-        if (v.mpc == members_per_cta) {
-            if (!v.usable) {
-                set_error("swe_ens_use_variant: %d members per CTA does not divide %d members", members_per_cta,
-                          g_ens.members);
-                return SWE_ERR_ARG;
-            }
-            g_ens.chosen = vi;
-            return g_ens.build_graph();
-        }
+    if (members_per_cta != 32 && members_per_cta != 64) {
+        set_error("swe_ens_use_variant: members per CTA must be 32 or 64, got %d", members_per_cta);
+        return SWE_ERR_ARG;
     }
-    set_error("swe_ens_use_variant: members per CTA must be 32 or 64, got %d", members_per_cta);
+    for (int vi = 0; vi < kEnsVariants; ++vi) {
+        const Variant& v = g_ens.var[vi];
+        if (v.tile != tile_nodes || v.mpc != members_per_cta) continue;
+        if (!v.usable) {
+            set_error("swe_ens_use_variant: %d members per CTA does not divide %d members", members_per_cta,
+                      g_ens.members);
+            return SWE_ERR_ARG;
+        }
+        if (!g_ens.usable(vi)) {
+            set_error("swe_ens_use_variant: split BF16 runs on 32-node tiles only");
+            return SWE_ERR_ARG;
+        }
+        g_ens.chosen = vi;
+        return g_ens.build_graph();
+    }
+    set_error("swe_ens_use_variant: no variant (%d, %d)", tile_nodes, members_per_cta);
     return SWE_ERR_ARG;
 }
 
 int swe_ens_config(int* out) {
     SWE_TRY(ens_ready());
     if (!out) { set_error("swe_ens_config: null out"); return SWE_ERR_ARG; }
-    out[0] = kEnsTileNodes;
-    out[1] = g_ens.var[g_ens.chosen].mpc;
-    out[2] = g_ens.max_rows;
-    out[3] = g_ens.ntiles;
+    const Variant& v = g_ens.var[g_ens.chosen];
+    const DevTables& tb = g_ens.tabs[Ensemble::shape_of(v.tile)];
+    out[0] = v.tile;
+    out[1] = v.mpc;
+    out[2] = tb.max_rows;
+    out[3] = tb.ntiles;
     out[4] = g_ens.prec;
     return SWE_OK;
 }
@@ -602,7 +638,11 @@ int swe_ens_set_precision(int precision) {
     }
     SWE_CUDA_TRY(cudaStreamSynchronize(g_ens.stream));
     g_ens.prec = precision;
-    g_ens.tune_ms[0] = g_ens.tune_ms[1] = -1.0;
+    for (double& t : g_ens.tune_ms) t = -1.0;
+    // split BF16 has 32-node tiles only: keep the members per CTA, move to 32-node tiles
+    if (!g_ens.usable(g_ens.chosen))
+        for (int vi = 0; vi < kEnsVariants; ++vi)
+            if (g_ens.var[vi].tile == 32 && g_ens.var[vi].mpc == g_ens.var[g_ens.chosen].mpc) g_ens.chosen = vi;
     return g_ens.build_graph();
 }
 

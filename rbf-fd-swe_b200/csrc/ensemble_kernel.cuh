@@ -55,9 +55,10 @@ constexpr uint32_t kEnsWaitTries = 1u << 22;              // final MMA drain: po
 constexpr uint32_t kEnsWaitHintNs = 20000;                 // one sleeping try: up to 20 us
 constexpr uint64_t kEnsWaitLimitNs = 2000000000ull;        // a wait gives up after 2 s
 
-template <int MPC, int PREC>
+template <int T, int MPC, int PREC>
 struct EnsCfg {
-    using Op = ens::Operands<MPC, PREC>;
+    using Op = ens::Operands<T, MPC, PREC>;
+    static constexpr int kT = T;                           // nodes per tile
     static constexpr int kN = 4 * MPC;                     // MMA N: member-fields per CTA
     static constexpr int kConvWarps = MPC / 8;             // 4 * MPC converter threads
     static constexpr int kConvThreads = 32 * kConvWarps;
@@ -67,9 +68,10 @@ struct EnsCfg {
     static constexpr int kStages = Op::kStages;            // ring slots
     static constexpr int kStageBytes = Op::kStageBytes;
     static constexpr int kXchStride = 36;                  // floats per (op, node) row; 9 x 16 B
-    static constexpr int kXchGroupFloats = 4 * kEnsTileNodes * kXchStride;
-    static constexpr int kTbRs = kEnsTileNodes * kPointStride * 4;   // per-tile buffer: PT, row sums, centre
-    static constexpr int kTbCen = kTbRs + kEnsTileNodes * 16;
+    static constexpr int kXchGroupFloats = 4 * T * kXchStride;
+    static constexpr int kTbRs = T * kPointStride * 4;     // per-tile buffer: PT, row sums, centre
+    static constexpr int kTbCen = kTbRs + T * 16;
+    static constexpr int kPairs = T / 16;                  // (node, member) pairs per epilogue thread and chunk
     static constexpr int kTileBuf = (kTbCen + kN * 4 + 127) / 128 * 128;
     static constexpr int kSmem = kStages * kStageBytes + 2 * kXchGroupFloats * 4 + 2 * kTileBuf;
     static constexpr int kTmemCols = (2 * kN <= 256) ? 256 : 512;
@@ -187,9 +189,9 @@ struct EpiSet {
 
 }  // namespace ens
 
-template <int MPC, int MODE, int PREC>
-__global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kernel(const EnsArgs a) {
-    using C = EnsCfg<MPC, PREC>;
+template <int T, int MPC, int MODE, int PREC>
+__global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_kernel(const EnsArgs a) {
+    using C = EnsCfg<T, MPC, PREC>;
     using Op = typename C::Op;
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t full_bar[C::kStages], empty_bar[C::kStages];
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
             const int tile = p.u / halves;
             const long col = (long)(p.u % halves) * C::kN + th.col();
             const float* cen_row = p.u != u_prev ? a.Kin + (long)__ldg(a.centre + tile) * a.mf : nullptr;
-            Op::fetch_ops(a.Kin, a.mf, col, a.W, (long)tile * kEnsTileNodes + th.at, cen_row, th, f, o, prev);
+            Op::fetch_ops(a.Kin, a.mf, col, a.W, (long)tile * T + th.at, cen_row, th, f, o, prev);
         };
         int g = 0;
         auto step = [&](typename Op::Set& o, typename Op::Set& nx, int u_cur) -> bool {
@@ -315,11 +317,11 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
         // per-tile pointwise records, row sums and centre row: bulk copies into tbuf[it & 1]
         auto issue_tile = [&](int u, int b) {
             const int tile = u / halves;
-            const int nn = min(kEnsTileNodes, a.n - tile * kEnsTileNodes);
+            const int nn = min(T, a.n - tile * T);
             unsigned char* tb = tbuf + b * C::kTileBuf;
             tc::mbar_arrive_expect_tx(&tile_bar[b], nn * (kPointStride * 4 + 16) + C::kN * 4);
-            tc::bulk_g2s(tb, a.PT + (long)tile * kEnsTileNodes * 5, nn * kPointStride * 4, &tile_bar[b]);
-            tc::bulk_g2s(tb + C::kTbRs, a.RS + (long)tile * kEnsTileNodes, nn * 16, &tile_bar[b]);
+            tc::bulk_g2s(tb, a.PT + (long)tile * T * 5, nn * kPointStride * 4, &tile_bar[b]);
+            tc::bulk_g2s(tb + C::kTbRs, a.RS + (long)tile * T, nn * 16, &tile_bar[b]);
             tc::bulk_g2s(tb + C::kTbCen, a.Kin + (long)__ldg(a.centre + tile) * a.mf + (u % halves) * C::kN,
                          C::kN * 4, &tile_bar[b]);
         };
@@ -329,9 +331,9 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
             const int tile = u / halves;
             const int col0 = (u % halves) * C::kN;
 #pragma unroll
-            for (int pi = 0; pi < 2; ++pi) {
+            for (int pi = 0; pi < C::kPairs; ++pi) {
                 const int pr = gt + 128 * pi;
-                const long node = (long)tile * kEnsTileNodes + (pr >> 3);
+                const long node = (long)tile * T + (pr >> 3);
                 if (node >= a.n) continue;
                 const int mfb = col0 + ch * 32 + 4 * (pr & 7);
                 const long e4 = node * a.mf + mfb;
@@ -357,27 +359,32 @@ __global__ void __launch_bounds__(EnsCfg<MPC, PREC>::kThreads, 1) ens_stage_kern
                 tc::tmem_ld16(taddr, v0);
                 tc::tmem_ld16(taddr + 16, v1);
                 tc::tmem_wait_ld();
-                float* row = xch + (op * 32 + lane) * C::kXchStride;
+                // (operator, node) row: TMEM lane `lane` of this quarter holds node `lane`
+                // (M = 128); with M = 64 the quarter's lanes 0..15 hold the tile's 16 nodes
+                if (lane < T) {
+                    float* row = xch + (op * T + lane) * C::kXchStride;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    *reinterpret_cast<float4*>(row + 4 * q) = make_float4(v0[4 * q], v0[4 * q + 1], v0[4 * q + 2], v0[4 * q + 3]);
-                    *reinterpret_cast<float4*>(row + 16 + 4 * q) =
-                        make_float4(v1[4 * q], v1[4 * q + 1], v1[4 * q + 2], v1[4 * q + 3]);
+                    for (int q = 0; q < 4; ++q) {
+                        *reinterpret_cast<float4*>(row + 4 * q) =
+                            make_float4(v0[4 * q], v0[4 * q + 1], v0[4 * q + 2], v0[4 * q + 3]);
+                        *reinterpret_cast<float4*>(row + 16 + 4 * q) =
+                            make_float4(v1[4 * q], v1[4 * q + 1], v1[4 * q + 2], v1[4 * q + 3]);
+                    }
                 }
             }
             ens::named_sync(2 + grp, 128);
 #pragma unroll
-            for (int pi = 0; pi < 2; ++pi) {
+            for (int pi = 0; pi < C::kPairs; ++pi) {
                 const int pr = gt + 128 * pi;
                 const int t = pr >> 3, bm = pr & 7;
-                const long node = (long)tile * kEnsTileNodes + t;
+                const long node = (long)tile * T + t;
                 if (node >= a.n) continue;
                 const int mfb = col0 + ch * 32 + 4 * bm;      // first mf of this member
                 const int member = mfb >> 2;
                 float S[16];
 #pragma unroll
                 for (int o2 = 0; o2 < 4; ++o2) {
-                    const float4 sv = *reinterpret_cast<const float4*>(xch + (o2 * 32 + t) * C::kXchStride + 4 * bm);
+                    const float4 sv = *reinterpret_cast<const float4*>(xch + (o2 * T + t) * C::kXchStride + 4 * bm);
                     S[4 * o2] = sv.x; S[4 * o2 + 1] = sv.y; S[4 * o2 + 2] = sv.z; S[4 * o2 + 3] = sv.w;
                 }
                 const float4 cen = *reinterpret_cast<const float4*>(tb + C::kTbCen / 4 + (mfb - col0));

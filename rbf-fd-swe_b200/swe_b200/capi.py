@@ -319,7 +319,11 @@ class Ensemble:
     def sync(self) -> None:
         check("swe_ens_sync", self.lib.swe_ens_sync())
 
+    # order of swe_ens_tune's table: (tile nodes, members per CTA)
+    TUNE_VARIANTS = ((32, 64), (32, 32), (16, 64), (16, 32))
+
     def tune(self) -> np.ndarray:
+        """ms per RK4 step of each variant in TUNE_VARIANTS order (-1: not usable)."""
         ms = np.zeros(4)
         check("swe_ens_tune", self.lib.swe_ens_tune(_p(ms)))
         return ms

@@ -21,7 +21,8 @@ from swe_b200 import capi, gen, swe_input
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [(32, 32), (32, 64)]
+# (tile nodes, members per CTA): 32-node tiles (M = 128) and 16-node tiles (M = 64, 3xTF32 only)
+VARIANTS = [(32, 32), (32, 64), (16, 32), (16, 64)]
 
 
 @pytest.fixture(scope="module")
@@ -50,8 +51,13 @@ def test_eval_rhs_every_variant(ens, model_l4, tile, mpc, prec):
     m = model_l4
     ens.init(m, 64)
     ens.set_precision(prec)
+    if prec == "bf16x3" and tile == 16:
+        with pytest.raises(capi.SweError, match="32-node tiles"):
+            ens.use_variant(tile, mpc)
+        return
     ens.use_variant(tile, mpc)
-    assert ens.config()["precision"] == prec
+    cfg = ens.config()
+    assert cfg["precision"] == prec and cfg["tile_nodes"] == tile and cfg["members_per_cta"] == mpc
     K = _members(m, 64)
     F = ens.eval_rhs(K)
     port = oracle.Port(m, "fp64")
@@ -85,6 +91,46 @@ def test_steps_match_fp64_oracle(ens, model_l4, prec):
         err = rel_err(H[b], want)
         print(f"20 steps {prec} member {b}: err {err} fp32 {fp32_err} ratio {err / fp32_err}")
         assert (err <= STEP_FACTOR[prec] * fp32_err).all(), (b, err, fp32_err)
+
+
+@pytest.mark.parametrize("tile,mpc", VARIANTS)
+def test_every_tile_shape_steps_like_the_oracle(ens, model_l4, tile, mpc):
+    """Each tile shape and members-per-CTA choice, forced, over 20 RK4 steps: the same
+    bar as the tuned kernel (3xTF32 within 5x the FP32 restatement's error)."""
+    m = model_l4
+    ens.init(m, 64)
+    ens.set_precision("tf32x3")
+    ens.use_variant(tile, mpc)
+    H0 = _members(m, 64)
+    ens.set_state(H0)
+    ens.step(20)
+    H = ens.get_state()
+    port, port32 = oracle.Port(m, "fp64"), oracle.Port(m, "fp32")
+    for b in (3, 50):
+        want = port.run(H0[b], 20)
+        fp32_err = rel_err(port32.run(H0[b], 20), want)
+        err = rel_err(H[b], want)
+        assert (err <= STEP_FACTOR["tf32x3"] * fp32_err).all(), (tile, mpc, b, err, fp32_err)
+
+
+def test_tuner_times_every_variant(ens, model_l4):
+    """swe_ens_tune times the four (tile, members-per-CTA) variants for 3xTF32 and keeps
+    the fastest; split BF16 has the two 32-node variants only."""
+    ens.init(model_l4, 64)
+    ens.set_precision("tf32x3")
+    ms = ens.tune()
+    assert (ms > 0).all(), ms
+    best = int(np.argmin(ms))
+    cfg = ens.config()
+    assert (cfg["tile_nodes"], cfg["members_per_cta"]) == VARIANTS_TUNE_ORDER[best]
+    ens.set_precision("bf16x3")
+    ms = ens.tune()
+    assert (ms[:2] > 0).all() and (ms[2:] < 0).all(), ms
+    assert ens.config()["tile_nodes"] == 32
+
+
+# the order of swe_ens_tune's table
+VARIANTS_TUNE_ORDER = [(32, 64), (32, 32), (16, 64), (16, 32)]
 
 
 def test_rejects_bad_precision(ens, model_l4):
