@@ -92,9 +92,32 @@ int swe_cuda_eval_rhs(const void* K, void* F);
  * reads the stage state that substep k-1 wrote. */
 int swe_cuda_rk_substep(int substep_id);
 
+/* Halo rows of a patch that is one part of a grid split across ranks (the
+ * reference's MPI patches, mpi/init_patches.c:21-92): rows outside
+ * compute_pid_s .. compute_pid_s + compute_size - 1 that the compute rows'
+ * stencils read.  swe_cuda_rk_substep steps such a patch (H and the K buffers
+ * hold all patch rows, D compute rows only, as in the reference); between
+ * substeps the caller refreshes the halo rows of the buffer the next substep
+ * reads, as the reference's exchange_SVM_halos does after eval_K and update_H
+ * (mpi/halos.c:11-35):
+ *   swe_cuda_halo_setup   patch rows this rank sends (compute rows) and
+ *                         receives (halo rows), host arrays, checked; once;
+ *   swe_cuda_halo_pack    the send rows of the buffer substep `substep_id`
+ *                         reads -> send_buf, a [n_send][4] device buffer;
+ *   swe_cuda_halo_unpack  recv_buf ([n_recv][4], device) -> the receive rows.
+ * Pack and unpack are asynchronous on the library's stream (swe_cuda_sync
+ * before handing the send buffer to a communication library).  After
+ * substep s the next substep is (s + 1) % 4, and its buffer is what to
+ * exchange.  Transport is the caller's (swe_b200/shard.py: NCCL send/recv over
+ * NVLink, or gloo); nothing here reads another GPU's memory. */
+int swe_cuda_halo_setup(const int* send_rows, int n_send, const int* recv_rows, int n_recv);
+int swe_cuda_halo_pack(int substep_id, void* send_buf);
+int swe_cuda_halo_unpack(int substep_id, const void* recv_buf);
+
 /* nsteps full RK4 steps (4 stages each) from a captured CUDA graph.
  * Asynchronous; requires compute_pid_s == 0 and patch_size == compute_size
- * (one GPU, no halo exchange). */
+ * (no halo rows: a patch with halo rows steps by swe_cuda_rk_substep with
+ * halo exchanges between substeps). */
 int swe_cuda_step(int nsteps);
 
 /* Waits for all work of the library's stream. */

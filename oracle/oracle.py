@@ -154,6 +154,12 @@ class Port:
         self.lib.oracle_run(ctypes.byref(self.grid), _ptr(H), int(nsteps))
         return H
 
+    def rk_substep(self, H: np.ndarray, K: np.ndarray, F: np.ndarray, D: np.ndarray, substep_id: int) -> None:
+        """RK_substep (rk4_rbffd_swe.c:30-72) on [n][4] arrays of this precision, in place."""
+        for a in (H, K, F, D):
+            assert a.dtype == self.dtype and a.flags.c_contiguous and a.size == 4 * self.n
+        self.lib.oracle_rk_substep(ctypes.byref(self.grid), _ptr(H), _ptr(K), _ptr(F), _ptr(D), int(substep_id))
+
     def invariants(self, H: np.ndarray) -> np.ndarray:
         """FP64 (mass, energy) per member for H of shape [members, n, 4] or [n, 4]."""
         H = np.ascontiguousarray(H, dtype=self.dtype).reshape(-1, self.n, 4)

@@ -95,6 +95,9 @@ struct Plain {
          *Kx = nullptr, *raw = nullptr, *Wl = nullptr;
     int* idx = nullptr;
     int* idxl = nullptr;            // node-per-lane kernel: tile-transposed weights / indices
+    int* halo_send = nullptr;       // patch rows this rank sends / receives (swe_cuda_halo_setup)
+    int* halo_recv = nullptr;
+    int n_send = 0, n_recv = 0;
     double* inv = nullptr;
     int* err = nullptr;             // pipelined kernel: bounded-wait error word
     int* err_host = nullptr;        // pinned copy of it, read back with the state
@@ -126,7 +129,9 @@ struct Plain {
         steps_done = 0;
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
-        for (void* p : {W, PT, H, Ka, Kb, D, F, Kx, raw, Wl}) if (p) cudaFree(p);
+        for (void* p : {W, PT, H, Ka, Kb, D, F, Kx, raw, Wl, (void*)halo_send, (void*)halo_recv}) if (p) cudaFree(p);
+        halo_send = halo_recv = nullptr;
+        n_send = n_recv = 0;
         if (idx) cudaFree(idx);
         if (idxl) cudaFree(idxl);
         if (inv) cudaFree(inv);
@@ -169,6 +174,11 @@ struct Plain {
         return SWE_OK;
     }
 
+    // The stage kernels index the compute rows 0..n-1 for everything they write (D, F,
+    // K_out, H) and read the gather source at patch rows.  H and the K buffers hold the
+    // whole patch, as the reference's do (eval_K and update_H write rows compute_pid_s +
+    // i, rk4_rbffd_swe.c:86-158), so the kernels get H and K_out starting at the first
+    // compute row; with no halo rows (compute_pid_s = 0) the offset is zero.
     template <typename T>
     StageArgs<T> args(int mode) const {
         StageArgs<T> a{};
@@ -177,21 +187,26 @@ struct Plain {
         a.idx = reinterpret_cast<const int4*>(idx);
         a.W = reinterpret_cast<const uint4*>(W);
         a.PT = reinterpret_cast<const T*>(PT);
-        a.H = reinterpret_cast<T*>(H);
+        a.H = reinterpret_cast<T*>(H) + 4L * pid0;
         a.D = reinterpret_cast<T*>(D);
         a.F = reinterpret_cast<T*>(F);
         a.gh0 = (T)gh0;
         const T dtT = (T)dt;
         a.dt6 = (double)dtT / 6.0;
+        T* ka = reinterpret_cast<T*>(Ka) + 4L * pid0;
+        T* kb = reinterpret_cast<T*>(Kb) + 4L * pid0;
         switch (mode) {
-            case 0: a.Kin = reinterpret_cast<const T*>(H); a.Kout = reinterpret_cast<T*>(Ka); a.c = (T)(dtT / 2.0); break;
-            case 1: a.Kin = reinterpret_cast<const T*>(Ka); a.Kout = reinterpret_cast<T*>(Kb); a.c = (T)(dtT / 2.0); break;
-            case 2: a.Kin = reinterpret_cast<const T*>(Kb); a.Kout = reinterpret_cast<T*>(Ka); a.c = dtT; break;
+            case 0: a.Kin = reinterpret_cast<const T*>(H); a.Kout = ka; a.c = (T)(dtT / 2.0); break;
+            case 1: a.Kin = reinterpret_cast<const T*>(Ka); a.Kout = kb; a.c = (T)(dtT / 2.0); break;
+            case 2: a.Kin = reinterpret_cast<const T*>(Kb); a.Kout = ka; a.c = dtT; break;
             case 3: a.Kin = reinterpret_cast<const T*>(Ka); a.Kout = nullptr; a.c = dtT; break;
             default: a.Kin = reinterpret_cast<const T*>(Kx); a.Kout = nullptr; a.c = T(0); break;
         }
         return a;
     }
+
+    // the buffer substep `s` reads its gather source from: H, Ka, Kb, Ka
+    void* stage_input(int s) const { return s == 0 ? H : s == 2 ? Kb : Ka; }
 
     bool use_tma() const { return tma_ok && kernel_choice == 0; }
 
@@ -608,10 +623,6 @@ int swe_cuda_rk_substep(int substep_id) {
     SWE_TRY(require_ready());
     if (substep_id < 0 || substep_id > 3) { set_error("substep_id %d not in 0..3", substep_id); return SWE_ERR_ARG; }
     Plain& P = g_plain;
-    if (P.pid0 != 0 || P.rows != P.n) {
-        set_error("time stepping needs compute_pid_s == 0 and patch_size == compute_size (no halos)");
-        return SWE_ERR_ARG;
-    }
     SWE_TRY(P.launch(substep_id));
     return substep_id == 3 ? after_step() : SWE_OK;
 }
@@ -621,7 +632,8 @@ int swe_cuda_step(int nsteps) {
     Plain& P = g_plain;
     if (nsteps < 0) { set_error("nsteps < 0"); return SWE_ERR_ARG; }
     if (P.pid0 != 0 || P.rows != P.n) {
-        set_error("time stepping needs compute_pid_s == 0 and patch_size == compute_size (no halos)");
+        set_error("swe_cuda_step runs whole steps without halo exchanges: a patch with halo rows steps by "
+                  "swe_cuda_rk_substep, with swe_cuda_halo_pack / swe_cuda_halo_unpack between substeps");
         return SWE_ERR_ARG;
     }
     if (P.timing) {
@@ -638,6 +650,88 @@ int swe_cuda_step(int nsteps) {
         P.step_timed = true;
     }
     return SWE_OK;
+}
+
+}  // extern "C"
+
+// Halo rows of a patch (rows outside compute_pid_s .. compute_pid_s + compute_size - 1
+// that the compute rows' stencils read): the caller exchanges them between substeps,
+// as the reference's exchange_SVM_halos does after eval_K and update_H
+// (rk4_rbffd_swe.c:86-158).  pack copies the listed patch rows of the buffer substep
+// `substep_id` reads into a [count][4] device buffer; unpack writes such a buffer into
+// the listed rows.  Row lists are set once by swe_cuda_halo_setup.
+template <typename T>
+__global__ void halo_copy_kernel(const int* __restrict__ rows, int count, const T* __restrict__ src, T* __restrict__ dst,
+                                 int to_rows) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count * 4) return;
+    const int j = t >> 2, f = t & 3;
+    const long r = rows[j];
+    if (to_rows) dst[4 * r + f] = src[t];
+    else dst[t] = src[4 * r + f];
+}
+
+static int halo_copy(int substep_id, void* ext, bool pack) {
+    SWE_TRY(require_ready());
+    Plain& P = g_plain;
+    if (substep_id < 0 || substep_id > 3) { set_error("substep_id %d not in 0..3", substep_id); return SWE_ERR_ARG; }
+    const int count = pack ? P.n_send : P.n_recv;
+    const int* rows = pack ? P.halo_send : P.halo_recv;
+    if (count == 0) return SWE_OK;
+    if (!ext) { set_error("swe_cuda_halo_%s: null buffer", pack ? "pack" : "unpack"); return SWE_ERR_ARG; }
+    void* buf = P.stage_input(substep_id);
+    const int threads = 256, blocks = ceil_div(4L * count, threads);
+    if (P.fsize == 8)
+        halo_copy_kernel<double><<<blocks, threads, 0, P.stream>>>(rows, count, (const double*)(pack ? buf : ext),
+                                                                  (double*)(pack ? ext : buf), pack ? 0 : 1);
+    else
+        halo_copy_kernel<float><<<blocks, threads, 0, P.stream>>>(rows, count, (const float*)(pack ? buf : ext),
+                                                                 (float*)(pack ? ext : buf), pack ? 0 : 1);
+    count_launch();
+    SWE_CUDA_TRY(cudaGetLastError());
+    return SWE_OK;
+}
+
+extern "C" {
+
+int swe_cuda_halo_setup(const int* send_rows, int n_send, const int* recv_rows, int n_recv) {
+    SWE_TRY(require_ready());
+    Plain& P = g_plain;
+    if (n_send < 0 || n_recv < 0 || (n_send && !send_rows) || (n_recv && !recv_rows)) {
+        set_error("swe_cuda_halo_setup: bad row lists");
+        return SWE_ERR_ARG;
+    }
+    for (int j = 0; j < n_send; ++j)
+        if (send_rows[j] < P.pid0 || send_rows[j] >= P.pid0 + P.n) {
+            set_error("swe_cuda_halo_setup: send row %d (entry %d) is not a compute row %d..%d", send_rows[j], j,
+                      P.pid0, P.pid0 + P.n - 1);
+            return SWE_ERR_INDEX;
+        }
+    for (int j = 0; j < n_recv; ++j)
+        if (recv_rows[j] < 0 || recv_rows[j] >= P.rows || (recv_rows[j] >= P.pid0 && recv_rows[j] < P.pid0 + P.n)) {
+            set_error("swe_cuda_halo_setup: receive row %d (entry %d) is not a halo row of the %d-row patch",
+                      recv_rows[j], j, P.rows);
+            return SWE_ERR_INDEX;
+        }
+    if (P.halo_send) cudaFree(P.halo_send);
+    if (P.halo_recv) cudaFree(P.halo_recv);
+    P.halo_send = P.halo_recv = nullptr;
+    P.n_send = P.n_recv = 0;
+    SWE_CUDA_TRY(cudaMalloc(&P.halo_send, sizeof(int) * std::max(n_send, 1)));
+    SWE_CUDA_TRY(cudaMalloc(&P.halo_recv, sizeof(int) * std::max(n_recv, 1)));
+    if (n_send)
+        SWE_CUDA_TRY(cudaMemcpyAsync(P.halo_send, send_rows, sizeof(int) * n_send, cudaMemcpyHostToDevice, P.stream));
+    if (n_recv)
+        SWE_CUDA_TRY(cudaMemcpyAsync(P.halo_recv, recv_rows, sizeof(int) * n_recv, cudaMemcpyHostToDevice, P.stream));
+    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    P.n_send = n_send;
+    P.n_recv = n_recv;
+    return SWE_OK;
+}
+
+int swe_cuda_halo_pack(int substep_id, void* send_buf) { return halo_copy(substep_id, send_buf, true); }
+int swe_cuda_halo_unpack(int substep_id, const void* recv_buf) {
+    return halo_copy(substep_id, const_cast<void*>(recv_buf), false);
 }
 
 int swe_cuda_sync(void) {

@@ -94,6 +94,9 @@ def load() -> ctypes.CDLL:
     lib.swe_srv_submit.argtypes = [i, i, i, vp]
     lib.swe_srv_poll.argtypes = [i, vp]
     lib.swe_srv_fetch.argtypes = [i, vp]
+    lib.swe_cuda_halo_setup.argtypes = [vp, i, vp, i]
+    lib.swe_cuda_halo_pack.argtypes = [i, vp]
+    lib.swe_cuda_halo_unpack.argtypes = [i, vp]
     lib.swe_srv_set_dep_limit.argtypes = [d]
     lib.swe_srv_test_withhold.argtypes = [i, i]
     lib.swe_srv_cancel.argtypes = [i]
@@ -223,6 +226,20 @@ class Plain:
 
     def stream(self) -> int:
         return int(self.lib.swe_cuda_stream() or 0)
+
+    def halo_setup(self, send_rows: np.ndarray, recv_rows: np.ndarray) -> None:
+        """Patch rows this rank sends (its compute rows other ranks read) and receives."""
+        s = np.ascontiguousarray(send_rows, dtype=np.int32)
+        r = np.ascontiguousarray(recv_rows, dtype=np.int32)
+        check("swe_cuda_halo_setup", self.lib.swe_cuda_halo_setup(_p(s), len(s), _p(r), len(r)))
+
+    def halo_pack(self, substep_id: int, send_ptr: int) -> None:
+        """Send rows of the buffer substep `substep_id` reads -> a [n_send][4] device buffer."""
+        check("swe_cuda_halo_pack", self.lib.swe_cuda_halo_pack(int(substep_id), send_ptr))
+
+    def halo_unpack(self, substep_id: int, recv_ptr: int) -> None:
+        """A [n_recv][4] device buffer -> the receive rows of that buffer."""
+        check("swe_cuda_halo_unpack", self.lib.swe_cuda_halo_unpack(int(substep_id), recv_ptr))
 
     def select_kernel(self, which: int) -> None:
         """0: bulk-copy pipelined stage kernel, 1: register-streaming kernel, 2 / 3 / 4: pipelined with
