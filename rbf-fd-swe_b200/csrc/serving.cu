@@ -61,6 +61,9 @@ struct alignas(16) ReqDesc {   // device table entry of an admitted request
     int members;
     int chunk_nodes;     // nodes per work item
     int per_stage;       // items per stage: chunks x members
+    int nchunks;         // node chunks of the grid
+    int reach;           // chunks a chunk's stencils reach on either side
+    int* cdone;          // [members][nchunks]: stages completed by each chunk of each member
     int total;           // items of the whole request
     int id;              // request id (written into the completion flag)
     int cancelled;
@@ -224,16 +227,24 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
                 __ldcg(reinterpret_cast<const uint4*>(reqs + it.slot) + threadIdx.x);
         __syncthreads();
         const ReqDesc& r = s_req;
-        // dependency: every chunk of the previous stage index has completed
+        // dependency: the member's chunks within reach of this one (the rows its
+        // stencils read) have completed the previous stage.  That also orders the
+        // writes: a chunk's stage q overwrites the K buffer stage q - 2 wrote, and its
+        // neighbours finished reading that buffer in stage q - 1.
         if (threadIdx.x == 0) {
             s_ok = 1;
-            const int need = it.q * r.per_stage;
+            const int* cd = r.cdone + (long)it.member * r.nchunks;
+            const int c_lo = max(0, it.chunk - r.reach), c_hi = min(r.nchunks - 1, it.chunk + r.reach);
             const unsigned long long limit = *(volatile const unsigned long long*)&dctl->dep_ns;
             const unsigned long long t0 = globaltimer();
-            // plain loads (served by L2, no atomic serialisation against the
-            // increments on the critical path) with exponential backoff
+            // plain loads (served by L2) with exponential backoff
             unsigned ns = 64;
-            while (*(volatile const int*)(done + it.slot) < need) {
+            auto ready = [&]() {
+                for (int c = c_lo; c <= c_hi; ++c)
+                    if (*(volatile const int*)(cd + c) < it.q) return false;
+                return true;
+            };
+            while (!ready()) {
                 if (*(volatile const int*)&dctl->stop) { s_ok = 0; break; }
                 if (globaltimer() - t0 > limit) {
                     s_ok = 0;
@@ -260,13 +271,18 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
+            // this chunk of this member has completed stage index q
+            *(volatile int*)(r.cdone + (long)it.member * r.nchunks + it.chunk) = it.q + 1;
+            __threadfence();
             const int c = atomicAdd(done + it.slot, 1) + 1;
-            ((volatile int*)mdone)[it.slot] = c;          // monotonic mirror for the scheduler
             const unsigned long long d = atomicAdd(items_done, 1ull) + 1;
             if ((d & 63) == 0) ctl->progress = (long long)d;
-            // push the mirrors out of the GPU's caches to host memory now:
-            // the scheduler paces its appends on them
-            __threadfence_system();
+            // the scheduler paces its appends on a per-request mirror in host memory,
+            // pushed out when a stage's worth of items has completed
+            if (c % r.per_stage == 0) {
+                ((volatile int*)mdone)[it.slot] = c;
+                __threadfence_system();
+            }
             if (c == r.total) {
                 __threadfence_system();
                 ((volatile int*)flags)[it.slot] = r.id;
@@ -282,6 +298,7 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
 
 struct Grid {
     int n, nnbr;
+    int reach = 0;          // work-item chunks a chunk's stencils reach on either side
     double gh0, dt;
     void* W = nullptr;
     int* idx = nullptr;
@@ -411,7 +428,8 @@ struct Server {
 
     static size_t state_bytes(int n, int members) {
         const size_t one = (size_t)n * 4 * sizeof(double) * members;
-        return ((one + 255) / 256 * 256) * 4;      // H, Ka, Kb, D
+        const size_t prog = (size_t)members * ((n + chunk_nodes(n) - 1) / chunk_nodes(n)) * sizeof(int);
+        return ((one + 255) / 256 * 256) * 4 + (prog + 255) / 256 * 256;   // H, Ka, Kb, D, chunk progress
     }
     // nodes per work item: about 2048 (tens of microseconds of FP64 stage work),
     // fewer on small grids so that they still split into several items
@@ -470,7 +488,7 @@ struct Server {
         r.offset = off;
         r.slot = free_slots.back();
         free_slots.pop_back();
-        const size_t one = r.bytes / 4;
+        const size_t one = ((size_t)G.n * 4 * sizeof(double) * r.members + 255) / 256 * 256;
         ReqDesc d{};
         d.W = reinterpret_cast<const uint4*>(G.W);
         d.idx = reinterpret_cast<const int4*>(G.idx);
@@ -480,7 +498,10 @@ struct Server {
         d.n = G.n;
         d.members = r.members;
         d.chunk_nodes = chunk_nodes(G.n);
-        d.per_stage = ((G.n + d.chunk_nodes - 1) / d.chunk_nodes) * r.members;
+        d.nchunks = (G.n + d.chunk_nodes - 1) / d.chunk_nodes;
+        d.reach = G.reach;
+        d.per_stage = d.nchunks * r.members;
+        d.cdone = reinterpret_cast<int*>(arena + off + 4 * one);
         d.total = d.per_stage * 4 * r.nsteps;
         d.id = r.id;
         d.cancelled = 0;
@@ -498,6 +519,7 @@ struct Server {
         // other requests meanwhile
         cudaMemcpyAsync(reqs_d + r.slot, &d, sizeof(d), cudaMemcpyHostToDevice, cstream);
         cudaMemcpyAsync(done_d + r.slot, &zero, sizeof(int), cudaMemcpyHostToDevice, cstream);
+        cudaMemsetAsync(d.cdone, 0, sizeof(int) * (size_t)d.nchunks * r.members, cstream);
         cudaMemcpyAsync(d.H, host_states(r), r.state_bytes, cudaMemcpyHostToDevice, cstream);
         if (cudaEventRecord(r.ev, cstream) != cudaSuccess) {
             fatal = "request upload failed";
@@ -756,6 +778,15 @@ int swe_srv_add_grid(int n, int nnbr, double gh0, double dt, const int* idx, con
     if (st != SWE_OK) return -st;
     Grid G;
     G.n = n; G.nnbr = nnbr; G.gh0 = gh0; G.dt = dt;
+    // how many work-item chunks a chunk's stencils reach on either side
+    {
+        const int cn = Server::chunk_nodes(n);
+        for (long i = 0; i < n; ++i)
+            for (int j = 0; j < nnbr; ++j) {
+                const int dc = std::abs(idx[i * nnbr + j] / cn - (int)(i / cn));
+                G.reach = std::max(G.reach, dc);
+            }
+    }
     G.W = ps.W;
     G.idx = ps.idx;
     G.PT = ps.PT;
