@@ -14,7 +14,8 @@ import re
 import numpy as np
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "lib", "libswe_b200.so")
+# SWE_B200_LIB names another build of the library (a test run against a variant build)
+LIB_PATH = os.environ.get("SWE_B200_LIB") or os.path.join(PKG_DIR, "lib", "libswe_b200.so")
 HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "swe_b200.h")
 
 SWE_LAYOUT_CFDL = 1
