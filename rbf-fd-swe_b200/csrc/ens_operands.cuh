@@ -67,7 +67,14 @@ struct Operands<T, MPC, kTf32x3> {
     static constexpr int kAHalf = (kM / 8) * kSboA;
     static constexpr int kBHalf = (kN / 8) * kSboB;
     static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
-    static constexpr int kStages = 3;
+    static constexpr int kStages = 2;
+    // staged gathers: per converter thread and chunk, 4 rows x 16 B of state and 4 rows x
+    // the thread's weights, in structure-of-arrays order (row-major over threads) so that
+    // each warp's shared-memory accesses are contiguous
+    static constexpr int kWBytes = 4 * kOps;                       // weight bytes per row and thread
+    static constexpr int kStgRows = 4 * kConvThreads * 16;
+    static constexpr int kStgBytes = kStgRows + 4 * kConvThreads * kWBytes;
+    static constexpr int kStgDepth = 3;                            // chunks in flight: g, g+1, g+2
     static_assert(T == 16 || T == 32, "tiles of 16 or 32 nodes");
     static_assert(kOps == 1 || kOps == 2 || kOps == 4, "A build: T nodes x 4 row groups x 4 operators");
     // the weights of the thread's operators: one, a pair or all four of (Dx, Dy, Dz, L)
@@ -98,6 +105,42 @@ struct Operands<T, MPC, kTf32x3> {
     __device__ static void fetch_idx(const int* rows, const uint32_t* jmap, int gc, const Thread& th, Fetch& f) {
         f.idx = __ldg(reinterpret_cast<const int4*>(rows + gc * kEnsKc + 4 * th.kg));
         f.jj = __ldg(jmap + (gc * 4 + th.akg) * T + th.at);
+    }
+    // cp.async of this thread's gathered rows and weights of one chunk into staging
+    // buffer `stg`; weights of rows outside the node's stencil are zero-filled.
+    __device__ static void stage_issue(unsigned char* stg, int ct, const float* Kin, int mf, long col, const float4* W,
+                                       long node, const Thread& th, const Fetch& f) {
+        const int r[4] = {f.idx.x, f.idx.y, f.idx.z, f.idx.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t dst = tc::smem_u32(stg + (i * kConvThreads + ct) * 16);
+            const float* src = Kin + (long)r[i] * mf + col;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+        }
+        unsigned char* wst = stg + kStgRows;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t j = (f.jj >> (8 * i)) & 0xffu;
+            const uint32_t dst = tc::smem_u32(wst + (i * kConvThreads + ct) * kWBytes);
+            // rows outside the stencil copy nothing (zero fill) from a valid address
+            const float* src = j != 0xffu ? reinterpret_cast<const float*>(W + node * 32 + j) + th.op0
+                                          : reinterpret_cast<const float*>(W);
+            const int n = j != 0xffu ? kWBytes : 0;
+            if constexpr (kWBytes == 16)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
+            else if constexpr (kWBytes == 8)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
+            else
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
+        }
+    }
+    __device__ static void stage_read(const unsigned char* stg, int ct, const float4& cen, Set& o) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) o.x[i] = *reinterpret_cast<const float4*>(stg + (i * kConvThreads + ct) * 16);
+        o.cen = cen;
+        const unsigned char* wst = stg + kStgRows;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) o.w[i] = *reinterpret_cast<const WT*>(wst + (i * kConvThreads + ct) * kWBytes);
     }
     __device__ static void fetch_ops(const float* Kin, int mf, long col, const float4* W, long node, const float* cen_row,
                                      const Thread& th, const Fetch& f, Set& o, const Set& prev) {
@@ -179,6 +222,7 @@ struct Operands<T, MPC, kTf32x3> {
 // --------------------------------------------------------------------------------------
 template <int MPC>
 struct Operands<32, MPC, kBf16x3> {
+    static constexpr int kStgDepth = 0, kStgBytes = 0;
     static constexpr int kN = 4 * MPC;
     static constexpr int kConvThreads = 4 * MPC;
     static constexpr int kOps = 256 / kConvThreads;

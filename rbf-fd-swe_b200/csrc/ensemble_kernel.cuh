@@ -26,11 +26,13 @@
 //
 // Persistent, warp-specialised CTA (one per SM; it owns all of tensor memory):
 //   * converter warps (MPC/8): for each 16-row chunk of K they gather the rows
-//     (16-byte loads issued one chunk ahead into a ping-pong register set),
+//     and weights (3xTF32: async copies into a staging buffer issued two chunks
+//     ahead, three buffers deep, so that no register waits on a gather; split
+//     BF16: 16-byte loads one chunk ahead into a ping-pong register set),
 //     centre and split them into the B operand, and write the matching A chunk
 //     densely, one 16-byte core row (4 chunk rows of one operator and node) per
-//     store, from a map of chunk rows to stencil slots; a ring of slots hands
-//     chunks to
+//     store, from a map of chunk rows to stencil slots; a ring of slots (2 for
+//     3xTF32, whose staging takes the third slot's shared memory) hands chunks to
 //   * the MMA warp: one thread issues the chunk's 3 products (128 x N x 16)
 //     into one of two TMEM accumulators and commits each chunk to the
 //     slot's "empty" barrier and each tile to the accumulator's "full" barrier;
@@ -73,7 +75,8 @@ struct EnsCfg {
     static constexpr int kTbCen = kTbRs + T * 16;
     static constexpr int kPairs = T / 16;                  // (node, member) pairs per epilogue thread and chunk
     static constexpr int kTileBuf = (kTbCen + kN * 4 + 127) / 128 * 128;
-    static constexpr int kSmem = kStages * kStageBytes + 2 * kXchGroupFloats * 4 + 2 * kTileBuf;
+    static constexpr int kStgOff = kStages * kStageBytes + 2 * kXchGroupFloats * 4 + 2 * kTileBuf;
+    static constexpr int kSmem = kStgOff + Op::kStgDepth * Op::kStgBytes;
     static constexpr int kTmemCols = (2 * kN <= 256) ? 256 : 512;
     static_assert(kConvThreads == Op::kConvThreads, "converter thread count");
     static_assert(kN % 64 == 0, "epilogue column chunks");
@@ -227,6 +230,64 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
 
     if (warp < C::kConvWarps) {
         // =============================== converters ===============================
+      if constexpr (PREC == kTf32x3) {
+        // staged gathers: chunk g + 2's rows and weights are in flight (cp.async) while
+        // chunk g is built from its staging buffer
+        const typename Op::Thread th(threadIdx.x);
+        const int ct = threadIdx.x;
+        unsigned char* stg0 = smem + C::kStgOff;
+        // chunk g's gathers are issued two steps ahead as async copies into staging
+        // buffer g % 3; the centre row of a new unit is loaded into a register then too
+        ens::Cursor cur = ens::first_cursor(a, halves);
+        ens::Cursor c1 = ens::next_cursor(cur, a, halves);
+        ens::Cursor c2 = ens::next_cursor(c1, a, halves);
+        typename Op::Fetch f2, f3;     // indices of chunks g + 2 and g + 3
+        float4 cen0 = make_float4(0.f, 0.f, 0.f, 0.f), cen1 = cen0, cen2 = cen0;   // centres of chunks g, g+1, g+2
+        // returns the centre state of chunk p's unit (a new unit loads it; else prev)
+        auto issue = [&](const ens::Cursor& p, const typename Op::Fetch& f, int slot, float4 prev) {
+            float4 c = prev;
+            if (p.valid) {
+                const int tile = p.u / halves;
+                const long col = (long)(p.u % halves) * C::kN + th.col();
+                Op::stage_issue(stg0 + slot * Op::kStgBytes, ct, a.Kin, a.mf, col, a.W, (long)tile * T + th.at, th, f);
+                if (p.gc == p.gc0) c = ens::ldg_f4(a.Kin + (long)__ldg(a.centre + tile) * a.mf + col);
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            return c;
+        };
+        if (cur.valid) {
+            typename Op::Fetch f0, f1;
+            Op::fetch_idx(a.rows, a.jmap, cur.gc, th, f0);
+            if (c1.valid) Op::fetch_idx(a.rows, a.jmap, c1.gc, th, f1);
+            if (c2.valid) Op::fetch_idx(a.rows, a.jmap, c2.gc, th, f2);
+            cen0 = issue(cur, f0, 0, cen0);
+            cen1 = issue(c1, f1, 1, cen0);
+        }
+        int g = 0;
+        while (cur.valid) {
+            // chunk g + 2's gathers, chunk g + 3's indices
+            cen2 = issue(c2, f2, (g + 2) % 3, cen1);
+            const ens::Cursor c3 = ens::next_cursor(c2, a, halves);
+            if (c3.valid) Op::fetch_idx(a.rows, a.jmap, c3.gc, th, f3);
+            asm volatile("cp.async.wait_group 2;" ::: "memory");
+            const int s = g % C::kStages;
+            if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) break;
+            typename Op::Set o;
+            Op::stage_read(stg0 + (g % 3) * Op::kStgBytes, ct, cen0, o);
+            Op::build(smem + s * C::kStageBytes, th, o);
+            tc::fence_async_smem();
+            __syncwarp();
+            if (lane == 0) ens::mbar_arrive(&full_bar[s]);
+            ++g;
+            cur = c1;
+            c1 = c2;
+            c2 = c3;
+            f2 = f3;
+            cen0 = cen1;
+            cen1 = cen2;
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+      } else {
         const typename Op::Thread th(threadIdx.x);
         ens::Cursor cur = ens::first_cursor(a, halves);
         typename Op::Fetch fx;         // indices of the step after the current one
@@ -271,6 +332,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             u = cur.u;
             if (!step(sb, sa, u)) break;
         }
+      }
     } else if (warp == C::kMmaWarp) {
         // =============================== MMA issuer ===============================
         if (lane == 0) {
