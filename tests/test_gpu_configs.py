@@ -7,11 +7,11 @@ N=40962, up to 100 steps).  This file runs the configured workloads themselves:
   four layouts, with and without RCM ordering: the library initialised from the
   reference's own PSMD_struct (oracle.Ref), eval_rhs against the reference's own
   eval_RHS_swe, and the 1000-step state against the oracle's 1000-step run.
-* N=655362 (level 8), FP64 and FP32: eval_rhs against the oracle and 20 RK4 steps
-  against the oracle's run.
+* N=655362 (level 8), FP64 and FP32, dt=60 s: eval_rhs against the oracle and the
+  configured 200 RK4 steps against the oracle's run.
 * N=163842 (level 7), 64 members, 3xTF32 batched form, 1000 steps at dt=120 s:
   h error of every member against the plain FP64 GPU run of that member, with
-  that plain run itself checked against the oracle for 20 steps.
+  that plain run itself checked against the oracle over the same 1000 steps.
 
 Bars and why:
 * FP64 states after 1000 steps, 1e-12 relative per field.  Two FP64 summation
@@ -22,7 +22,7 @@ Bars and why:
   the state by >1e-6 within a few steps).
 * FP64 eval_rhs, 1e-12 relative (the drop-in contract), and FP32 eval_rhs within
   the FP32 bound of the condition-normalised error (conftest.cond_err).
-* FP32 20-step states: within 4x the error the oracle's own FP32 restatement
+* FP32 200-step states: within 4x the error the oracle's own FP32 restatement
   makes against the FP64 oracle (two FP32 orders of one formula), and within the
   reference's FP32 verify tolerance, 4e-2 absolute (swe_config.h:80).
 * Batched h after 1000 steps: 1e-6 of max|h| for every member (the stated target
@@ -95,7 +95,7 @@ def model_l8():
     return m
 
 
-def test_n655362_fp64_eval_rhs_and_20_steps(plain, model_l8):
+def test_n655362_fp64_eval_rhs_and_200_steps(plain, model_l8):
     m = model_l8
     plain.init_model(m, "fp64")
     port = oracle.Port(m, "fp64")
@@ -104,15 +104,16 @@ def test_n655362_fp64_eval_rhs_and_20_steps(plain, model_l8):
     F_ref = port.eval_rhs(K)
     assert rel_err(F, F_ref).max() <= 1e-12
     assert cond_err(F, F_ref, m, K) <= 4e-16
+    assert m.dt == 60.0
     plain.set_state(m.H_init)
-    plain.step(20)
+    plain.step(200)
     H = plain.get_state().reshape(-1, 4)
-    err = rel_err(H, port.run(m.H_init, 20))
-    print(f"N=655362 FP64 20-step rel err per field {err}")
+    err = rel_err(H, port.run(m.H_init, 200))
+    print(f"N=655362 FP64 200-step rel err per field {err}")
     assert err.max() <= 1e-12
 
 
-def test_n655362_fp32_eval_rhs_and_20_steps(plain, model_l8):
+def test_n655362_fp32_eval_rhs_and_200_steps(plain, model_l8):
     m = model_l8
     plain.init_model(m, "fp32")
     K = _perturbed(m.H_init).astype(np.float32)
@@ -122,12 +123,12 @@ def test_n655362_fp32_eval_rhs_and_20_steps(plain, model_l8):
     F64 = port64.eval_rhs(K.astype(np.float64))
     assert (np.abs(F.reshape(-1, 4) - F64).max(0) / scale).max() <= 4e-6
     plain.set_state(m.H_init.astype(np.float32))
-    plain.step(20)
+    plain.step(200)
     H = plain.get_state().reshape(-1, 4).astype(np.float64)
-    H64 = port64.run(m.H_init, 20)
-    H32 = oracle.Port(m, "fp32").run(m.H_init.astype(np.float32), 20)
+    H64 = port64.run(m.H_init, 200)
+    H32 = oracle.Port(m, "fp32").run(m.H_init.astype(np.float32), 200)
     err, err32 = scaled_err(H, H64), scaled_err(H32, H64)
-    print(f"N=655362 FP32 20-step error per field {err}, FP32 oracle's {err32}")
+    print(f"N=655362 FP32 200-step error per field {err}, FP32 oracle's {err32}")
     assert err.max() <= 4 * err32.max()
     assert np.abs(H - H64).max() <= 4e-2
 
@@ -142,8 +143,9 @@ def test_n163842_b64_tf32x3_1000_steps_h_error_every_member(plain):
     # against the oracle (natural node order, as the batched form exchanges states)
     plain.init_model(m, "fp64")
     plain.set_state(H0[0])
-    plain.step(20)
-    err = rel_err(plain.get_state(), oracle.Port(m, "fp64").run(H0[0], 20))
+    plain.step(steps)
+    err = rel_err(plain.get_state(), oracle.Port(m, "fp64").run(H0[0], steps))
+    print(f"N=163842 plain FP64 {steps} steps vs oracle: rel err per field {err}")
     assert err.max() <= 1e-12, err
     ens = capi.Ensemble()
     try:
