@@ -231,7 +231,10 @@ int swe_selftest_wait_timeout(double limit_s, double* waited_s);
  * Precision: stencil products in 3xTF32 (or split BF16, see
  * swe_ens_set_precision) on tcgen05 with FP32 accumulation;
  * u, v, w and the stage states K in FP32; the RK4 accumulation of h (base
- * state and D register) in FP64; invariants in FP64. */
+ * state and D register) in FP64; invariants in FP64.
+ * Device memory: besides the member states (about 40 B per node and member),
+ * the static weights are kept split for the tensor cores, about 7 KB per node
+ * for the two tile shapes together (1.2 GB at N=163842). */
 int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int* idx,
                  const double* Dx, const double* Dy, const double* Dz, const double* L,
                  const double* x, const double* y, const double* z, const double* f,
@@ -251,14 +254,16 @@ int swe_ens_stage(int substep_id);
  * or 32) -- in the current precision on the live state, restores the state and
  * keeps the fastest.  ms_per_step[4] (may be NULL) receives the timings in the
  * order (tile, members per CTA) = (32, 64), (32, 32), (16, 64), (16, 32), -1
- * where a variant does not apply.  config[5] = {tile nodes, members per CTA,
- * largest neighbour set of a tile, tiles, precision}. */
+ * where a variant does not apply.  config[6] = {tile nodes, members per CTA,
+ * largest neighbour set of a tile, tiles, precision, 16-row chunks of
+ * neighbour rows over all tiles}. */
 int swe_ens_tune(double* ms_per_step);
 int swe_ens_config(int* config);
 /* Forces one variant (tile_nodes 32 or 16, members_per_cta 64 or 32). */
 int swe_ens_use_variant(int tile_nodes, int members_per_cta);
-/* Precision of the stencil products: 0 = 3xTF32 (default; hi and lo parts both
- * exact TF32, |x - hi - lo| <= 2^-22 |x|), 1 = split BF16 (2^-17), both with
+/* Precision of the stencil products: 0 = 3xTF32 (default; hi = x rounded to
+ * TF32, lo = x - hi kept in FP32 and read by the tensor core at TF32
+ * precision, |x - hi - lo| <= 2^-21 |x|), 1 = split BF16 (2^-17), both with
  * FP32 accumulation and the same FP64 h accumulation. */
 int swe_ens_set_precision(int precision);
 /* FP64 (mass, energy) per member, [members][2], definitions as swe_cuda_invariants;

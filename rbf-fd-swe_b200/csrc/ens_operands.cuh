@@ -1,7 +1,7 @@
 // Operand policies of the batched-ensemble kernel: how the converter threads
-// gather one 16-row chunk of a tile's neighbour rows and weights, split them
-// into hi / lo parts in the tensor core's shared-memory layout, and how the
-// MMA thread issues the chunk's three products.
+// gather one 16-row chunk of a tile's neighbour rows (and, for split BF16, its
+// weights), split them into hi / lo parts in the tensor core's shared-memory
+// layout, and how the MMA thread issues the chunk's three products.
 //
 //   Tf32x3: kind::tf32, hi = tf32(x) rounded to nearest, lo = x - hi kept in
 //           FP32 and read by the tensor core at TF32 precision
@@ -52,64 +52,55 @@ template <int T, int MPC, int PREC>
 struct Operands;
 
 // --------------------------------------------------------------------------------------
-// 3xTF32, tiles of T = 32 or 16 nodes (M = 4T = 128 or 64).  B thread: member-fields
-// 4q..4q+3 of rows 4kg..4kg+3.  A thread: node t, rows 4akg..4akg+3, operators
-// op0 .. op0 + kOps - 1 (kOps = 16 T / converter threads: 1, 2 or 4).
+// 3xTF32, tiles of T = 32 or 16 nodes (M = 4T = 128 or 64).  The A (weight) operand of
+// every chunk is static: it is split once at init into an image of the slot's A part
+// (a_offset below) and streamed into the slot by one bulk copy per chunk.  B thread:
+// member-fields 4q..4q+3 of rows 4kg..4kg+3.
 // --------------------------------------------------------------------------------------
 template <int T, int MPC>
 struct Operands<T, MPC, kTf32x3> {
     static constexpr int kN = 4 * MPC;
     static constexpr int kM = 4 * T;
     static constexpr int kConvThreads = 4 * MPC;
-    static constexpr int kOps = 16 * T / kConvThreads;
     static constexpr int kSboA = (kEnsKc / 4) * 128;
     static constexpr int kSboB = (kEnsKc / 4) * 128 + 16;
     static constexpr int kAHalf = (kM / 8) * kSboA;
     static constexpr int kBHalf = (kN / 8) * kSboB;
+    static constexpr int kABytes = 2 * kAHalf;                     // one chunk's A image: hi, then lo
     static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
     static constexpr int kStages = 2;
-    // staged gathers: per converter thread and chunk, 4 rows x 16 B of state and 4 rows x
-    // the thread's weights, in structure-of-arrays order (row-major over threads) so that
-    // each warp's shared-memory accesses are contiguous
-    static constexpr int kWBytes = 4 * kOps;                       // weight bytes per row and thread
-    static constexpr int kStgRows = 4 * kConvThreads * 16;
-    static constexpr int kStgBytes = kStgRows + 4 * kConvThreads * kWBytes;
+    // staged gathers: per converter thread and chunk, 4 rows x 16 B of state in
+    // structure-of-arrays order (row-major over threads) so that each warp's
+    // shared-memory accesses are contiguous
+    static constexpr int kStgBytes = 4 * kConvThreads * 16;
     static constexpr int kStgDepth = 3;                            // chunks in flight: g, g+1, g+2
     static_assert(T == 16 || T == 32, "tiles of 16 or 32 nodes");
-    static_assert(kOps == 1 || kOps == 2 || kOps == 4, "A build: T nodes x 4 row groups x 4 operators");
-    // the weights of the thread's operators: one, a pair or all four of (Dx, Dy, Dz, L)
-    using WT = typename std::conditional<kOps == 1, float, typename std::conditional<kOps == 2, float2, float4>::type>::type;
+
+    // Byte offset, within A_hi (and A_lo), of the 16-byte core row holding the weights
+    // of operator-node row r (r = T op + t) for the chunk rows 4 akg .. 4 akg + 3.
+    __host__ __device__ static constexpr int a_offset(int r, int akg) {
+        return (r >> 3) * kSboA + akg * 128 + (r & 7) * 16;
+    }
 
     struct Thread {
-        int quad, kg, at, akg, op0;
-        __device__ explicit Thread(int ct)
-            : quad(ct % MPC), kg(ct / MPC), at(ct % T), akg((ct / T) & 3), op0((ct / (4 * T)) * kOps) {}
+        int quad, kg;
+        __device__ explicit Thread(int ct) : quad(ct % MPC), kg(ct / MPC) {}
         __device__ int col() const { return 4 * quad; }
     };
     struct Fetch {
         int4 idx = make_int4(-1, -1, -1, -1);
-        uint32_t jj = 0xffffffffu;
     };
     struct Set {
         float4 x[4];          // 4 gathered rows x 4 member-fields
         float4 cen;           // centre state of the same member-fields
-        WT w[4];              // weights of the thread's operators for the 4 chunk rows
     };
 
-    __device__ static float wget(const WT& w, int q) {
-        if constexpr (kOps == 1) return w;
-        else if constexpr (kOps == 2) return q ? w.y : w.x;
-        else return q == 0 ? w.x : q == 1 ? w.y : q == 2 ? w.z : w.w;
-    }
-
-    __device__ static void fetch_idx(const int* rows, const uint32_t* jmap, int gc, const Thread& th, Fetch& f) {
+    __device__ static void fetch_idx(const int* rows, int gc, const Thread& th, Fetch& f) {
         f.idx = __ldg(reinterpret_cast<const int4*>(rows + gc * kEnsKc + 4 * th.kg));
-        f.jj = __ldg(jmap + (gc * 4 + th.akg) * T + th.at);
     }
-    // cp.async of this thread's gathered rows and weights of one chunk into staging
-    // buffer `stg`; weights of rows outside the node's stencil are zero-filled.
-    __device__ static void stage_issue(unsigned char* stg, int ct, const float* Kin, int mf, long col, const float4* W,
-                                       long node, const Thread& th, const Fetch& f) {
+    // cp.async of this thread's 4 gathered rows of one chunk into staging buffer `stg`
+    __device__ static void stage_issue(unsigned char* stg, int ct, const float* Kin, int mf, long col,
+                                       const Fetch& f) {
         const int r[4] = {f.idx.x, f.idx.y, f.idx.z, f.idx.w};
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -117,66 +108,16 @@ struct Operands<T, MPC, kTf32x3> {
             const float* src = Kin + (long)r[i] * mf + col;
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
         }
-        unsigned char* wst = stg + kStgRows;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const uint32_t j = (f.jj >> (8 * i)) & 0xffu;
-            const uint32_t dst = tc::smem_u32(wst + (i * kConvThreads + ct) * kWBytes);
-            // rows outside the stencil copy nothing (zero fill) from a valid address
-            const float* src = j != 0xffu ? reinterpret_cast<const float*>(W + node * 32 + j) + th.op0
-                                          : reinterpret_cast<const float*>(W);
-            const int n = j != 0xffu ? kWBytes : 0;
-            if constexpr (kWBytes == 16)
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
-            else if constexpr (kWBytes == 8)
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
-            else
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
-        }
     }
     __device__ static void stage_read(const unsigned char* stg, int ct, const float4& cen, Set& o) {
 #pragma unroll
         for (int i = 0; i < 4; ++i) o.x[i] = *reinterpret_cast<const float4*>(stg + (i * kConvThreads + ct) * 16);
         o.cen = cen;
-        const unsigned char* wst = stg + kStgRows;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) o.w[i] = *reinterpret_cast<const WT*>(wst + (i * kConvThreads + ct) * kWBytes);
     }
-    __device__ static void fetch_ops(const float* Kin, int mf, long col, const float4* W, long node, const float* cen_row,
-                                     const Thread& th, const Fetch& f, Set& o, const Set& prev) {
-        const int r[4] = {f.idx.x, f.idx.y, f.idx.z, f.idx.w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) o.x[i] = ldg_f4(Kin + (long)r[i] * mf + col);
-        o.cen = cen_row ? ldg_f4(cen_row + col) : prev.cen;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const uint32_t j = (f.jj >> (8 * i)) & 0xffu;
-            if constexpr (kOps == 4) {
-                o.w[i] = j != 0xffu ? __ldg(W + node * 32 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
-            } else {
-                const WT* wp = reinterpret_cast<const WT*>(W + node * 32 + j) + th.op0 / kOps;
-                o.w[i] = j != 0xffu ? __ldg(wp) : WT{};
-            }
-        }
-    }
+    // the B operand of one chunk: centred rows split into hi and lo
     __device__ static void build(unsigned char* slot, const Thread& th, const Set& o) {
-        unsigned char* A_hi = slot;
-        unsigned char* A_lo = slot + kAHalf;
         unsigned char* B_hi = slot + 2 * kAHalf;
         unsigned char* B_lo = B_hi + kBHalf;
-        // A: one 16-byte core row (4 chunk rows) of (operator, node) per operator handled
-#pragma unroll
-        for (int q = 0; q < kOps; ++q) {
-            const int r = T * (th.op0 + q) + th.at;
-            float4 hi, lo;
-            tc::tf32_split_lo_fp32(wget(o.w[0], q), hi.x, lo.x);
-            tc::tf32_split_lo_fp32(wget(o.w[1], q), hi.y, lo.y);
-            tc::tf32_split_lo_fp32(wget(o.w[2], q), hi.z, lo.z);
-            tc::tf32_split_lo_fp32(wget(o.w[3], q), hi.w, lo.w);
-            const uint32_t off = (r >> 3) * kSboA + th.akg * 128 + (r & 7) * 16;
-            *reinterpret_cast<float4*>(A_hi + off) = hi;
-            *reinterpret_cast<float4*>(A_lo + off) = lo;
-        }
         // B: each member-field's 4 rows are one 16-byte core row
         const float xv[4][4] = {{o.x[0].x, o.x[0].y, o.x[0].z, o.x[0].w},
                                 {o.x[1].x, o.x[1].y, o.x[1].z, o.x[1].w},

@@ -136,13 +136,48 @@ struct Variant {
 
 // Device copies of one tile shape's tables.
 struct DevTables {
-    int ntiles = 0, max_rows = 0;
+    int ntiles = 0, max_rows = 0, nchunks = 0;
     int *row_off = nullptr, *rows = nullptr, *centre = nullptr;
     uint32_t* jmap = nullptr;
+    unsigned char* aimg = nullptr;   // [chunk] 3xTF32 A operand image (hi, then lo), 512 T bytes a chunk
 };
 constexpr int kEnsShapes = 2;          // tiles of 32 and 16 nodes
 constexpr int kEnsShapeNodes[kEnsShapes] = {32, 16};
 constexpr int kEnsVariants = 4;        // (32, 64), (32, 32), (16, 64), (16, 32)
+
+// The 3xTF32 A operand of every chunk, split once (the weights are static): one
+// thread per (chunk, operator-node row r = T op + t, row group akg) writes the 4
+// chunk rows' weights of that row as one 16-byte core row of the hi image and one
+// of the lo image (zero where a chunk row is not in node t's stencil).
+template <int T>
+__global__ void ens_build_aimg(const uint32_t* __restrict__ jmap, const int* __restrict__ chunk_tile,
+                              const float4* __restrict__ W, int n, int nchunks, unsigned char* __restrict__ img) {
+    using Op = ens::Operands<T, 32, kTf32x3>;   // the A layout does not depend on the members per CTA
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)nchunks * 16 * T) return;
+    const int akg = (int)(t & 3);
+    const int r = (int)((t >> 2) % (4 * T));
+    const long gc = (t >> 2) / (4 * T);
+    const int op = r / T, at = r % T;
+    const long node = (long)chunk_tile[gc] * T + at;
+    const uint32_t jj = jmap[(gc * 4 + akg) * T + at];
+    float v[4];
+    for (int i = 0; i < 4; ++i) {
+        const uint32_t j = (jj >> (8 * i)) & 0xffu;
+        v[i] = (j != 0xffu && node < n) ? reinterpret_cast<const float*>(W + node * 32 + j)[op] : 0.f;
+    }
+    float4 hi, lo;
+    tc::tf32_split_lo_fp32(v[0], hi.x, lo.x);
+    tc::tf32_split_lo_fp32(v[1], hi.y, lo.y);
+    tc::tf32_split_lo_fp32(v[2], hi.z, lo.z);
+    tc::tf32_split_lo_fp32(v[3], hi.w, lo.w);
+    unsigned char* base = img + (size_t)gc * Op::kABytes + Op::a_offset(r, akg);
+    *reinterpret_cast<float4*>(base) = hi;
+    *reinterpret_cast<float4*>(base + Op::kAHalf) = lo;
+}
+
+static_assert(ens::Operands<32, 64, kTf32x3>::kABytes == 512 * 32 && ens::Operands<16, 64, kTf32x3>::kABytes == 512 * 16,
+              "A image: 512 bytes per tile node and chunk");
 
 __global__ void ens_invariants_kernel(const float* __restrict__ H32, const double* __restrict__ Hh,
                                       const float4* __restrict__ PT, int n, int members, double gh0,
@@ -227,7 +262,7 @@ struct Ensemble {
         void* ps[] = {perm, PT, RS, H32, D32, Ka, Kb, F, Kx, Hh, Dh, io, inv, bkH32, bkHh, err, W};
         for (void* p : ps) if (p) cudaFree(p);
         for (DevTables& t : tabs) {
-            void* tp[] = {t.row_off, t.rows, t.centre, t.jmap};
+            void* tp[] = {t.row_off, t.rows, t.centre, t.jmap, t.aimg};
             for (void* p : tp) if (p) cudaFree(p);
             t = DevTables{};
         }
@@ -251,7 +286,7 @@ struct Ensemble {
         a.members = members;
         a.units = tb.ntiles * (members / mpc);
         a.mf = mf;
-        a.row_off = tb.row_off; a.rows = tb.rows; a.jmap = tb.jmap; a.W = W;
+        a.row_off = tb.row_off; a.rows = tb.rows; a.jmap = tb.jmap; a.W = W; a.Aimg = tb.aimg;
         a.centre = tb.centre;
         a.PT = PT;
         a.RS = RS;
@@ -482,12 +517,39 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
         DevTables& d = E.tabs[sh];
         d.ntiles = tbs[sh].ntiles;
         d.max_rows = tbs[sh].max_rows;
+        d.nchunks = tbs[sh].nchunks;
         SWE_TRY(upload(&d.row_off, tbs[sh].row_off));
         SWE_TRY(upload(&d.rows, tbs[sh].rows));
         SWE_TRY(upload(&d.jmap, tbs[sh].jmap));
         SWE_TRY(upload(&d.centre, tbs[sh].centre));
     }
     SWE_TRY(upload(reinterpret_cast<float**>(&E.W), w));
+    // 3xTF32 A images of both tile shapes (about 4 KB per node for 32-node tiles,
+    // 3 KB for 16-node tiles): built on the device from the tables and the weights
+    for (int sh = 0; sh < kEnsShapes; ++sh) {
+        const int T = kEnsShapeNodes[sh];
+        const TileTables& tb = tbs[sh];
+        std::vector<int> chunk_tile(tb.nchunks);
+        for (int tile = 0; tile < tb.ntiles; ++tile)
+            for (int c = tb.row_off[tile] / kEnsKc; c < tb.row_off[tile + 1] / kEnsKc; ++c) chunk_tile[c] = tile;
+        int* dct = nullptr;
+        SWE_TRY(upload(&dct, chunk_tile));
+        const size_t bytes = (size_t)tb.nchunks * 512 * T;
+        const int rc = [&]() -> int {
+            SWE_CUDA_TRY(cudaMalloc(&E.tabs[sh].aimg, std::max<size_t>(bytes, 16)));
+            const long work = (long)tb.nchunks * 16 * T;
+            const int blocks = (int)std::max<long>(1, (work + 255) / 256);
+            if (T == 32) ens_build_aimg<32><<<blocks, 256, 0, E.stream>>>(E.tabs[sh].jmap, dct, E.W, n, tb.nchunks,
+                                                                            E.tabs[sh].aimg);
+            else ens_build_aimg<16><<<blocks, 256, 0, E.stream>>>(E.tabs[sh].jmap, dct, E.W, n, tb.nchunks,
+                                                                    E.tabs[sh].aimg);
+            SWE_CUDA_TRY(cudaGetLastError());
+            SWE_CUDA_TRY(cudaStreamSynchronize(E.stream));
+            return SWE_OK;
+        }();
+        cudaFree(dct);
+        if (rc != SWE_OK) return rc;
+    }
     for (float** p : {&E.H32, &E.D32, &E.Ka, &E.Kb, &E.F, &E.Kx, &E.bkH32}) SWE_CUDA_TRY(cudaMalloc(p, s32));
     for (double** p : {&E.Hh, &E.Dh, &E.bkHh}) SWE_CUDA_TRY(cudaMalloc(p, s64));
     SWE_CUDA_TRY(cudaMalloc(&E.io, (size_t)n * members * 4 * sizeof(double)));
@@ -627,6 +689,7 @@ int swe_ens_config(int* out) {
     out[2] = tb.max_rows;
     out[3] = tb.ntiles;
     out[4] = g_ens.prec;
+    out[5] = tb.nchunks;
     return SWE_OK;
 }
 

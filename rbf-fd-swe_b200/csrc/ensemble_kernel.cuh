@@ -26,16 +26,21 @@
 //
 // Persistent, warp-specialised CTA (one per SM; it owns all of tensor memory):
 //   * converter warps (MPC/8): for each 16-row chunk of K they gather the rows
-//     and weights (3xTF32: async copies into a staging buffer issued two chunks
-//     ahead, three buffers deep, so that no register waits on a gather; split
-//     BF16: 16-byte loads one chunk ahead into a ping-pong register set),
-//     centre and split them into the B operand, and write the matching A chunk
-//     densely, one 16-byte core row (4 chunk rows of one operator and node) per
-//     store, from a map of chunk rows to stencil slots; a ring of slots (2 for
-//     3xTF32, whose staging takes the third slot's shared memory) hands chunks to
-//   * the MMA warp: one thread issues the chunk's 3 products (128 x N x 16)
-//     into one of two TMEM accumulators and commits each chunk to the
-//     slot's "empty" barrier and each tile to the accumulator's "full" barrier;
+//     (3xTF32: async copies into a staging buffer issued two chunks ahead, three
+//     buffers deep, so that no register waits on a gather; split BF16: 16-byte
+//     loads one chunk ahead into a ping-pong register set) and centre and split
+//     them into the B operand.  Split BF16 converters also gather the weights and
+//     write the matching A chunk densely, one 16-byte core row (8 chunk rows of
+//     one operator and node) per store, from a map of chunk rows to stencil slots;
+//   * the A producer warp (3xTF32): the A chunks are static, so they are split
+//     once at init into an image of the slot's A part; one thread streams each
+//     chunk's image into its slot with one bulk copy (and prefetches the image
+//     two chunks ahead into L2);
+//   * a ring of slots (2 for 3xTF32, whose staging takes the third slot's shared
+//     memory) hands chunks to the MMA warp: one thread issues the chunk's 3
+//     products (128 x N x 16) into one of two TMEM accumulators once the
+//     converters and the A copy have filled the slot, and commits each chunk to
+//     the slot's "empty" barrier and each tile to the accumulator's "full" barrier;
 //   * 8 epilogue warps (two per TMEM lane quarter): tcgen05.ld the accumulator
 //     32 columns at a time, transpose (op, node) rows to (node, member) sets
 //     through shared memory, add the centre back, evaluate the pointwise part
@@ -66,7 +71,8 @@ struct EnsCfg {
     static constexpr int kConvThreads = 32 * kConvWarps;
     static constexpr int kMmaWarp = kConvWarps;
     static constexpr int kEpiWarp0 = kConvWarps + 1;
-    static constexpr int kThreads = 32 * (kConvWarps + 1 + kEnsEpiWarps);
+    static constexpr int kProdWarp = kEpiWarp0 + kEnsEpiWarps;   // A producer (idle for split BF16)
+    static constexpr int kThreads = 32 * (kConvWarps + 2 + kEnsEpiWarps);
     static constexpr int kStages = Op::kStages;            // ring slots
     static constexpr int kStageBytes = Op::kStageBytes;
     static constexpr int kXchStride = 36;                  // floats per (op, node) row; 9 x 16 B
@@ -92,6 +98,7 @@ struct EnsArgs {
     const int* rows;       // unique neighbour rows of each tile, ascending; padded with the centring node
     const uint32_t* jmap;  // [chunk][row group][node t]: stencil slot of each of the 4 rows, 255 = none
     const float4* W;       // [n][32] (Dx, Dy, Dz, L) per stencil slot
+    const unsigned char* Aimg;   // 3xTF32: [chunk] A operand image (hi, then lo) in the slot's layout
     const int* centre;     // [ntiles] node whose state centres the tile
     const float4* PT;      // [n][5] pointwise record (20 floats)
     const float4* RS;      // [n] row sums of the four operators
@@ -197,7 +204,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
     using C = EnsCfg<T, MPC, PREC>;
     using Op = typename C::Op;
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full_bar[C::kStages], empty_bar[C::kStages];
+    __shared__ __align__(8) uint64_t full_bar[C::kStages], empty_bar[C::kStages], afull_bar[C::kStages];
     __shared__ __align__(8) uint64_t accf_bar[2], acce_bar[2], tile_bar[2], fin_bar;
     __shared__ uint32_t tmem_s;
     __shared__ int abort_s;
@@ -209,6 +216,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
         for (int s = 0; s < C::kStages; ++s) {
             tc::mbar_init(&full_bar[s], C::kConvWarps);
             tc::mbar_init(&empty_bar[s], 1);
+            tc::mbar_init(&afull_bar[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
             tc::mbar_init(&accf_bar[b], 1);
@@ -231,8 +239,8 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
     if (warp < C::kConvWarps) {
         // =============================== converters ===============================
       if constexpr (PREC == kTf32x3) {
-        // staged gathers: chunk g + 2's rows and weights are in flight (cp.async) while
-        // chunk g is built from its staging buffer
+        // staged gathers: chunk g + 2's rows are in flight (cp.async) while chunk g is
+        // built from its staging buffer
         const typename Op::Thread th(threadIdx.x);
         const int ct = threadIdx.x;
         unsigned char* stg0 = smem + C::kStgOff;
@@ -249,7 +257,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             if (p.valid) {
                 const int tile = p.u / halves;
                 const long col = (long)(p.u % halves) * C::kN + th.col();
-                Op::stage_issue(stg0 + slot * Op::kStgBytes, ct, a.Kin, a.mf, col, a.W, (long)tile * T + th.at, th, f);
+                Op::stage_issue(stg0 + slot * Op::kStgBytes, ct, a.Kin, a.mf, col, f);
                 if (p.gc == p.gc0) c = ens::ldg_f4(a.Kin + (long)__ldg(a.centre + tile) * a.mf + col);
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
@@ -257,9 +265,9 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
         };
         if (cur.valid) {
             typename Op::Fetch f0, f1;
-            Op::fetch_idx(a.rows, a.jmap, cur.gc, th, f0);
-            if (c1.valid) Op::fetch_idx(a.rows, a.jmap, c1.gc, th, f1);
-            if (c2.valid) Op::fetch_idx(a.rows, a.jmap, c2.gc, th, f2);
+            Op::fetch_idx(a.rows, cur.gc, th, f0);
+            if (c1.valid) Op::fetch_idx(a.rows, c1.gc, th, f1);
+            if (c2.valid) Op::fetch_idx(a.rows, c2.gc, th, f2);
             cen0 = issue(cur, f0, 0, cen0);
             cen1 = issue(c1, f1, 1, cen0);
         }
@@ -268,7 +276,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             // chunk g + 2's gathers, chunk g + 3's indices
             cen2 = issue(c2, f2, (g + 2) % 3, cen1);
             const ens::Cursor c3 = ens::next_cursor(c2, a, halves);
-            if (c3.valid) Op::fetch_idx(a.rows, a.jmap, c3.gc, th, f3);
+            if (c3.valid) Op::fetch_idx(a.rows, c3.gc, th, f3);
             asm volatile("cp.async.wait_group 2;" ::: "memory");
             const int s = g % C::kStages;
             if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) break;
@@ -348,6 +356,8 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                 for (int gc = gc0; gc < gc1; ++gc, ++g) {
                     const int s = g % C::kStages;
                     if (!ens::wait(&full_bar[s], (g / C::kStages) & 1, abort_v, a.err, 5)) { ok = false; break; }
+                    if constexpr (PREC == kTf32x3)
+                        if (!ens::wait(&afull_bar[s], (g / C::kStages) & 1, abort_v, a.err, 9)) { ok = false; break; }
                     tc::fence_after_sync();
                     Op::issue(tc::smem_u32(smem + s * C::kStageBytes), d, gc == gc0);
                     tc::mma_commit(&empty_bar[s]);
@@ -361,6 +371,30 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             if (!tc::mbar_wait_bounded(&fin_bar, 0, kEnsWaitTries)) {
                 *abort_v = 1;
                 atomicExch(a.err, 6);
+            }
+        }
+        __syncwarp();
+    } else if (warp == C::kProdWarp) {
+        // ====================== A operand producer (3xTF32) ======================
+        if constexpr (PREC == kTf32x3) {
+            if (lane == 0) {
+                constexpr uint32_t kABytes = Op::kABytes;
+                ens::Cursor cur = ens::first_cursor(a, halves);
+                ens::Cursor pf = ens::next_cursor(ens::next_cursor(cur, a, halves), a, halves);
+                int g = 0;
+                while (cur.valid) {
+                    const int s = g % C::kStages;
+                    if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 10)) break;
+                    tc::mbar_arrive_expect_tx(&afull_bar[s], kABytes);
+                    tc::bulk_g2s(smem + s * C::kStageBytes, a.Aimg + (size_t)cur.gc * kABytes, kABytes, &afull_bar[s]);
+                    if (pf.valid) prefetch_l2_bulk(a.Aimg + (size_t)pf.gc * kABytes, kABytes);
+                    ++g;
+                    cur = ens::next_cursor(cur, a, halves);
+                    pf = ens::next_cursor(pf, a, halves);
+                }
+                // the copies of the last chunks land before the CTA ends, consumed or not
+                for (int k = g > C::kStages ? g - C::kStages : 0; k < g; ++k)
+                    tc::mbar_wait_bounded(&afull_bar[k % C::kStages], (k / C::kStages) & 1, kEnsWaitTries);
             }
         }
         __syncwarp();
@@ -504,18 +538,25 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
         };
         constexpr int kCh = C::kN / 64;          // chunks per group per tile
         ens::EpiSet sa;
-        if (et == 0 && blockIdx.x < a.units) issue_tile(blockIdx.x, 0);
+        // pend: the iteration whose tile copy thread 0 has issued and not yet seen land
+        int pend = -1;
+        if (et == 0 && blockIdx.x < a.units) {
+            issue_tile(blockIdx.x, 0);
+            pend = 0;
+        }
         int it = 0;
         for (int u = blockIdx.x; u < a.units; u += gridDim.x, ++it) {
             const int ab = it & 1;
             const bool got = ens::wait(&accf_bar[ab], (it >> 1) & 1, abort_v, a.err, 7) &&
                              ens::wait(&tile_bar[it & 1], (it >> 1) & 1, abort_v, a.err, 8);
+            if (got && pend == it) pend = -1;
             // every epilogue thread is done with the previous tile (and its tile buffer)
             if (!ens::named_and(4, 32 * kEnsEpiWarps, got && !*abort_v)) break;
             tc::fence_after_sync();
             if (et == 0 && u + (int)gridDim.x < a.units) {
                 tc::fence_async_smem();   // the buffer's earlier reads come before the copy's writes
                 issue_tile(u + gridDim.x, (it + 1) & 1);
+                pend = it + 1;
             }
 #pragma unroll 1
             for (int c = 0; c < kCh; ++c) {
@@ -528,6 +569,8 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&acce_bar[ab]);
         }
+        // after an abort, a tile copy still in flight lands before the CTA ends
+        if (pend >= 0) tc::mbar_wait_bounded(&tile_bar[pend & 1], (pend >> 1) & 1, kEnsWaitTries);
     }
 
     tc::fence_before_sync();

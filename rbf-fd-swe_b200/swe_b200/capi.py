@@ -358,11 +358,11 @@ class Ensemble:
         check("swe_ens_set_precision", self.lib.swe_ens_set_precision(self.PRECISIONS.index(name)))
 
     def config(self) -> dict:
-        out = np.zeros(5, dtype=np.int32)
+        out = np.zeros(6, dtype=np.int32)
         check("swe_ens_config", self.lib.swe_ens_config(_p(out)))
         return {"tile_nodes": int(out[0]), "members_per_cta": int(out[1]),
                 "max_rows_per_tile": int(out[2]), "tiles": int(out[3]),
-                "precision": self.PRECISIONS[int(out[4])]}
+                "precision": self.PRECISIONS[int(out[4])], "chunks": int(out[5])}
 
     def invariants(self) -> np.ndarray:
         """FP64 (mass, energy) per member; raises SweError (SWE_ERR_NONFINITE) naming the first
