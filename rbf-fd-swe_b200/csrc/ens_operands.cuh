@@ -11,7 +11,8 @@
 //           half the shared-memory bytes of Tf32x3 and twice the tensor rate.
 //
 // Padding rows of a tile's neighbour list name the tile's centring node, so their
-// centred values are exactly zero (their weights are zero as well).
+// centred values are exactly zero (their weights are zero as well).  Every tile has
+// at least one: with 3xTF32 its last padding row is the add-back row (see build).
 //
 // Both are K-major without swizzle: 8-row x 16-byte core matrices, LBO = 128
 // (the next core matrix along K), SBO = the stride between 8-row groups.  The
@@ -31,6 +32,19 @@ constexpr int kEnsTileNodes = 32;   // nodes per tile of the default shape (M = 
 constexpr int kEnsKc = 16;          // neighbour rows per pipeline chunk
 
 enum EnsPrecision { kTf32x3 = 0, kBf16x3 = 1 };
+
+// Row of the A operand (and TMEM lane of the accumulator) that holds operator op of
+// tile node t: each 32-lane quarter of tensor memory holds T/4 consecutive tile nodes
+// with their four operators in adjacent lanes (lanes 0..15 of each quarter when
+// M = 64), so that one epilogue warp reads all four operators of its nodes.
+template <int T>
+__host__ __device__ constexpr int ens_a_row(int op, int t) {
+    return T * (t / (T / 4)) + 4 * (t % (T / 4)) + op;
+}
+template <int T>
+__host__ __device__ constexpr int ens_a_row_op(int r) { return r & 3; }
+template <int T>
+__host__ __device__ constexpr int ens_a_row_node(int r) { return (r / T) * (T / 4) + ((r % T) >> 2); }
 
 struct EnsArgs;
 
@@ -114,10 +128,14 @@ struct Operands<T, MPC, kTf32x3> {
         for (int i = 0; i < 4; ++i) o.x[i] = *reinterpret_cast<const float4*>(stg + (i * kConvThreads + ct) * 16);
         o.cen = cen;
     }
-    // the B operand of one chunk: centred rows split into hi and lo
-    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o) {
+    // The B operand of one chunk: centred rows split into hi and lo.  Row 15 of a
+    // unit's last chunk (last = true) is its add-back row: it carries the centre state
+    // itself, not centred, and its A weights are the operators' row sums, so the
+    // accumulator receives c * sum_k W with the stencil sums.
+    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o, bool last) {
         unsigned char* B_hi = slot + 2 * kAHalf;
         unsigned char* B_lo = B_hi + kBHalf;
+        const bool keep15 = last && th.kg == 3;
         // B: each member-field's 4 rows are one 16-byte core row
         const float xv[4][4] = {{o.x[0].x, o.x[0].y, o.x[0].z, o.x[0].w},
                                 {o.x[1].x, o.x[1].y, o.x[1].z, o.x[1].w},
@@ -131,6 +149,7 @@ struct Operands<T, MPC, kTf32x3> {
             float y[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) y[i] = xv[i][j] - cv[j];
+            if (keep15) y[3] = xv[3][j];
             tc::tf32_split_lo_fp32(y[0], hi.x, lo.x);
             tc::tf32_split_lo_fp32(y[1], hi.y, lo.y);
             tc::tf32_split_lo_fp32(y[2], hi.z, lo.z);
@@ -237,7 +256,7 @@ struct Operands<32, MPC, kBf16x3> {
             hi.y = bf16x2_split(v[2], v[3], lo.y);
             hi.z = bf16x2_split(v[4], v[5], lo.z);
             hi.w = bf16x2_split(v[6], v[7], lo.w);
-            const int r = 32 * op + th.at;
+            const int r = ens_a_row<32>(op, th.at);
             const uint32_t off = (r >> 3) * kSboA + th.akh * 128 + (r & 7) * 16;
             *reinterpret_cast<uint4*>(A_hi + off) = hi;
             *reinterpret_cast<uint4*>(A_lo + off) = lo;

@@ -92,7 +92,8 @@ TileTables build_tiles(int T, int n, int nnbr, const std::vector<int>& ridx, con
         std::sort(u.begin(), u.end());
         u.erase(std::unique(u.begin(), u.end()), u.end());
         tb.max_rows = std::max(tb.max_rows, (int)u.size());
-        const int nch = ((int)u.size() + kEnsKc - 1) / kEnsKc;
+        // at least one padding row: the last one is the 3xTF32 add-back row
+        const int nch = ((int)u.size() + 1 + kEnsKc - 1) / kEnsKc;
         const int kpad = nch * kEnsKc;
         // padding rows: the centring node (chosen below), whose centred state is exactly 0
         const size_t pad0 = tb.rows.size() + u.size();
@@ -146,26 +147,31 @@ constexpr int kEnsShapeNodes[kEnsShapes] = {32, 16};
 constexpr int kEnsVariants = 4;        // (32, 64), (32, 32), (16, 64), (16, 32)
 
 // The 3xTF32 A operand of every chunk, split once (the weights are static): one
-// thread per (chunk, operator-node row r = T op + t, row group akg) writes the 4
-// chunk rows' weights of that row as one 16-byte core row of the hi image and one
-// of the lo image (zero where a chunk row is not in node t's stencil).
+// thread per (chunk, A row r = ens_a_row(op, t), row group akg) writes the 4 chunk
+// rows' weights of that row as one 16-byte core row of the hi image and one of the
+// lo image (zero where a chunk row is not in node t's stencil).  Row 15 of a tile's
+// last chunk is the add-back row: its weights are the operators' row sums.
 template <int T>
 __global__ void ens_build_aimg(const uint32_t* __restrict__ jmap, const int* __restrict__ chunk_tile,
-                              const float4* __restrict__ W, int n, int nchunks, unsigned char* __restrict__ img) {
+                              const int* __restrict__ row_off, const float4* __restrict__ W,
+                              const float4* __restrict__ RS, int n, int nchunks, unsigned char* __restrict__ img) {
     using Op = ens::Operands<T, 32, kTf32x3>;   // the A layout does not depend on the members per CTA
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)nchunks * 16 * T) return;
     const int akg = (int)(t & 3);
     const int r = (int)((t >> 2) % (4 * T));
     const long gc = (t >> 2) / (4 * T);
-    const int op = r / T, at = r % T;
-    const long node = (long)chunk_tile[gc] * T + at;
+    const int op = ens_a_row_op<T>(r), at = ens_a_row_node<T>(r);
+    const int tile = chunk_tile[gc];
+    const long node = (long)tile * T + at;
     const uint32_t jj = jmap[(gc * 4 + akg) * T + at];
     float v[4];
     for (int i = 0; i < 4; ++i) {
         const uint32_t j = (jj >> (8 * i)) & 0xffu;
         v[i] = (j != 0xffu && node < n) ? reinterpret_cast<const float*>(W + node * 32 + j)[op] : 0.f;
     }
+    if (akg == 3 && (gc + 1) * kEnsKc == row_off[tile + 1] && node < n)
+        v[3] = reinterpret_cast<const float*>(RS + node)[op];
     float4 hi, lo;
     tc::tf32_split_lo_fp32(v[0], hi.x, lo.x);
     tc::tf32_split_lo_fp32(v[1], hi.y, lo.y);
@@ -539,10 +545,11 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
             SWE_CUDA_TRY(cudaMalloc(&E.tabs[sh].aimg, std::max<size_t>(bytes, 16)));
             const long work = (long)tb.nchunks * 16 * T;
             const int blocks = (int)std::max<long>(1, (work + 255) / 256);
-            if (T == 32) ens_build_aimg<32><<<blocks, 256, 0, E.stream>>>(E.tabs[sh].jmap, dct, E.W, n, tb.nchunks,
-                                                                            E.tabs[sh].aimg);
-            else ens_build_aimg<16><<<blocks, 256, 0, E.stream>>>(E.tabs[sh].jmap, dct, E.W, n, tb.nchunks,
-                                                                    E.tabs[sh].aimg);
+            const DevTables& d = E.tabs[sh];
+            if (T == 32)
+                ens_build_aimg<32><<<blocks, 256, 0, E.stream>>>(d.jmap, dct, d.row_off, E.W, E.RS, n, tb.nchunks, d.aimg);
+            else
+                ens_build_aimg<16><<<blocks, 256, 0, E.stream>>>(d.jmap, dct, d.row_off, E.W, E.RS, n, tb.nchunks, d.aimg);
             SWE_CUDA_TRY(cudaGetLastError());
             SWE_CUDA_TRY(cudaStreamSynchronize(E.stream));
             return SWE_OK;

@@ -7,9 +7,10 @@
 // unique neighbour rows per tile on the icosahedral grids).  For one tile the
 // stencil products of a block of MPC members are one dense contraction
 //
-//     D[32*op + t][mf] = sum_k  W_op(node t, row_k) * (X[row_k][mf] - c[mf])
+//     D[row(op, t)][mf] = sum_k  W_op(node t, row_k) * (X[row_k][mf] - c[mf])
 //
-// M = 128 (4 operators Dx, Dy, Dz, L x 32 nodes), N = 4*MPC member-fields,
+// M = 128 (4 operators Dx, Dy, Dz, L x 32 nodes; row(op, t) = ens_a_row puts the
+// four operators of a node in adjacent rows), N = 4*MPC member-fields,
 // K = the tile's unique neighbour rows (W is zero where row_k is not in node
 // t's stencil).  Each unique row is gathered once per tile instead of once per
 // stencil slot.
@@ -18,10 +19,12 @@
 // + A_lo B_hi accumulates in FP32 in tensor memory; the split is 3xTF32
 // (|x - hi - lo| <= 2^-21 |x| as the tensor core reads it) or split BF16
 // (2^-17), see ens_operands.cuh.  The gathered states are
-// centred on the state of one node of the tile (c[mf]) before the split;
-// c * sum_k W (row sums of the FP64 weights) is added back in the epilogue.  Derivative and hyperviscosity weights annihilate constants,
-// so the added-back term is small and the cancellation that limits FP32
-// stencil sums mostly disappears.  The RK4 accumulation of h (base state and
+// centred on the state of one node of the tile (c[mf]) before the split, and
+// c * sum_k W (row sums of the FP64 weights) is added back: with 3xTF32 by the
+// MMA itself, through one more K row whose B values are c and whose A weights
+// are the row sums; with split BF16 in the epilogue.  Derivative and
+// hyperviscosity weights annihilate constants, so the added-back term is small
+// and the cancellation that limits FP32 stencil sums mostly disappears.  The RK4 accumulation of h (base state and
 // D register) is FP64; u, v, w and every stage state K are FP32.
 //
 // Persistent, warp-specialised CTA (one per SM; it owns all of tensor memory):
@@ -41,12 +44,13 @@
 //     products (128 x N x 16) into one of two TMEM accumulators once the
 //     converters and the A copy have filled the slot, and commits each chunk to
 //     the slot's "empty" barrier and each tile to the accumulator's "full" barrier;
-//   * 8 epilogue warps (two per TMEM lane quarter): tcgen05.ld the accumulator
-//     32 columns at a time, transpose (op, node) rows to (node, member) sets
-//     through shared memory, add the centre back, evaluate the pointwise part
-//     of eval_RHS_swe (rk4_rbffd_swe.c:320-353) and apply the RK_substep
-//     combine (:30-72) for one (node, member) per thread, while the tensor
-//     cores already fill the other accumulator.
+//   * 8 epilogue warps (two per TMEM lane quarter, each quarter holding T/4
+//     nodes with their four operators): each warp tcgen05.ld's its quarter 32
+//     columns at a time, transposes its (node, operator) rows to (node, member)
+//     sets through its own shared-memory rows (no barrier between warps),
+//     evaluates the pointwise part of eval_RHS_swe (rk4_rbffd_swe.c:320-353)
+//     and applies the RK_substep combine (:30-72) for one (node, member) per
+//     thread and pair, while the tensor cores already fill the other accumulator.
 // Every mbarrier wait is bounded; a timeout sets an error word and a shared
 // abort flag that makes every role leave its loop.
 #pragma once
@@ -76,12 +80,12 @@ struct EnsCfg {
     static constexpr int kStages = Op::kStages;            // ring slots
     static constexpr int kStageBytes = Op::kStageBytes;
     static constexpr int kXchStride = 36;                  // floats per (op, node) row; 9 x 16 B
-    static constexpr int kXchGroupFloats = 4 * T * kXchStride;
+    static constexpr int kXchWarpFloats = T * kXchStride;  // an epilogue warp's exchange rows
     static constexpr int kTbRs = T * kPointStride * 4;     // per-tile buffer: PT, row sums, centre
     static constexpr int kTbCen = kTbRs + T * 16;
     static constexpr int kPairs = T / 16;                  // (node, member) pairs per epilogue thread and chunk
     static constexpr int kTileBuf = (kTbCen + kN * 4 + 127) / 128 * 128;
-    static constexpr int kStgOff = kStages * kStageBytes + 2 * kXchGroupFloats * 4 + 2 * kTileBuf;
+    static constexpr int kStgOff = kStages * kStageBytes + kEnsEpiWarps * kXchWarpFloats * 4 + 2 * kTileBuf;
     static constexpr int kSmem = kStgOff + Op::kStgDepth * Op::kStgBytes;
     static constexpr int kTmemCols = (2 * kN <= 256) ? 256 : 512;
     static_assert(kConvThreads == Op::kConvThreads, "converter thread count");
@@ -117,9 +121,6 @@ struct EnsArgs {
 
 namespace ens {
 
-__device__ __forceinline__ void named_sync(int id, int nthreads) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
-}
 // Named barrier with an AND reduction: every participant gets the same verdict.
 __device__ __forceinline__ bool named_and(int id, int nthreads, bool v) {
     uint32_t r;
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) break;
             typename Op::Set o;
             Op::stage_read(stg0 + (g % 3) * Op::kStgBytes, ct, cen0, o);
-            Op::build(smem + s * C::kStageBytes, th, o);
+            Op::build(smem + s * C::kStageBytes, th, o, cur.gc + 1 == cur.gc_end);
             tc::fence_async_smem();
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&full_bar[s]);
@@ -403,33 +404,38 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
         const int e = warp - C::kEpiWarp0;       // 0..7
         const int et = threadIdx.x - 32 * C::kEpiWarp0;   // 0..255
         const int grp = e >> 2;                  // column chunks alternate between the two groups
-        const int op = warp & 3;                 // TMEM lane quarter = operator
-        const int gt = et & 127;                 // thread within the group
-        float* xch = reinterpret_cast<float*>(smem + C::kStages * C::kStageBytes) + grp * C::kXchGroupFloats;
-        unsigned char* tbuf = smem + C::kStages * C::kStageBytes + 2 * C::kXchGroupFloats * 4;
+        const int qt = warp & 3;                 // TMEM lane quarter: tile nodes qt T/4 .. qt T/4 + T/4 - 1
+        // this warp's exchange rows: one per TMEM lane (node, operator) of its quarter
+        float* xch = reinterpret_cast<float*>(smem + C::kStages * C::kStageBytes) + e * C::kXchWarpFloats;
+        unsigned char* tbuf = smem + C::kStages * C::kStageBytes + kEnsEpiWarps * C::kXchWarpFloats * 4;
         const int members = a.members;
         const float c32 = (float)a.c;
         constexpr bool kHD = MODE == kStage1 || MODE == kStage2 || MODE == kStage3;
-        // per-tile pointwise records, row sums and centre row: bulk copies into tbuf[it & 1]
+        // per-tile pointwise records (and, for split BF16, whose accumulator lacks the
+        // add-back, the row sums and centre row): bulk copies into tbuf[it & 1]
         auto issue_tile = [&](int u, int b) {
             const int tile = u / halves;
             const int nn = min(T, a.n - tile * T);
             unsigned char* tb = tbuf + b * C::kTileBuf;
-            tc::mbar_arrive_expect_tx(&tile_bar[b], nn * (kPointStride * 4 + 16) + C::kN * 4);
+            constexpr bool kAddBack = PREC == kBf16x3;
+            tc::mbar_arrive_expect_tx(&tile_bar[b], nn * kPointStride * 4 + (kAddBack ? nn * 16 + C::kN * 4 : 0));
             tc::bulk_g2s(tb, a.PT + (long)tile * T * 5, nn * kPointStride * 4, &tile_bar[b]);
-            tc::bulk_g2s(tb + C::kTbRs, a.RS + (long)tile * T, nn * 16, &tile_bar[b]);
-            tc::bulk_g2s(tb + C::kTbCen, a.Kin + (long)__ldg(a.centre + tile) * a.mf + (u % halves) * C::kN,
-                         C::kN * 4, &tile_bar[b]);
+            if constexpr (kAddBack) {
+                tc::bulk_g2s(tb + C::kTbRs, a.RS + (long)tile * T, nn * 16, &tile_bar[b]);
+                tc::bulk_g2s(tb + C::kTbCen, a.Kin + (long)__ldg(a.centre + tile) * a.mf + (u % halves) * C::kN,
+                             C::kN * 4, &tile_bar[b]);
+            }
         };
-        // streamed per-(node, member) operands of one chunk for this thread's two pairs
+        // streamed per-(node, member) operands of one chunk for this thread's pairs: pair pi
+        // is node qt T/4 + (p >> 3), member p & 7 of the chunk, with p = lane + 32 pi
         auto fetch = [&](int u, int ch, ens::EpiSet& o) {
             if (u >= a.units) return;
             const int tile = u / halves;
             const int col0 = (u % halves) * C::kN;
 #pragma unroll
             for (int pi = 0; pi < C::kPairs; ++pi) {
-                const int pr = gt + 128 * pi;
-                const long node = (long)tile * T + (pr >> 3);
+                const int pr = lane + 32 * pi;
+                const long node = (long)tile * T + qt * (T / 4) + (pr >> 3);
                 if (node >= a.n) continue;
                 const int mfb = col0 + ch * 32 + 4 * (pr & 7);
                 const long e4 = node * a.mf + mfb;
@@ -450,15 +456,15 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             const int col0 = (u % halves) * C::kN;
             const float* tb = reinterpret_cast<const float*>(tbuf + (it & 1) * C::kTileBuf);
             {
-                const uint32_t taddr = tmem + ((uint32_t)(32 * op) << 16) + ab * C::kN + ch * 32;
+                const uint32_t taddr = tmem + ((uint32_t)(32 * qt) << 16) + ab * C::kN + ch * 32;
                 float v0[16], v1[16];
                 tc::tmem_ld16(taddr, v0);
                 tc::tmem_ld16(taddr + 16, v1);
                 tc::tmem_wait_ld();
-                // (operator, node) row: TMEM lane `lane` of this quarter holds node `lane`
-                // (M = 128); with M = 64 the quarter's lanes 0..15 hold the tile's 16 nodes
+                // lane 4 j + op of the quarter holds operator op of the quarter's node j
+                // (ens_a_row); with M = 64 only lanes 0..15 hold rows
                 if (lane < T) {
-                    float* row = xch + (op * T + lane) * C::kXchStride;
+                    float* row = xch + lane * C::kXchStride;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         *reinterpret_cast<float4*>(row + 4 * q) =
@@ -468,11 +474,12 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                     }
                 }
             }
-            ens::named_sync(2 + grp, 128);
+            __syncwarp();
 #pragma unroll
             for (int pi = 0; pi < C::kPairs; ++pi) {
-                const int pr = gt + 128 * pi;
-                const int t = pr >> 3, bm = pr & 7;
+                const int pr = lane + 32 * pi;
+                const int j = pr >> 3, bm = pr & 7;
+                const int t = qt * (T / 4) + j;
                 const long node = (long)tile * T + t;
                 if (node >= a.n) continue;
                 const int mfb = col0 + ch * 32 + 4 * bm;      // first mf of this member
@@ -480,17 +487,20 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                 float S[16];
 #pragma unroll
                 for (int o2 = 0; o2 < 4; ++o2) {
-                    const float4 sv = *reinterpret_cast<const float4*>(xch + (o2 * T + t) * C::kXchStride + 4 * bm);
+                    const float4 sv = *reinterpret_cast<const float4*>(xch + (4 * j + o2) * C::kXchStride + 4 * bm);
                     S[4 * o2] = sv.x; S[4 * o2 + 1] = sv.y; S[4 * o2 + 2] = sv.z; S[4 * o2 + 3] = sv.w;
                 }
-                const float4 cen = *reinterpret_cast<const float4*>(tb + C::kTbCen / 4 + (mfb - col0));
-                const float4 rs4 = *reinterpret_cast<const float4*>(tb + C::kTbRs / 4 + 4 * t);
-                const float cf[4] = {cen.x, cen.y, cen.z, cen.w};
-                const float rs[4] = {rs4.x, rs4.y, rs4.z, rs4.w};
+                if constexpr (PREC == kBf16x3) {
+                    // the centre term c * sum_k W (3xTF32 accumulates it in its add-back row)
+                    const float4 cen = *reinterpret_cast<const float4*>(tb + C::kTbCen / 4 + (mfb - col0));
+                    const float4 rs4 = *reinterpret_cast<const float4*>(tb + C::kTbRs / 4 + 4 * t);
+                    const float cf[4] = {cen.x, cen.y, cen.z, cen.w};
+                    const float rs[4] = {rs4.x, rs4.y, rs4.z, rs4.w};
 #pragma unroll
-                for (int o2 = 0; o2 < 4; ++o2)
+                    for (int o2 = 0; o2 < 4; ++o2)
 #pragma unroll
-                    for (int f = 0; f < 4; ++f) S[4 * o2 + f] = fmaf(cf[f], rs[o2], S[4 * o2 + f]);
+                        for (int f = 0; f < 4; ++f) S[4 * o2 + f] = fmaf(cf[f], rs[o2], S[4 * o2 + f]);
+                }
                 const float q[4] = {o.own[pi].x, o.own[pi].y, o.own[pi].z, o.own[pi].w};
                 float pt[kPointStride];
 #pragma unroll
@@ -534,7 +544,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                                     __double2float_rn((double)h4.z + a.dt6 * (double)dw), __double2float_rn(h));
                 }
             }
-            ens::named_sync(2 + grp, 128);
+            __syncwarp();   // the exchange rows are rewritten by the next chunk
         };
         constexpr int kCh = C::kN / 64;          // chunks per group per tile
         ens::EpiSet sa;
