@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             }
         };
         // one 32-column chunk: accumulator -> exchange -> (node, member) epilogue
-        auto chunk = [&](int u, int it, int ch, const ens::EpiSet& o) {
+        auto chunk = [&](int u, int it, int ch, ens::EpiSet& o) {
             const int ab = it & 1;
             const int tile = u / halves;
             const int col0 = (u % halves) * C::kN;
@@ -474,6 +474,9 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                     }
                 }
             }
+            // the streamed operands are requested after the exchange stores: issued
+            // before them, the loads hold the stores up in the load/store queue
+            fetch(u, ch, o);
             __syncwarp();
 #pragma unroll
             for (int pi = 0; pi < C::kPairs; ++pi) {
@@ -569,12 +572,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                 pend = it + 1;
             }
 #pragma unroll 1
-            for (int c = 0; c < kCh; ++c) {
-                // streamed operands first: their latency overlaps the accumulator read and exchange
-                const int ch = grp + 2 * c;
-                fetch(u, ch, sa);
-                chunk(u, it, ch, sa);
-            }
+            for (int c = 0; c < kCh; ++c) chunk(u, it, grp + 2 * c, sa);
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&acce_bar[ab]);
