@@ -5,16 +5,17 @@
 // device memory frees up (first fit in one arena of the configured HBM budget),
 // uploads their states on a copy stream, and appends their work to a queue:
 // round-robin over the active requests, one RK4 step (4 stages x node chunks x
-// members) per request per round, at most two steps ahead of a request's
+// blocks of two members) per request per round, at most two steps ahead of a request's
 // progress, so that new requests join the mix at once.  One persistent kernel -- one CTA per SM slot -- claims work
 // items from that queue (kept in device memory and published by copies on the
 // copy stream, so nothing polls across PCIe), waits (bounded) until the request's previous stage
 // has completed everywhere, runs the plain form's fused FP64 stage math on the
-// chunk for every member, and publishes completion counters; the last item of
+// chunk for its members, and publishes completion counters; the last item of
 // a request raises its completion flag in host memory.  Each work item runs the
 // plain form's node-per-lane split (stage_lane.cuh): two lanes per node over a
-// tile-transposed copy of the grid's weights and indices; the per-node math never
-// depends on the other items, so a request's result does not depend on what it
+// tile-transposed copy of the grid's weights and indices, each weight and index
+// loaded once for the item's two members; every member's sums run in the same
+// order as for a member alone, so a request's result does not depend on what it
 // was mixed with.
 //
 // Waits are bounded (%globaltimer): an idle kernel exits after a while (the
@@ -48,7 +49,7 @@ struct Item {            // one queue entry (16 bytes)
     int slot;            // request slot
     int q;               // stage index within the request: step * 4 + stage
     int chunk;           // node chunk [chunk * chunk_nodes, ...)
-    int member;          // ensemble member
+    int member;          // first ensemble member of the item's block (kSrvMB members)
 };
 
 struct alignas(16) ReqDesc {   // device table entry of an admitted request
@@ -60,7 +61,7 @@ struct alignas(16) ReqDesc {   // device table entry of an admitted request
     int n;               // nodes
     int members;
     int chunk_nodes;     // nodes per work item
-    int per_stage;       // items per stage: chunks x members
+    int per_stage;       // items per stage: chunks x member blocks
     int nchunks;         // node chunks of the grid
     int reach;           // chunks a chunk's stencils reach on either side
     int* cdone;          // [members][nchunks]: stages completed by each chunk of each member
@@ -110,35 +111,10 @@ __device__ __forceinline__ void load_row_cg(const double* p, double (&v)[4]) {
 // between stages inside one launch).  Nodes at or past `end` belong to another
 // work item (or pad the last tile): they are computed on valid rows and not stored.
 constexpr int kSrvLpn = 2, kSrvNpw = 32 / kSrvLpn;
-__device__ void serve_lanes(const ReqDesc& r, int stage, long base, long end, double* __restrict__ Hm,
-                            double* __restrict__ Kam, double* __restrict__ Kbm, double* __restrict__ Dm, int lane) {
-    const double* Kin = stage == 0 ? Hm : stage == 1 ? Kam : stage == 2 ? Kbm : Kam;
-    double* Kout = stage == 0 ? Kam : stage == 1 ? Kbm : Kam;
-    const int tl = lane % kSrvNpw, sub = lane / kSrvNpw;
-    const long i = base + tl;
-    const long tile = i / kLaneTile;
-    const int t = (int)(i % kLaneTile);
-    const int* ip = r.idxl + (tile * kSlots + sub) * kLaneTile + t;
-    const uint4* wp = r.Wl + (tile * kSlots + sub) * 2 * kLaneTile + t;
-    double acc[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-#pragma unroll
-    for (int jj = 0; jj < kSlots / kSrvLpn; ++jj) {
-        const int p = lane::ld_stream(ip + jj * kSrvLpn * kLaneTile);
-        double w[4], kv[4];
-        lane::weights(wp + jj * kSrvLpn * 2 * kLaneTile, w);
-        load_row_cg(Kin + 4L * p, kv);
-#pragma unroll
-        for (int op = 0; op < 4; ++op)
-#pragma unroll
-            for (int f = 0; f < 4; ++f) acc[op * 4 + f] += w[op] * kv[f];
-    }
-#pragma unroll
-    for (int o = kSrvNpw; o < 32; o <<= 1)
-#pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-    if (sub != 0 || i >= end) return;
+constexpr int kSrvMB = 2;   // members per work item: each weight and index is loaded once for them
+// pointwise RHS and RK combine of node i of one member
+__device__ __forceinline__ void serve_epilogue(const ReqDesc& r, int stage, long i, const double (&acc)[16], double* __restrict__ Hm,
+                               const double* __restrict__ Kin, double* __restrict__ Kout, double* __restrict__ Dm) {
     double q[4], F[4];
     load_row_cg(Kin + 4 * i, q);
     pointwise_rhs(acc, q, r.PT + i * kPointStride, r.gh0, F);
@@ -172,6 +148,50 @@ __device__ void serve_lanes(const ReqDesc& r, int stage, long base, long end, do
             Quad<double>::store_row(Hm + 4 * i, h);
         }
     }
+}
+
+// MB members m = 0 .. MB-1 of one request; member m's arrays start at + m * moff
+template <int MB>
+__device__ void serve_lanes(const ReqDesc& r, int stage, long base, long end, long moff, double* __restrict__ Hm,
+                            double* __restrict__ Kam, double* __restrict__ Kbm, double* __restrict__ Dm, int lane) {
+    const double* Kin = stage == 0 ? Hm : stage == 1 ? Kam : stage == 2 ? Kbm : Kam;
+    double* Kout = stage == 0 ? Kam : stage == 1 ? Kbm : Kam;
+    const int tl = lane % kSrvNpw, sub = lane / kSrvNpw;
+    const long i = base + tl;
+    const long tile = i / kLaneTile;
+    const int t = (int)(i % kLaneTile);
+    const int* ip = r.idxl + (tile * kSlots + sub) * kLaneTile + t;
+    const uint4* wp = r.Wl + (tile * kSlots + sub) * 2 * kLaneTile + t;
+    double acc[MB][16];
+#pragma unroll
+    for (int m = 0; m < MB; ++m)
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[m][q] = 0.0;
+#pragma unroll
+    for (int jj = 0; jj < kSlots / kSrvLpn; ++jj) {
+        const int p = lane::ld_stream(ip + jj * kSrvLpn * kLaneTile);
+        double w[4];
+        lane::weights(wp + jj * kSrvLpn * 2 * kLaneTile, w);
+#pragma unroll
+        for (int m = 0; m < MB; ++m) {
+            double kv[4];
+            load_row_cg(Kin + m * moff + 4L * p, kv);
+#pragma unroll
+            for (int op = 0; op < 4; ++op)
+#pragma unroll
+                for (int f = 0; f < 4; ++f) acc[m][op * 4 + f] += w[op] * kv[f];
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < MB; ++m)
+#pragma unroll
+        for (int o = kSrvNpw; o < 32; o <<= 1)
+#pragma unroll
+            for (int q = 0; q < 16; ++q) acc[m][q] += __shfl_xor_sync(0xffffffffu, acc[m][q], o);
+    if (sub != 0 || i >= end) return;
+#pragma unroll
+    for (int m = 0; m < MB; ++m)
+        serve_epilogue(r, stage, i, acc[m], Hm + m * moff, Kin + m * moff, Kout + m * moff, Dm + m * moff);
 }
 
 // Exit is collective: the first CTA that has found the queue empty for kIdleNs
@@ -231,6 +251,7 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
         // stencils read) have completed the previous stage.  That also orders the
         // writes: a chunk's stage q overwrites the K buffer stage q - 2 wrote, and its
         // neighbours finished reading that buffer in stage q - 1.
+        const int mb = min(kSrvMB, r.members - it.member);   // members of this item
         if (threadIdx.x == 0) {
             s_ok = 1;
             const int* cd = r.cdone + (long)it.member * r.nchunks;
@@ -240,8 +261,9 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
             // plain loads (served by L2) with exponential backoff
             unsigned ns = 64;
             auto ready = [&]() {
-                for (int c = c_lo; c <= c_hi; ++c)
-                    if (*(volatile const int*)(cd + c) < it.q) return false;
+                for (int m = 0; m < mb; ++m)
+                    for (int c = c_lo; c <= c_hi; ++c)
+                        if (*(volatile const int*)(cd + (long)m * r.nchunks + c) < it.q) return false;
                 return true;
             };
             while (!ready()) {
@@ -265,14 +287,20 @@ serve_kernel(Shared* ctl, const DevCtl* dctl, const Item* __restrict__ ring, lon
             const long begin = (long)it.chunk * r.chunk_nodes;
             const long end = min((long)r.n, begin + r.chunk_nodes);
             // chunks start on 32-node tiles, so a warp's 16 nodes lie in one tile
-            for (long base = begin + warp * (long)kSrvNpw; base < end; base += kStageWarps * (long)kSrvNpw)
-                serve_lanes(r, stage, base, end, r.H + off, r.Ka + off, r.Kb + off, r.D + off, lane);
+            const long moff = 4L * r.n;
+            for (long base = begin + warp * (long)kSrvNpw; base < end; base += kStageWarps * (long)kSrvNpw) {
+                if (mb == kSrvMB)
+                    serve_lanes<kSrvMB>(r, stage, base, end, moff, r.H + off, r.Ka + off, r.Kb + off, r.D + off, lane);
+                else
+                    serve_lanes<1>(r, stage, base, end, moff, r.H + off, r.Ka + off, r.Kb + off, r.D + off, lane);
+            }
         }
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
-            // this chunk of this member has completed stage index q
-            *(volatile int*)(r.cdone + (long)it.member * r.nchunks + it.chunk) = it.q + 1;
+            // this chunk of these members has completed stage index q
+            for (int m = 0; m < mb; ++m)
+                *(volatile int*)(r.cdone + (long)(it.member + m) * r.nchunks + it.chunk) = it.q + 1;
             __threadfence();
             const int c = atomicAdd(done + it.slot, 1) + 1;
             const unsigned long long d = atomicAdd(items_done, 1ull) + 1;
@@ -451,12 +479,13 @@ struct Server {
         count_launch();
     }
 
+    static int member_blocks(int members) { return (members + kSrvMB - 1) / kSrvMB; }
     int items_per_step(const Request& r) const {
         const int n = grids[r.grid].n, cn = chunk_nodes(n);
-        return 4 * ((n + cn - 1) / cn) * r.members;
+        return 4 * ((n + cn - 1) / cn) * member_blocks(r.members);
     }
 
-    // append one RK4 step (4 stage indices x chunks x members) of request r
+    // append one RK4 step (4 stage indices x chunks x member blocks) of request r
     void append_step(Request& r) {
         const Grid& G = grids[r.grid];
         const int cn = chunk_nodes(G.n);
@@ -464,7 +493,7 @@ struct Server {
         for (int st = 0; st < 4; ++st) {
             const int q = r.next_step * 4 + st;
             for (int c = 0; c < nch; ++c)
-                for (int mb = 0; mb < r.members; ++mb) {
+                for (int mb = 0; mb < r.members; mb += kSrvMB) {
                     if (q == r.withhold_q && c == 0 && mb == 0) {    // test hook: never queued
                         ++r.appended;
                         continue;
@@ -500,7 +529,7 @@ struct Server {
         d.chunk_nodes = chunk_nodes(G.n);
         d.nchunks = (G.n + d.chunk_nodes - 1) / d.chunk_nodes;
         d.reach = G.reach;
-        d.per_stage = d.nchunks * r.members;
+        d.per_stage = d.nchunks * member_blocks(r.members);
         d.cdone = reinterpret_cast<int*>(arena + off + 4 * one);
         d.total = d.per_stage * 4 * r.nsteps;
         d.id = r.id;
