@@ -4,12 +4,13 @@
 // states) arrive while others run.  A host scheduler thread admits them as
 // device memory frees up (first fit in one arena of the configured HBM budget),
 // uploads their states on a copy stream, and appends their work to a queue:
-// round-robin over the active requests, one RK4 step (4 stages x node chunks x
-// blocks of two members) per request per round, at most two steps ahead of a request's
-// progress, so that new requests join the mix at once.  One persistent kernel -- one CTA per SM slot -- claims work
-// items from that queue (kept in device memory and published by copies on the
-// copy stream, so nothing polls across PCIe), waits (bounded) until the request's previous stage
-// has completed everywhere, runs the plain form's fused FP64 stage math on the
+// round-robin over the active requests, one RK4 stage (node chunks x blocks of
+// two members) per request per round, at most two steps ahead of a request's
+// progress, so that new requests join the mix at once.  One persistent kernel --
+// one CTA per SM slot -- claims work items from that queue (kept in device
+// memory and published by copies on the copy stream, so nothing polls across
+// PCIe), waits (bounded) until the chunks its stencils reach have completed the
+// request's previous stage, runs the plain form's fused FP64 stage math on the
 // chunk for its members, and publishes completion counters; the last item of
 // a request raises its completion flag in host memory.  Each work item runs the
 // plain form's node-per-lane split (stage_lane.cuh): two lanes per node over a
@@ -343,7 +344,7 @@ struct Request {
     double* pinned = nullptr;            // states in the pinned pool (initial, later final)
     size_t pin_off = 0;
     cudaEvent_t ev = nullptr;            // completion of its current upload / download
-    int next_step = 0;                   // steps appended so far
+    int next_stage = 0;                  // stage indices (4 per RK4 step) appended so far
     long long appended = 0;              // items appended so far
     enum State { PENDING, UPLOADING, RUNNING, DRAINING, DONE, CANCELLED, FAILED } state = PENDING;
     long long withhold_q = -1;           // test hook: stage index whose first item is never queued
@@ -466,7 +467,7 @@ struct Server {
         c = (c + 31) / 32 * 32;
         return std::min(c, n);
     }
-    static constexpr int kLookaheadSteps = 2;
+    static constexpr int kLookaheadStages = 8;   // two RK4 steps
 
     bool kernel_running() { return cudaStreamQuery(kstream) == cudaErrorNotReady; }
 
@@ -480,34 +481,32 @@ struct Server {
     }
 
     static int member_blocks(int members) { return (members + kSrvMB - 1) / kSrvMB; }
-    int items_per_step(const Request& r) const {
+    int items_per_stage(const Request& r) const {
         const int n = grids[r.grid].n, cn = chunk_nodes(n);
-        return 4 * ((n + cn - 1) / cn) * member_blocks(r.members);
+        return ((n + cn - 1) / cn) * member_blocks(r.members);
     }
 
-    // append one RK4 step (4 stage indices x chunks x member blocks) of request r
-    void append_step(Request& r) {
+    // append the next stage index (chunks x member blocks, chunk-major) of request r
+    void append_stage(Request& r) {
         const Grid& G = grids[r.grid];
         const int cn = chunk_nodes(G.n);
         const int nch = (G.n + cn - 1) / cn;
-        for (int st = 0; st < 4; ++st) {
-            const int q = r.next_step * 4 + st;
-            for (int c = 0; c < nch; ++c)
-                for (int mb = 0; mb < r.members; mb += kSrvMB) {
-                    if (q == r.withhold_q && c == 0 && mb == 0) {    // test hook: never queued
-                        ++r.appended;
-                        continue;
-                    }
-                    Item& it = ring_h[tail % ring_cap];
-                    it.slot = r.slot;
-                    it.q = q;
-                    it.chunk = c;
-                    it.member = mb;
-                    ++tail;
+        const int q = r.next_stage;
+        for (int c = 0; c < nch; ++c)
+            for (int mb = 0; mb < r.members; mb += kSrvMB) {
+                if (q == r.withhold_q && c == 0 && mb == 0) {    // test hook: never queued
                     ++r.appended;
+                    continue;
                 }
-        }
-        ++r.next_step;
+                Item& it = ring_h[tail % ring_cap];
+                it.slot = r.slot;
+                it.q = q;
+                it.chunk = c;
+                it.member = mb;
+                ++tail;
+                ++r.appended;
+            }
+        ++r.next_stage;
     }
 
     int admit(Request& r) {
@@ -660,21 +659,22 @@ struct Server {
             if (st == 1) it = pending.erase(it);
             else ++it;
         }
-        // work: round-robin, one RK4 step per request per round, at most
-        // kLookaheadSteps steps queued or in flight per request (so that CTAs
-        // waiting on a request's previous stage stay few)
+        // work: round-robin, one stage per request per round, so that other
+        // requests' stages sit between a request's stage and the next one that
+        // depends on it; at most kLookaheadStages stages queued or in flight per
+        // request (so that CTAs waiting on a request's previous stage stay few)
         const long long done_items = ctl->progress;
         bool appended = false;
-        for (int round = 0; round < kLookaheadSteps; ++round) {
+        for (int round = 0; round < kLookaheadStages; ++round) {
             bool any = false;
             for (int id : active) {
                 Request& r = requests[id];
-                if (r.state != Request::RUNNING || r.next_step >= r.nsteps) continue;
-                const int ips = items_per_step(r);
+                if (r.state != Request::RUNNING || r.next_stage >= 4 * r.nsteps) continue;
+                const int ips = items_per_stage(r);
                 const long long outstanding = r.appended - ((volatile int*)mdone)[r.slot];
-                if (outstanding >= (long long)kLookaheadSteps * ips) continue;
+                if (outstanding >= (long long)kLookaheadStages * ips) continue;
                 if (tail + ips > ring_cap + done_items - 1024) break;       // ring full
-                append_step(r);
+                append_stage(r);
                 any = appended = true;
             }
             if (!any) break;
@@ -693,7 +693,7 @@ struct Server {
                         (work && !was_running) ? " RELAUNCH" : "");
                 for (int id : active) {
                     const Request& r = requests[id];
-                    fprintf(stderr, " | r%d st%d step %d/%d app %lld done %d", id, (int)r.state, r.next_step, r.nsteps,
+                    fprintf(stderr, " | r%d st%d stage %d/%d app %lld done %d", id, (int)r.state, r.next_stage, 4 * r.nsteps,
                             r.appended, r.slot >= 0 ? ((volatile int*)mdone)[r.slot] : -1);
                 }
                 fprintf(stderr, "\n");
@@ -911,7 +911,7 @@ int swe_srv_test_withhold(int id, int stage_index) {
     auto it = S.requests.find(id);
     if (it == S.requests.end()) { set_error("swe_srv_test_withhold: unknown request %d", id); return SWE_ERR_ARG; }
     Request& r = it->second;
-    if (stage_index < 4 * r.next_step || stage_index >= 4 * r.nsteps) {
+    if (stage_index < r.next_stage || stage_index >= 4 * r.nsteps) {
         set_error("swe_srv_test_withhold: stage index %d already queued or past the request's end", stage_index);
         return SWE_ERR_ARG;
     }
