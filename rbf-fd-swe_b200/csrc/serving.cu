@@ -113,6 +113,7 @@ __device__ __forceinline__ void load_row_cg(const double* p, double (&v)[4]) {
 // work item (or pad the last tile): they are computed on valid rows and not stored.
 constexpr int kSrvLpn = 2, kSrvNpw = 32 / kSrvLpn;
 constexpr int kSrvMB = 2;   // members per work item: each weight and index is loaded once for them
+static_assert(kSrvMB == 2, "serve_kernel dispatches blocks of one or two members");
 // pointwise RHS and RK combine of node i of one member
 __device__ __forceinline__ void serve_epilogue(const ReqDesc& r, int stage, long i, const double (&acc)[16], double* __restrict__ Hm,
                                const double* __restrict__ Kin, double* __restrict__ Kout, double* __restrict__ Dm) {
