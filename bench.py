@@ -465,14 +465,21 @@ def ensemble_target(wl: str, local: int, steps: int, warmup: int, flush, world: 
         ens.step(1)
     ens.sync()
     stream = torch.cuda.ExternalStream(ens.stream())
-    launches0 = capi.kernel_launches()
+    counted = {}
+
+    def timed():
+        # launches of the timed steps only (the clock sampler's keep-busy steps come after)
+        launches0 = capi.kernel_launches()
+        out = timed_steps(lambda: ens.step(1), stream, steps, flush)
+        counted["launches"] = capi.kernel_launches() - launches0
+        return out
 
     def busy():
         for _ in range(5):
             ens.step(1)
         ens.sync()
-    t, clocks = sample_clocks(local, lambda: timed_steps(lambda: ens.step(1), stream, steps, flush), busy)
-    launches = capi.kernel_launches() - launches0
+    t, clocks = sample_clocks(local, timed, busy)
+    launches = counted["launches"]
     t_total = max_over_ranks(sum(t), f"cuda:{local}")
     member_steps = members * steps * world / t_total
     t_stage = t_total / (4 * steps)
