@@ -294,7 +294,8 @@ int swe_ens_finalize(void);
  * to admission and to completion, -1 until known); swe_srv_fetch copies the
  * final states and forgets the request.  swe_srv_stats fills out[10] =
  * {kernel launches, admitted, completed, arena bytes in use, peak bytes in
- * use, budget, work items done, queued requests, running requests,
+ * use, budget, work items done (an item is one stage of one node chunk for
+ * up to two members of a request), queued requests, running requests,
  * dependency-wait failures}.
  *
  * Failure path.  Every wait of the persistent kernel is bounded.  A work item
@@ -304,9 +305,9 @@ int swe_ens_finalize(void);
  * then fails (swe_srv_poll returns -SWE_ERR_TIMEOUT naming it), while queued
  * and later requests run normally on a relaunched kernel.
  * swe_srv_test_withhold(request, stage_index) is a test hook: the first work
- * item of that stage (step * 4 + stage) of that request (of the next request
- * submitted, when request < 0) is never queued, so the next stage's wait runs
- * out. */
+ * item of that stage (step * 4 + stage; chunk 0, members 0-1) of that request
+ * (of the next request submitted, when request < 0) is never queued, so the
+ * next stage's wait runs out. */
 int swe_srv_start(double budget_bytes, int max_requests);
 int swe_srv_add_grid(int n, int nnbr, double gh0, double dt, const int* idx,
                      const double* Dx, const double* Dy, const double* Dz, const double* L,
