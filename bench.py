@@ -819,7 +819,7 @@ def main():
     targets = None
     if args.workload == "plain_fp64_n40962" and not args.no_targets:
         targets = {}
-        for wl in ("plain_fp64_n163842", "plain_fp64_n655362"):
+        for wl in ("plain_fp64_n163842", "plain_fp64_n655362", "plain_fp32_n655362"):
             targets[wl] = plain_target(wl, local, args.target_steps, args.warmup, flush, world)
         targets["ens_tf32_n163842_b64"] = ensemble_target(
             "ens_tf32_n163842_b64", local, args.target_steps, args.warmup, flush, world,
