@@ -1,7 +1,8 @@
 // Operand policies of the batched-ensemble kernel: how the converter threads
-// gather one 16-row chunk of a tile's neighbour rows (and, for split BF16, its
-// weights), split them into hi / lo parts in the tensor core's shared-memory
-// layout, and how the MMA thread issues the chunk's three products.
+// gather one 16-row chunk of a tile's neighbour rows and split them into hi / lo
+// parts in the tensor core's shared-memory layout (the B operand), where the A
+// (weight) operand's image sits in the slot, and how the MMA thread issues the
+// chunk's three products.
 //
 //   Tf32x3: kind::tf32, hi = tf32(x) rounded to nearest, lo = x - hi kept in
 //           FP32 and read by the tensor core at TF32 precision
@@ -22,7 +23,6 @@
 
 #include <cuda_bf16.h>
 
-#include <type_traits>
 
 #include "tcgen05.cuh"
 
@@ -177,91 +177,59 @@ struct Operands<T, MPC, kTf32x3> {
 };
 
 // --------------------------------------------------------------------------------------
-// split BF16, tiles of 32 nodes.  B thread: member-fields 2p, 2p+1 of rows 8kh..8kh+7;
-// A thread: node t, rows 8akh..8akh+7, operators op0 .. op0 + kOps - 1.
+// split BF16, tiles of 32 nodes.  B thread: member-fields 2p, 2p+1 of rows 8kh..8kh+7.
+// The A operand comes from an image split once at init (a_offset), like 3xTF32's.
 // --------------------------------------------------------------------------------------
 template <int MPC>
 struct Operands<32, MPC, kBf16x3> {
     static constexpr int kStgDepth = 0, kStgBytes = 0;
     static constexpr int kN = 4 * MPC;
     static constexpr int kConvThreads = 4 * MPC;
-    static constexpr int kOps = 256 / kConvThreads;
     static constexpr int kSboA = (kEnsKc / 8) * 128;
     static constexpr int kSboB = (kEnsKc / 8) * 128 + 16;
     static constexpr int kAHalf = (128 / 8) * kSboA;
     static constexpr int kBHalf = (kN / 8) * kSboB;
+    static constexpr int kABytes = 2 * kAHalf;                     // one chunk's A image: hi, then lo
     static constexpr int kStageBytes = ((2 * kAHalf + 2 * kBHalf) + 127) / 128 * 128;
     static constexpr int kStages = 5;
-    static_assert(kOps == 1 || kOps == 2, "A build covers 32 nodes x 2 row halves x 4 operators");
+
+    // Byte offset, within A_hi (and A_lo), of the 16-byte core row holding the weights
+    // of A row r for the chunk rows 8 akh .. 8 akh + 7.
+    __host__ __device__ static constexpr int a_offset(int r, int akh) {
+        return (r >> 3) * kSboA + akh * 128 + (r & 7) * 16;
+    }
 
     struct Thread {
-        int p, kh, at, akh, op0;
-        __device__ explicit Thread(int ct)
-            : p(ct % (kN / 2)), kh(ct / (kN / 2)), at(ct & 31), akh((ct >> 5) & 1), op0((ct >> 6) * kOps) {}
+        int p, kh;
+        __device__ explicit Thread(int ct) : p(ct % (kN / 2)), kh(ct / (kN / 2)) {}
         __device__ int col() const { return 2 * p; }
     };
     struct Fetch {
         int4 idx[2] = {make_int4(-1, -1, -1, -1), make_int4(-1, -1, -1, -1)};
-        uint32_t jj[2] = {0xffffffffu, 0xffffffffu};
     };
-    // weights of the thread's operators for the 8 chunk rows: one operator, or the pair op0, op0 + 1
-    using WT = typename std::conditional<kOps == 1, float, float2>::type;
     struct Set {
         float2 x[8];          // 8 gathered rows x 2 member-fields
         float2 cen;
-        WT w[8];
     };
 
-    __device__ static void fetch_idx(const int* rows, const uint32_t* jmap, int gc, const Thread& th, Fetch& f) {
+    __device__ static void fetch_idx(const int* rows, int gc, const Thread& th, Fetch& f) {
         const int4* r = reinterpret_cast<const int4*>(rows + gc * kEnsKc + 8 * th.kh);
         f.idx[0] = __ldg(r);
         f.idx[1] = __ldg(r + 1);
-        f.jj[0] = __ldg(jmap + (gc * 4 + 2 * th.akh) * 32 + th.at);
-        f.jj[1] = __ldg(jmap + (gc * 4 + 2 * th.akh + 1) * 32 + th.at);
     }
-    __device__ static void fetch_ops(const float* Kin, int mf, long col, const float4* W, long node, const float* cen_row,
-                                     const Thread& th, const Fetch& f, Set& o, const Set& prev) {
+    __device__ static void fetch_ops(const float* Kin, int mf, long col, const float* cen_row, const Fetch& f, Set& o,
+                                     const Set& prev) {
         const int r[8] = {f.idx[0].x, f.idx[0].y, f.idx[0].z, f.idx[0].w,
                           f.idx[1].x, f.idx[1].y, f.idx[1].z, f.idx[1].w};
 #pragma unroll
         for (int i = 0; i < 8; ++i) o.x[i] = ldg_f2(Kin + (long)r[i] * mf + col);
         o.cen = cen_row ? ldg_f2(cen_row + col) : prev.cen;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const uint32_t j = (f.jj[i >> 2] >> (8 * (i & 3))) & 0xffu;
-            if constexpr (kOps == 1)
-                o.w[i] = j != 0xffu ? __ldg(reinterpret_cast<const float*>(W + node * 32 + j) + th.op0) : 0.f;
-            else
-                o.w[i] = j != 0xffu ? __ldg(reinterpret_cast<const float2*>(W + node * 32 + j) + (th.op0 >> 1))
-                                    : make_float2(0.f, 0.f);
-        }
     }
+    // the B operand of one chunk: centred rows split into hi and lo, each member-field's
+    // 8 rows one 16-byte core row
     __device__ static void build(unsigned char* slot, const Thread& th, const Set& o) {
-        unsigned char* A_hi = slot;
-        unsigned char* A_lo = slot + kAHalf;
         unsigned char* B_hi = slot + 2 * kAHalf;
         unsigned char* B_lo = B_hi + kBHalf;
-        // A: one 16-byte core row (8 chunk rows) of (operator, node) per operator handled
-#pragma unroll
-        for (int q = 0; q < kOps; ++q) {
-            const int op = th.op0 + q;
-            float v[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if constexpr (kOps == 1) v[i] = o.w[i];
-                else v[i] = (op & 1) ? o.w[i].y : o.w[i].x;
-            }
-            uint4 hi, lo;
-            hi.x = bf16x2_split(v[0], v[1], lo.x);
-            hi.y = bf16x2_split(v[2], v[3], lo.y);
-            hi.z = bf16x2_split(v[4], v[5], lo.z);
-            hi.w = bf16x2_split(v[6], v[7], lo.w);
-            const int r = ens_a_row<32>(op, th.at);
-            const uint32_t off = (r >> 3) * kSboA + th.akh * 128 + (r & 7) * 16;
-            *reinterpret_cast<uint4*>(A_hi + off) = hi;
-            *reinterpret_cast<uint4*>(A_lo + off) = lo;
-        }
-        // B: each member-field's 8 rows are one 16-byte core row
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const float c = j ? o.cen.y : o.cen.x;

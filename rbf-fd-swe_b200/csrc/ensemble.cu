@@ -141,6 +141,7 @@ struct DevTables {
     int *row_off = nullptr, *rows = nullptr, *centre = nullptr;
     uint32_t* jmap = nullptr;
     unsigned char* aimg = nullptr;   // [chunk] 3xTF32 A operand image (hi, then lo), 512 T bytes a chunk
+    unsigned char* aimg_bf16 = nullptr;   // 32-node tiles: [chunk] split-BF16 A operand image, 8 KB a chunk
 };
 constexpr int kEnsShapes = 2;          // tiles of 32 and 16 nodes
 constexpr int kEnsShapeNodes[kEnsShapes] = {32, 16};
@@ -180,6 +181,38 @@ __global__ void ens_build_aimg(const uint32_t* __restrict__ jmap, const int* __r
     unsigned char* base = img + (size_t)gc * Op::kABytes + Op::a_offset(r, akg);
     *reinterpret_cast<float4*>(base) = hi;
     *reinterpret_cast<float4*>(base + Op::kAHalf) = lo;
+}
+
+// The split-BF16 A operand of every chunk (32-node tiles): one thread per (chunk, A row
+// r, row half akh) writes the 8 chunk rows' weights of that row as one 16-byte core row
+// of BF16 pairs for hi and one for lo.  The add-back row stays zero: split BF16 adds
+// the centre term back in the epilogue.
+__global__ void ens_build_aimg_bf16(const uint32_t* __restrict__ jmap, const int* __restrict__ chunk_tile,
+                                    const float4* __restrict__ W, int n, int nchunks, unsigned char* __restrict__ img) {
+    using Op = ens::Operands<32, 32, kBf16x3>;   // the A layout does not depend on the members per CTA
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)nchunks * 256) return;
+    const int akh = (int)(t & 1);
+    const int r = (int)((t >> 1) & 127);
+    const long gc = t >> 8;
+    const int op = ens_a_row_op<32>(r), at = ens_a_row_node<32>(r);
+    const long node = (long)chunk_tile[gc] * 32 + at;
+    float v[8];
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t jj = jmap[(gc * 4 + 2 * akh + h) * 32 + at];
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t j = (jj >> (8 * i)) & 0xffu;
+            v[4 * h + i] = (j != 0xffu && node < n) ? reinterpret_cast<const float*>(W + node * 32 + j)[op] : 0.f;
+        }
+    }
+    uint4 hi, lo;
+    hi.x = ens::bf16x2_split(v[0], v[1], lo.x);
+    hi.y = ens::bf16x2_split(v[2], v[3], lo.y);
+    hi.z = ens::bf16x2_split(v[4], v[5], lo.z);
+    hi.w = ens::bf16x2_split(v[6], v[7], lo.w);
+    unsigned char* base = img + (size_t)gc * Op::kABytes + Op::a_offset(r, akh);
+    *reinterpret_cast<uint4*>(base) = hi;
+    *reinterpret_cast<uint4*>(base + Op::kAHalf) = lo;
 }
 
 static_assert(ens::Operands<32, 64, kTf32x3>::kABytes == 512 * 32 && ens::Operands<16, 64, kTf32x3>::kABytes == 512 * 16,
@@ -268,7 +301,7 @@ struct Ensemble {
         void* ps[] = {perm, PT, RS, H32, D32, Ka, Kb, F, Kx, Hh, Dh, io, inv, bkH32, bkHh, err, W};
         for (void* p : ps) if (p) cudaFree(p);
         for (DevTables& t : tabs) {
-            void* tp[] = {t.row_off, t.rows, t.centre, t.jmap, t.aimg};
+            void* tp[] = {t.row_off, t.rows, t.centre, t.jmap, t.aimg, t.aimg_bf16};
             for (void* p : tp) if (p) cudaFree(p);
             t = DevTables{};
         }
@@ -292,7 +325,8 @@ struct Ensemble {
         a.members = members;
         a.units = tb.ntiles * (members / mpc);
         a.mf = mf;
-        a.row_off = tb.row_off; a.rows = tb.rows; a.jmap = tb.jmap; a.W = W; a.Aimg = tb.aimg;
+        a.row_off = tb.row_off; a.rows = tb.rows;
+        a.Aimg = prec == kBf16x3 ? tb.aimg_bf16 : tb.aimg;
         a.centre = tb.centre;
         a.PT = PT;
         a.RS = RS;
@@ -545,11 +579,16 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
             SWE_CUDA_TRY(cudaMalloc(&E.tabs[sh].aimg, std::max<size_t>(bytes, 16)));
             const long work = (long)tb.nchunks * 16 * T;
             const int blocks = (int)std::max<long>(1, (work + 255) / 256);
-            const DevTables& d = E.tabs[sh];
-            if (T == 32)
+            DevTables& d = E.tabs[sh];
+            if (T == 32) {
                 ens_build_aimg<32><<<blocks, 256, 0, E.stream>>>(d.jmap, dct, d.row_off, E.W, E.RS, n, tb.nchunks, d.aimg);
-            else
+                SWE_CUDA_TRY(cudaMalloc(&d.aimg_bf16, std::max<size_t>((size_t)tb.nchunks * 8192, 16)));
+                const long wb = (long)tb.nchunks * 256;
+                ens_build_aimg_bf16<<<(int)std::max<long>(1, (wb + 255) / 256), 256, 0, E.stream>>>(d.jmap, dct, E.W, n,
+                                                                                               tb.nchunks, d.aimg_bf16);
+            } else {
                 ens_build_aimg<16><<<blocks, 256, 0, E.stream>>>(d.jmap, dct, d.row_off, E.W, E.RS, n, tb.nchunks, d.aimg);
+            }
             SWE_CUDA_TRY(cudaGetLastError());
             SWE_CUDA_TRY(cudaStreamSynchronize(E.stream));
             return SWE_OK;

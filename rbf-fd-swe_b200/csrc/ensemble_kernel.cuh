@@ -24,21 +24,20 @@
 // MMA itself, through one more K row whose B values are c and whose A weights
 // are the row sums; with split BF16 in the epilogue.  Derivative and
 // hyperviscosity weights annihilate constants, so the added-back term is small
-// and the cancellation that limits FP32 stencil sums mostly disappears.  The RK4 accumulation of h (base state and
-// D register) is FP64; u, v, w and every stage state K are FP32.
+// and the cancellation that limits FP32 stencil sums mostly disappears.  The RK4
+// accumulation of h (base state and D register) is FP64; u, v, w and every stage
+// state K are FP32.
 //
 // Persistent, warp-specialised CTA (one per SM; it owns all of tensor memory):
 //   * converter warps (MPC/8): for each 16-row chunk of K they gather the rows
 //     (3xTF32: async copies into a staging buffer issued two chunks ahead, three
 //     buffers deep, so that no register waits on a gather; split BF16: 16-byte
 //     loads one chunk ahead into a ping-pong register set) and centre and split
-//     them into the B operand.  Split BF16 converters also gather the weights and
-//     write the matching A chunk densely, one 16-byte core row (8 chunk rows of
-//     one operator and node) per store, from a map of chunk rows to stencil slots;
-//   * the A producer warp (3xTF32): the A chunks are static, so they are split
-//     once at init into an image of the slot's A part; one thread streams each
-//     chunk's image into its slot with one bulk copy (and prefetches the image
-//     two chunks ahead into L2);
+//     them into the B operand;
+//   * the A producer warp: the A chunks are static, so they are split once at
+//     init into an image of the slot's A part (per precision); one thread streams
+//     each chunk's image into its slot with one bulk copy (and prefetches the
+//     image two chunks ahead into L2);
 //   * a ring of slots (2 for 3xTF32, whose staging takes the third slot's shared
 //     memory) hands chunks to the MMA warp: one thread issues the chunk's 3
 //     products (128 x N x 16) into one of two TMEM accumulators once the
@@ -75,7 +74,7 @@ struct EnsCfg {
     static constexpr int kConvThreads = 32 * kConvWarps;
     static constexpr int kMmaWarp = kConvWarps;
     static constexpr int kEpiWarp0 = kConvWarps + 1;
-    static constexpr int kProdWarp = kEpiWarp0 + kEnsEpiWarps;   // A producer (idle for split BF16)
+    static constexpr int kProdWarp = kEpiWarp0 + kEnsEpiWarps;   // A operand producer
     static constexpr int kThreads = 32 * (kConvWarps + 2 + kEnsEpiWarps);
     static constexpr int kStages = Op::kStages;            // ring slots
     static constexpr int kStageBytes = Op::kStageBytes;
@@ -100,9 +99,7 @@ struct EnsArgs {
     int mf;                // 4 * members (row length of the state arrays)
     const int* row_off;    // [ntiles + 1] offsets into rows, multiples of kEnsKc
     const int* rows;       // unique neighbour rows of each tile, ascending; padded with the centring node
-    const uint32_t* jmap;  // [chunk][row group][node t]: stencil slot of each of the 4 rows, 255 = none
-    const float4* W;       // [n][32] (Dx, Dy, Dz, L) per stencil slot
-    const unsigned char* Aimg;   // 3xTF32: [chunk] A operand image (hi, then lo) in the slot's layout
+    const unsigned char* Aimg;   // [chunk] A operand image (hi, then lo) in the slot's layout
     const int* centre;     // [ntiles] node whose state centres the tile
     const float4* PT;      // [n][5] pointwise record (20 floats)
     const float4* RS;      // [n] row sums of the four operators
@@ -307,7 +304,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             const int tile = p.u / halves;
             const long col = (long)(p.u % halves) * C::kN + th.col();
             const float* cen_row = p.u != u_prev ? a.Kin + (long)__ldg(a.centre + tile) * a.mf : nullptr;
-            Op::fetch_ops(a.Kin, a.mf, col, a.W, (long)tile * T + th.at, cen_row, th, f, o, prev);
+            Op::fetch_ops(a.Kin, a.mf, col, cen_row, f, o, prev);
         };
         int g = 0;
         auto step = [&](typename Op::Set& o, typename Op::Set& nx, int u_cur) -> bool {
@@ -315,7 +312,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             ens::Cursor nxt = ens::next_cursor(cur, a, halves);
             fetch_ops(nxt, fx, nx, o, u_cur);
             ens::Cursor nxt2 = ens::next_cursor(nxt, a, halves);
-            if (nxt2.valid) Op::fetch_idx(a.rows, a.jmap, nxt2.gc, th, fx);
+            if (nxt2.valid) Op::fetch_idx(a.rows, nxt2.gc, th, fx);
             const int s = g % C::kStages;
             if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) return false;
             Op::build(smem + s * C::kStageBytes, th, o);
@@ -328,10 +325,10 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
         };
         if (cur.valid) {
             typename Op::Fetch f0;
-            Op::fetch_idx(a.rows, a.jmap, cur.gc, th, f0);
+            Op::fetch_idx(a.rows, cur.gc, th, f0);
             fetch_ops(cur, f0, sa, sa, -1);
             const ens::Cursor n1 = ens::next_cursor(cur, a, halves);
-            if (n1.valid) Op::fetch_idx(a.rows, a.jmap, n1.gc, th, fx);
+            if (n1.valid) Op::fetch_idx(a.rows, n1.gc, th, fx);
         }
         // two steps per trip so that the ping-pong sets never need copying
         while (cur.valid) {
@@ -357,8 +354,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                 for (int gc = gc0; gc < gc1; ++gc, ++g) {
                     const int s = g % C::kStages;
                     if (!ens::wait(&full_bar[s], (g / C::kStages) & 1, abort_v, a.err, 5)) { ok = false; break; }
-                    if constexpr (PREC == kTf32x3)
-                        if (!ens::wait(&afull_bar[s], (g / C::kStages) & 1, abort_v, a.err, 9)) { ok = false; break; }
+                    if (!ens::wait(&afull_bar[s], (g / C::kStages) & 1, abort_v, a.err, 9)) { ok = false; break; }
                     tc::fence_after_sync();
                     Op::issue(tc::smem_u32(smem + s * C::kStageBytes), d, gc == gc0);
                     tc::mma_commit(&empty_bar[s]);
@@ -376,8 +372,8 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
         }
         __syncwarp();
     } else if (warp == C::kProdWarp) {
-        // ====================== A operand producer (3xTF32) ======================
-        if constexpr (PREC == kTf32x3) {
+        // =========================== A operand producer ===========================
+        {
             if (lane == 0) {
                 constexpr uint32_t kABytes = Op::kABytes;
                 ens::Cursor cur = ens::first_cursor(a, halves);
