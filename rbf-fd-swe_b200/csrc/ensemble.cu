@@ -216,7 +216,8 @@ __global__ void ens_build_aimg_bf16(const uint32_t* __restrict__ jmap, const int
 }
 
 static_assert(ens::Operands<32, 64, kTf32x3>::kABytes == 512 * 32 && ens::Operands<16, 64, kTf32x3>::kABytes == 512 * 16,
-              "A image: 512 bytes per tile node and chunk");
+              "3xTF32 A image: 512 bytes per tile node and chunk");
+static_assert(ens::Operands<32, 64, kBf16x3>::kABytes == 8192, "split-BF16 A image: 8 KB per chunk");
 
 __global__ void ens_invariants_kernel(const float* __restrict__ H32, const double* __restrict__ Hh,
                                       const float4* __restrict__ PT, int n, int members, double gh0,
@@ -282,7 +283,7 @@ struct Ensemble {
     int* err = nullptr;
     // tile tables, one set per tile shape (32 and 16 nodes)
     DevTables tabs[kEnsShapes];
-    float4* W = nullptr;
+    float4* W = nullptr;         // raw FP32 weights [n][32], only while the A images are built
     Variant var[kEnsVariants];   // (tile nodes, members per CTA): (32, 64), (32, 32), (16, 64), (16, 32)
     int chosen = -1;
     int prec = kTf32x3;
@@ -564,8 +565,9 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
         SWE_TRY(upload(&d.centre, tbs[sh].centre));
     }
     SWE_TRY(upload(reinterpret_cast<float**>(&E.W), w));
-    // 3xTF32 A images of both tile shapes (about 4 KB per node for 32-node tiles,
-    // 3 KB for 16-node tiles): built on the device from the tables and the weights
+    // A images: 3xTF32 for both tile shapes (about 4 KB per node for 32-node tiles,
+    // 3 KB for 16-node tiles) and split BF16 for 32-node tiles (2 KB per node), built
+    // on the device from the tables and the weights
     for (int sh = 0; sh < kEnsShapes; ++sh) {
         const int T = kEnsShapeNodes[sh];
         const TileTables& tb = tbs[sh];
@@ -596,6 +598,9 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
         cudaFree(dct);
         if (rc != SWE_OK) return rc;
     }
+    // the stage kernels read only the images: the raw weights are not kept
+    cudaFree(E.W);
+    E.W = nullptr;
     for (float** p : {&E.H32, &E.D32, &E.Ka, &E.Kb, &E.F, &E.Kx, &E.bkH32}) SWE_CUDA_TRY(cudaMalloc(p, s32));
     for (double** p : {&E.Hh, &E.Dh, &E.bkHh}) SWE_CUDA_TRY(cudaMalloc(p, s64));
     SWE_CUDA_TRY(cudaMalloc(&E.io, (size_t)n * members * 4 * sizeof(double)));
