@@ -194,6 +194,32 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+SPEC_HBM_GBS = 8000.0   # the B200 HBM3e specification figure the hot path's targets are stated against
+
+
+def measured_peak_bf16_tflops():
+    """Dense BF16 GEMM throughput (cuBLAS, burst) of this pool's B200s, or the fallback."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def ensemble_tensor_roofline(cfg: dict, members: int, precision: str, t_stage: float) -> dict:
+    """Tensor-core side of the batched kernel: the MMA work one stage issues (every 16-row
+    chunk: M = 4 x tile nodes, N = 4 x members over the member blocks, K = 16, three
+    products) over the stage time, against the dense peak of the MMA kind (TF32 runs at half
+    the BF16 rate)."""
+    flops = cfg["chunks"] * 16 * (4 * cfg["tile_nodes"]) * (4 * members) * 2 * 3
+    bf16, src = measured_peak_bf16_tflops()
+    peak = bf16 / 2 if precision == "tf32x3" else bf16
+    achieved = flops / t_stage / 1e12
+    return {"mma_flops_per_launch": flops, "achieved": round(achieved, 1), "peak": round(peak, 1),
+            "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+            "peak_source": f"{src} BF16 GEMM" + (" / 2 for TF32" if precision == "tf32x3" else "")}
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
 
@@ -434,7 +460,8 @@ def plain_target(wl: str, local: int, steps: int, warmup: int, flush, world: int
             "unit": "node-stage updates/s", "member_steps_per_s": steps * world / t_total,
             "steps": steps, "ms_per_step": 1e3 * t_total / steps, "dtype": "f64" if prec == "fp64" else "f32",
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(wl),
+                         "frac": round(achieved / peak, 4), "frac_of_spec_8tbs": round(achieved / SPEC_HBM_GBS, 4),
+                         "traffic": TRAFFIC_BYTES.get(wl),
                          "peak_source": peak_kind, "kernel": "swe::stage_lane_kernel" if kinfo["in_use"] == "lane"
                          else kinfo["in_use"], "kernel_us": round(t_kernel * 1e6, 2),
                          "alg_bytes_per_node_stage": ALG_BYTES[prec], "kernel_choice": kinfo},
@@ -554,9 +581,11 @@ def ensemble_target(wl: str, local: int, steps: int, warmup: int, flush, world: 
                               "h_worst_member": int(err_idx[int(errs[:, 3].argmax())])},
             "e2e": e2e, "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": TRAFFIC_BYTES.get(wl),
+                         "frac": round(achieved / peak, 4), "frac_of_spec_8tbs": round(achieved / SPEC_HBM_GBS, 4),
+                         "traffic": TRAFFIC_BYTES.get(wl),
                          "peak_source": peak_kind, "kernel": "swe::ens_stage_kernel",
-                         "kernel_us": round(t_stage * 1e6, 2), "alg_bytes_per_node_stage": ens_bytes},
+                         "kernel_us": round(t_stage * 1e6, 2), "alg_bytes_per_node_stage": ens_bytes,
+                         "tensor": ensemble_tensor_roofline(cfg, members, precision, t_stage)},
             "clocks": clocks, "state_finite": bool(np.isfinite(Hens).all())}
 
 
@@ -802,7 +831,8 @@ def main():
     # for most of each step: its roofline is not an HBM roofline
     l2_resident = alg_per_launch < 100e6
     roofline = {"bound": "l2-resident" if l2_resident else "hbm", "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "frac_of_spec_8tbs": round(achieved / SPEC_HBM_GBS, 4),
+                "traffic": traffic, "peak_source": peak_kind,
                 "kernel": {"pipelined": "swe::stage_tma_kernel", "register": "swe::stage_kernel",
                            "lane": "swe::stage_lane_kernel"}[kinfo["in_use"]],
                 "kernel_us": round(t_kernel * 1e6, 2), "kernel_us_isolated": round(t_isolated * 1e6, 2),
