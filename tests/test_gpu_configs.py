@@ -12,6 +12,8 @@ N=40962, up to 100 steps).  This file runs the configured workloads themselves:
 * N=163842 (level 7), 64 members, 3xTF32 batched form, 1000 steps at dt=120 s:
   h error of every member against the plain FP64 GPU run of that member, with
   that plain run itself checked against the oracle over the same 1000 steps.
+* N=40962, 32 members (32 per CTA), both precisions, 200 steps: every member
+  against its plain FP64 GPU run.
 
 Bars and why:
 * FP64 states after 1000 steps, 1e-12 relative per field.  Two FP64 summation
@@ -167,3 +169,36 @@ def test_n163842_b64_tf32x3_1000_steps_h_error_every_member(plain):
           f"h worst member {worst}, h median {np.median(errs[:, 3]):.3e}")
     assert np.isfinite(H).all()
     assert errs[:, 3].max() <= 1e-6, (worst, errs[worst])
+
+
+@pytest.mark.parametrize("precision", ["tf32x3", "bf16x3"])
+def test_n40962_b32_200_steps_every_member(plain, precision):
+    """A 32-member ensemble (32 members per CTA: the (32, 32) and (16, 32) tile shapes the
+    tuner chooses between) on the N=40962 grid, 200 steps at dt=225 s, every member
+    against its plain FP64 GPU run.  3xTF32 is held to the batched form's h bar, 1e-6 of
+    max|h|; split BF16 (2^-17 operand splits) to 1e-5."""
+    _, d = generated_input(6)
+    m = swe_input.to_model(d)
+    members, steps = 32, 200
+    H0 = np.stack([gen.perturb_h(m.H_init, 500 + b) for b in range(members)])
+    ens = capi.Ensemble()
+    try:
+        ens.init(m, members)
+        ens.set_precision(precision)
+        ens.tune()
+        cfg = ens.config()
+        ens.set_state(H0)
+        ens.step(steps)
+        H = ens.get_state()
+    finally:
+        ens.finalize()
+    assert cfg["members_per_cta"] == 32
+    plain.init_model(m, "fp64")
+    errs = np.empty((members, 4))
+    for b in range(members):
+        plain.set_state(H0[b])
+        plain.step(steps)
+        errs[b] = scaled_err(H[b], plain.get_state())
+    print(f"N=40962 B=32 {precision} {cfg} {steps} steps: per-field max over members {errs.max(0)}")
+    assert np.isfinite(H).all()
+    assert errs[:, 3].max() <= (1e-6 if precision == "tf32x3" else 1e-5)
