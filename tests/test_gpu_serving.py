@@ -9,14 +9,16 @@
 * every served member equals the FP64 oracle's run of the same state and step
   count (rk4_rbffd_swe.c:30-72) within 1e-12 relative per field;
 * a dependency wait that runs out (a work item withheld by the test hook) fails
-  the request with SWE_ERR_TIMEOUT, and the server then completes a clean request.
+  the request with SWE_ERR_TIMEOUT, and the server then completes a clean request;
+* on the N=40962 grid in the device level order (20 node chunks per member, work
+  items of two members), concurrent requests of 1 to 7 members match the oracle.
 """
 import numpy as np
 import pytest
 
 import oracle
 from conftest import generated_input, rel_err
-from swe_b200 import capi, gen, swe_input
+from swe_b200 import capi, gen, layout, swe_input
 
 pytestmark = pytest.mark.gpu
 
@@ -156,3 +158,27 @@ def test_dependency_timeout_fails_request_then_server_recovers(models):
     port = oracle.Port(m3, "fp64")
     for b in range(2):
         assert rel_err(out[b], port.run(H0[b], 12)).max() <= 1e-12
+
+
+def test_n40962_device_order_requests_match_oracle():
+    """Several requests on the N=40962 grid registered in the device level order (the
+    serving bench's setup): member counts 1, 2, 5 and 7 (odd counts end in a one-member
+    block), different lengths, all in flight together; every member against the
+    oracle's own RK4 run (1e-12 relative per field)."""
+    _, d = generated_input(6)
+    m = swe_input.to_model(d)
+    m = layout.reorder(m, layout.rcm_mapping(m, device=True))
+    plan = [(1, 30, 3), (2, 20, 13), (5, 12, 23), (7, 25, 33)]
+    srv = capi.Server(4 << 30)
+    try:
+        g = srv.add_grid(m)
+        states = [_states(m, mb, seed) for mb, st, seed in plan]
+        rids = [srv.submit(g, H0, st) for (mb, st, seed), H0 in zip(plan, states)]
+        srv.wait(rids)
+        outs = [srv.fetch(r) for r in rids]
+    finally:
+        srv.stop()
+    port = oracle.Port(m, "fp64")
+    for (mb, st, seed), H0, out in zip(plan, states, outs):
+        for b in range(mb):
+            assert rel_err(out[b], port.run(H0[b], st)).max() <= 1e-12, (mb, st, b)
