@@ -14,7 +14,8 @@ read so that the write's dirty lines are written back before the step: each
 step starts from a cold, clean L2); `e2e` = the
 same metric through the C ABI with host buffers (pinned H2D of the state,
 one RK4 step, D2H of the state every step); `roofline` = the fused stage
-kernel's algorithmic bytes (1396 B per FP64 node-stage, 760 B FP32) over its
+kernel's algorithmic bytes (1396 B per FP64 node-stage, 760 B FP32; 62 B less when
+the node-per-lane kernel reads the stencil rows as 16-bit offsets) over its
 average duration in the timed region (a timed step is the four stage kernels and
 nothing else, so step time / 4) against the measured HBM copy bandwidth.  Multi-GPU runs
 are independent replicas (the path does not shard across GPUs here): every
@@ -80,6 +81,14 @@ def vs_recorded(workload: str, value: float):
 
 
 ALG_BYTES = {"fp64": 1396, "fp32": 760}      # per node-stage (FP64: 4*31*8+31*4+17*8+4*8+14*8)
+
+
+def plain_alg_bytes(prec: str, kinfo: dict) -> int:
+    """Bytes per node-stage of the representation the stage kernel reads: the
+    node-per-lane kernel reads the 31 stencil rows as 16-bit offsets (2 B, not 4)
+    when every offset fits."""
+    narrow = kinfo["in_use"] == "lane" and kinfo.get("index_offsets_16bit", False)
+    return ALG_BYTES[prec] - (31 * 2 if narrow else 0)
 # batched form, per node-stage: shared 4*31*4 (weights) + 31*4 (idx) + 17*4 (pointwise)
 # plus per member 4*4 (K read once) + 14*4 (RK combine) + 4 (FP64 h registers)
 ENS_SHARED_BYTES = 4 * 31 * 4 + 31 * 4 + 17 * 4
@@ -100,11 +109,12 @@ L2_NOTE_BOTH = ("GPU arm: L2 flushed between timed steps (256 MB write, then 256
 TRAFFIC_BYTES = {
     # DRAM read + write bytes per stage launch, mean over 8 launches of the timed
     # steps (ncu --cache-control none inside the bench's own flushed loop, so
-    # stage 0 of each step starts cold and stages 1-3 see what L2 kept)
-    "plain_fp64_n40962": 32.50e6,       # swe::stage_lane_kernel<double, *, 2, 4>, L2 prefetch on
-    "plain_fp64_n163842": 197.34e6,     # swe::stage_lane_kernel<double, *, 2, 4>
-    "plain_fp64_n655362": 948.31e6,     # swe::stage_lane_kernel<double, *, 2, 4>
-    "plain_fp32_n655362": 506.57e6,     # swe::stage_lane_kernel<float, *, 1, 4>
+    # stage 0 of each step starts cold and stages 1-3 see what L2 kept; plain
+    # kernels reading the stencil rows as 16-bit offsets)
+    "plain_fp64_n40962": 29.64e6,       # swe::stage_lane_kernel<double, *, 2, 5, true>, L2 prefetch on
+    "plain_fp64_n163842": 186.95e6,     # swe::stage_lane_kernel<double, *, 2, 4, true>
+    "plain_fp64_n655362": 905.71e6,     # swe::stage_lane_kernel<double, *, 2, 4, true>
+    "plain_fp32_n655362": 461.12e6,     # swe::stage_lane_kernel<float, *, 1, 4, true>
     # swe::ens_stage_kernel<32, 64, stage, 3xTF32>, 12 launches (cold); 707 MB of it is
     # the streamed A-operand image (16 KB per 16-row chunk, 43128 chunks)
     "ens_tf32_n163842_b64": 1668.31e6,
@@ -453,8 +463,9 @@ def plain_target(wl: str, local: int, steps: int, warmup: int, flush, world: int
     t_total = max_over_ranks(sum(t), f"cuda:{local}")
     t_kernel = t_total / (4 * steps)
     peak, peak_kind = measured_peak_hbm()
-    achieved = ALG_BYTES[prec] * N / t_kernel / 1e9
     kinfo = plain.kernel_info()
+    alg = plain_alg_bytes(prec, kinfo)
+    achieved = alg * N / t_kernel / 1e9
     plain.finalize()
     return {"workload": wl, "description": desc, "value": 4.0 * N * steps * world / t_total,
             "unit": "node-stage updates/s", "member_steps_per_s": steps * world / t_total,
@@ -464,7 +475,7 @@ def plain_target(wl: str, local: int, steps: int, warmup: int, flush, world: int
                          "traffic": TRAFFIC_BYTES.get(wl),
                          "peak_source": peak_kind, "kernel": "swe::stage_lane_kernel" if kinfo["in_use"] == "lane"
                          else kinfo["in_use"], "kernel_us": round(t_kernel * 1e6, 2),
-                         "alg_bytes_per_node_stage": ALG_BYTES[prec], "kernel_choice": kinfo},
+                         "alg_bytes_per_node_stage": alg, "kernel_choice": kinfo},
             "clocks": clocks}
 
 
@@ -823,9 +834,10 @@ def main():
     # programmatic dependent launch, which per-launch events would break up)
     t_kernel = t_total / (4 * args.steps)
     t_isolated = k_time / max(k_launches, 1)
-    achieved = ALG_BYTES[prec] * N / t_kernel / 1e9
     kinfo = plain.kernel_info()
-    alg_per_launch = ALG_BYTES[prec] * N
+    alg = plain_alg_bytes(prec, kinfo)
+    achieved = alg * N / t_kernel / 1e9
+    alg_per_launch = alg * N
     traffic = TRAFFIC_BYTES.get(args.workload)
     # data that fits the 126 MB L2 (with the flush's lines and headroom) is served from L2
     # for most of each step: its roofline is not an HBM roofline
@@ -836,7 +848,7 @@ def main():
                 "kernel": {"pipelined": "swe::stage_tma_kernel", "register": "swe::stage_kernel",
                            "lane": "swe::stage_lane_kernel"}[kinfo["in_use"]],
                 "kernel_us": round(t_kernel * 1e6, 2), "kernel_us_isolated": round(t_isolated * 1e6, 2),
-                "alg_bytes_per_node_stage": ALG_BYTES[prec], "alg_bytes_per_launch": alg_per_launch,
+                "alg_bytes_per_node_stage": alg, "alg_bytes_per_launch": alg_per_launch,
                 "kernel_choice": kinfo}
     if l2_resident:
         roofline["note"] = (f"{alg_per_launch / 1e6:.1f} MB of algorithmic bytes per launch fit the 126 MB L2: "

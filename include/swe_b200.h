@@ -134,10 +134,13 @@ int swe_cuda_sync(void);
  * bars; it runs at 3, 4 or 5 CTAs per SM and can bulk-prefetch each warp's
  * contiguous blocks into L2 at its start).  swe_cuda_init times every kernel
  * and shape on the patch, keeps the fastest shape of each, and uses the fastest
- * kernel.  info[8] = {kernel in use (0/1/2), pipelined tile in nodes (0 if
+ * kernel.  info[9] = {kernel in use (0/1/2), pipelined tile in nodes (0 if
  * unavailable), ns per eval launch of kernel 0 (its fastest tile), of kernel 1,
  * lanes per node of kernel 2, ns per eval launch of kernel 2 (its fastest
- * shape), kernel 2's L2 prefetch (0/1), kernel 2's CTAs per SM (3/4/5)}.
+ * shape), kernel 2's L2 prefetch (0/1), kernel 2's CTAs per SM (3/4/5),
+ * kernel 2 reads its gather rows as 16-bit offsets from each node's own row
+ * (1: every stencil row lies within 32767 rows of its node, as in any
+ * RCM-ordered grid; 0: 32-bit indices)}.
  * swe_cuda_select_kernel takes which = 0 / 1 (kernels 0 / 1), 2 / 3 / 4 (the
  * pipelined kernel with 64- / 32- / 16-node tiles), 5 (kernel 2, its current
  * shape) and 6 + s for kernel 2's shape s in 0..17: 1 / 2 / 4 lanes per node
@@ -146,6 +149,10 @@ int swe_cuda_sync(void);
  * prefetch when s >= 15. */
 int swe_cuda_select_kernel(int which);
 int swe_cuda_kernel_info(int* info);
+/* Index width of kernel 2's gather rows: 16 (the default whenever every stencil
+ * row lies within 32767 rows of its node; SWE_ERR_ARG otherwise) or 32.  The
+ * results are the same bits either way; 16 halves the index bytes. */
+int swe_cuda_set_index_width(int bits);
 
 /* Timing of the fused stage kernels, measured with CUDA events on the
  * library's stream while enabled.  out[0] = seconds of stage kernels since

@@ -34,17 +34,33 @@ constexpr int kEnsKc = 16;          // neighbour rows per pipeline chunk
 enum EnsPrecision { kTf32x3 = 0, kBf16x3 = 1 };
 
 // Row of the A operand (and TMEM lane of the accumulator) that holds operator op of
-// tile node t: each 32-lane quarter of tensor memory holds T/4 consecutive tile nodes
-// with their four operators in adjacent lanes (lanes 0..15 of each quarter when
-// M = 64), so that one epilogue warp reads all four operators of its nodes.
+// tile node t.  Each 32-lane quarter of tensor memory holds T/4 consecutive tile nodes,
+// so that one epilogue warp reads all four operators of its nodes:
+//   T = 32: operator op of quarter node j in lane j + 8 op.  A 16x256b load of lanes
+//           0..15 then gives thread i operators 0 and 1 of node i / 4, and one of lanes
+//           16..31 operators 2 and 3 (tmem_ld16x256);
+//   T = 16 (M = 64, lanes 0..15 of each quarter): the four operators of a node in
+//           adjacent lanes 4 j + op, read with 32x32b loads and exchanged through
+//           shared memory.
 template <int T>
 __host__ __device__ constexpr int ens_a_row(int op, int t) {
-    return T * (t / (T / 4)) + 4 * (t % (T / 4)) + op;
+    return T == 32 ? 32 * (t / 8) + 8 * op + (t % 8) : T * (t / (T / 4)) + 4 * (t % (T / 4)) + op;
 }
 template <int T>
-__host__ __device__ constexpr int ens_a_row_op(int r) { return r & 3; }
+__host__ __device__ constexpr int ens_a_row_op(int r) { return T == 32 ? (r & 31) >> 3 : r & 3; }
 template <int T>
-__host__ __device__ constexpr int ens_a_row_node(int r) { return (r / T) * (T / 4) + ((r % T) >> 2); }
+__host__ __device__ constexpr int ens_a_row_node(int r) {
+    return T == 32 ? (r >> 5) * 8 + (r & 7) : (r / T) * (T / 4) + ((r % T) >> 2);
+}
+
+// Column of the B operand (and of the accumulator) within a 32-column chunk that holds
+// field f of chunk member m (0..7).  T = 32: thread i's columns in a 16x256b load,
+// 8 k + 2 (i % 4) + b, are fields 0..3 of members i % 4 and i % 4 + 4 (member
+// i % 4 + 4 (k & 1), field 2 (k >> 1) + b).  T = 16: member-major, 4 m + f.
+template <int T>
+__host__ __device__ constexpr int ens_b_col(int m, int f) {
+    return T == 32 ? 8 * (2 * (f >> 1) + (m >> 2)) + 2 * (m & 3) + (f & 1) : 4 * m + f;
+}
 
 struct EnsArgs;
 
@@ -144,7 +160,7 @@ struct Operands<T, MPC, kTf32x3> {
         const float cv[4] = {o.cen.x, o.cen.y, o.cen.z, o.cen.w};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const int nrow = 4 * th.quad + j;
+            const int nrow = 32 * (th.quad >> 3) + ens_b_col<T>(th.quad & 7, j);
             float4 hi, lo;
             float y[4];
 #pragma unroll
@@ -177,8 +193,9 @@ struct Operands<T, MPC, kTf32x3> {
 };
 
 // --------------------------------------------------------------------------------------
-// split BF16, tiles of 32 nodes.  B thread: member-fields 2p, 2p+1 of rows 8kh..8kh+7.
-// The A operand comes from an image split once at init (a_offset), like 3xTF32's.
+// split BF16, tiles of 32 nodes.  B thread: columns 2p, 2p+1 (fields f, f + 1 of one
+// member, ens_b_col) of rows 8kh..8kh+7.  The A operand comes from an image split once
+// at init (a_offset), like 3xTF32's.
 // --------------------------------------------------------------------------------------
 template <int MPC>
 struct Operands<32, MPC, kBf16x3> {
@@ -202,7 +219,12 @@ struct Operands<32, MPC, kBf16x3> {
     struct Thread {
         int p, kh;
         __device__ explicit Thread(int ct) : p(ct % (kN / 2)), kh(ct / (kN / 2)) {}
-        __device__ int col() const { return 2 * p; }
+        // member-field (state column) of B column 2p: within its 32-column chunk,
+        // 2p = 8 k + 2 i holds member i + 4 (k & 1), fields 2 (k >> 1) and + 1
+        __device__ int col() const {
+            const int k = (p >> 2) & 3, i = p & 3;
+            return 32 * (p >> 4) + 4 * (i + 4 * (k & 1)) + 2 * (k >> 1);
+        }
     };
     struct Fetch {
         int4 idx[2] = {make_int4(-1, -1, -1, -1), make_int4(-1, -1, -1, -1)};

@@ -79,7 +79,9 @@ struct EnsCfg {
     static constexpr int kStages = Op::kStages;            // ring slots
     static constexpr int kStageBytes = Op::kStageBytes;
     static constexpr int kXchStride = 36;                  // floats per (op, node) row; 9 x 16 B
-    static constexpr int kXchWarpFloats = T * kXchStride;  // an epilogue warp's exchange rows
+    // an epilogue warp's exchange rows (16-node tiles only: 32-node tiles read their
+    // sums straight from tensor memory)
+    static constexpr int kXchWarpFloats = T == 32 ? 0 : T * kXchStride;
     static constexpr int kTbRs = T * kPointStride * 4;     // per-tile buffer: PT, row sums, centre
     static constexpr int kTbCen = kTbRs + T * 16;
     static constexpr int kPairs = T / 16;                  // (node, member) pairs per epilogue thread and chunk
@@ -88,6 +90,7 @@ struct EnsCfg {
     static constexpr int kSmem = kStgOff + Op::kStgDepth * Op::kStgBytes;
     static constexpr int kTmemCols = (2 * kN <= 256) ? 256 : 512;
     static_assert(kConvThreads == Op::kConvThreads, "converter thread count");
+    static_assert(kSmem + 1024 <= 227 * 1024, "dynamic shared memory beside the barriers fits 227 KB");
     static_assert(kN % 64 == 0, "epilogue column chunks");
 };
 
@@ -422,18 +425,22 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                              C::kN * 4, &tile_bar[b]);
             }
         };
-        // streamed per-(node, member) operands of one chunk for this thread's pairs: pair pi
-        // is node qt T/4 + (p >> 3), member p & 7 of the chunk, with p = lane + 32 pi
+        // this thread's pair pi of a chunk: tile node pair_node(pi) and chunk member
+        // pair_member(pi).  32-node tiles: node qt 8 + lane / 4, members lane % 4 and
+        // lane % 4 + 4 (the columns tmem_ld16x256 gives the thread, ens_b_col);
+        // 16-node tiles: node qt 4 + (p >> 3), member p & 7, with p = lane + 32 pi.
+        auto pair_node = [&](int pi) { return T == 32 ? qt * 8 + (lane >> 2) : qt * (T / 4) + ((lane + 32 * pi) >> 3); };
+        auto pair_member = [&](int pi) { return T == 32 ? (lane & 3) + 4 * pi : (lane + 32 * pi) & 7; };
+        // streamed per-(node, member) operands of one chunk for this thread's pairs
         auto fetch = [&](int u, int ch, ens::EpiSet& o) {
             if (u >= a.units) return;
             const int tile = u / halves;
             const int col0 = (u % halves) * C::kN;
 #pragma unroll
             for (int pi = 0; pi < C::kPairs; ++pi) {
-                const int pr = lane + 32 * pi;
-                const long node = (long)tile * T + qt * (T / 4) + (pr >> 3);
+                const long node = (long)tile * T + pair_node(pi);
                 if (node >= a.n) continue;
-                const int mfb = col0 + ch * 32 + 4 * (pr & 7);
+                const int mfb = col0 + ch * 32 + 4 * pair_member(pi);
                 const long e4 = node * a.mf + mfb;
                 const long eh = node * members + (mfb >> 2);
                 o.own[pi] = ens::ldg_f4(a.Kin + e4);
@@ -451,9 +458,17 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             const int tile = u / halves;
             const int col0 = (u % halves) * C::kN;
             const float* tb = reinterpret_cast<const float*>(tbuf + (it & 1) * C::kTileBuf);
-            {
-                const uint32_t taddr = tmem + ((uint32_t)(32 * qt) << 16) + ab * C::kN + ch * 32;
-                float v0[16], v1[16];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * qt) << 16) + ab * C::kN + ch * 32;
+            float v0[16], v1[16];
+            if constexpr (T == 32) {
+                // no exchange: lanes 0..15 of the quarter hold operators 0 and 1 of its
+                // 8 nodes, lanes 16..31 operators 2 and 3 (ens_a_row), and a 16x256b
+                // load hands each thread both members' 16 sums (ens_b_col)
+                fetch(u, ch, o);
+                tc::tmem_ld16x256(taddr, v0);
+                tc::tmem_ld16x256(taddr + (16u << 16), v1);
+                tc::tmem_wait_ld();
+            } else {
                 tc::tmem_ld16(taddr, v0);
                 tc::tmem_ld16(taddr + 16, v1);
                 tc::tmem_wait_ld();
@@ -469,25 +484,37 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                             make_float4(v1[4 * q], v1[4 * q + 1], v1[4 * q + 2], v1[4 * q + 3]);
                     }
                 }
+                // the streamed operands are requested after the exchange stores: issued
+                // before them, the loads hold the stores up in the load/store queue
+                fetch(u, ch, o);
+                __syncwarp();
             }
-            // the streamed operands are requested after the exchange stores: issued
-            // before them, the loads hold the stores up in the load/store queue
-            fetch(u, ch, o);
-            __syncwarp();
 #pragma unroll
             for (int pi = 0; pi < C::kPairs; ++pi) {
-                const int pr = lane + 32 * pi;
-                const int j = pr >> 3, bm = pr & 7;
-                const int t = qt * (T / 4) + j;
+                const int t = pair_node(pi);
                 const long node = (long)tile * T + t;
                 if (node >= a.n) continue;
+                const int bm = pair_member(pi);
                 const int mfb = col0 + ch * 32 + 4 * bm;      // first mf of this member
                 const int member = mfb >> 2;
                 float S[16];
+                if constexpr (T == 32) {
 #pragma unroll
-                for (int o2 = 0; o2 < 4; ++o2) {
-                    const float4 sv = *reinterpret_cast<const float4*>(xch + (4 * j + o2) * C::kXchStride + 4 * bm);
-                    S[4 * o2] = sv.x; S[4 * o2 + 1] = sv.y; S[4 * o2 + 2] = sv.z; S[4 * o2 + 3] = sv.w;
+                    for (int f = 0; f < 4; ++f) {
+                        const int k = 2 * (f >> 1) + pi, b = f & 1;
+                        S[f] = v0[4 * k + b];
+                        S[4 + f] = v0[4 * k + 2 + b];
+                        S[8 + f] = v1[4 * k + b];
+                        S[12 + f] = v1[4 * k + 2 + b];
+                    }
+                } else {
+                    const int j = (lane + 32 * pi) >> 3;
+#pragma unroll
+                    for (int o2 = 0; o2 < 4; ++o2) {
+                        const float4 sv =
+                            *reinterpret_cast<const float4*>(xch + (4 * j + o2) * C::kXchStride + 4 * bm);
+                        S[4 * o2] = sv.x; S[4 * o2 + 1] = sv.y; S[4 * o2 + 2] = sv.z; S[4 * o2 + 3] = sv.w;
+                    }
                 }
                 if constexpr (PREC == kBf16x3) {
                     // the centre term c * sum_k W (3xTF32 accumulates it in its add-back row)
@@ -543,7 +570,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                                     __double2float_rn((double)h4.z + a.dt6 * (double)dw), __double2float_rn(h));
                 }
             }
-            __syncwarp();   // the exchange rows are rewritten by the next chunk
+            if constexpr (T != 32) __syncwarp();   // the exchange rows are rewritten by the next chunk
         };
         constexpr int kCh = C::kN / 64;          // chunks per group per tile
         ens::EpiSet sa;

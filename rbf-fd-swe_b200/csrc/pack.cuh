@@ -8,7 +8,8 @@
 // device once and rearranged there by two kernels into every layout the stage
 // kernels read:
 //   * W / idx:   the 8-lanes-per-node layout (stage_kernel.cuh, stage_tma.cuh),
-//   * Wl / idxl: the tile-transposed node-per-lane layout (stage_lane.cuh),
+//   * Wl / idxl: the tile-transposed node-per-lane layout (stage_lane.cuh), and
+//     idxs, the same indices as 16-bit offsets from each node's own row,
 //   * PT:        the pointwise records [node][kPointStride].
 // Slots j >= nnbr get zero weights and gather the node's own row; nodes past n in
 // the last 32-node tile of Wl / idxl get zero weights and gather row pid0.  An
@@ -33,10 +34,13 @@ struct PackedStatic {
     int* idx = nullptr;   // 8-lanes-per-node indices
     T* Wl = nullptr;      // tile-transposed weights
     int* idxl = nullptr;  // tile-transposed indices
+    short* idxs = nullptr;  // the same as 16-bit offsets from the node's own row
+    bool idxs_ok = false;   // every offset fits 16 bits
     T* PT = nullptr;      // pointwise records
     void release() {
-        for (void* p : {(void*)W, (void*)idx, (void*)Wl, (void*)idxl, (void*)PT}) if (p) cudaFree(p);
-        W = nullptr; idx = nullptr; Wl = nullptr; idxl = nullptr; PT = nullptr;
+        for (void* p : {(void*)W, (void*)idx, (void*)Wl, (void*)idxl, (void*)idxs, (void*)PT}) if (p) cudaFree(p);
+        W = nullptr; idx = nullptr; Wl = nullptr; idxl = nullptr; idxs = nullptr; PT = nullptr;
+        idxs_ok = false;
     }
 };
 
@@ -46,6 +50,7 @@ __global__ void pack_stencils_kernel(const T* __restrict__ Dx, const T* __restri
                                      const T* __restrict__ L, const int* __restrict__ idx_raw, CallerLayout cl,
                                      int n, long npad, int nnbr, int rows, int pid0, T* __restrict__ W,
                                      int* __restrict__ idxp, T* __restrict__ Wl, int* __restrict__ idxl,
+                                     short* __restrict__ idxs, int* __restrict__ wide,
                                      unsigned long long* __restrict__ bad) {
     constexpr int U = Quad<T>::kUnits;
     constexpr int per_unit = 16 / (int)sizeof(T);
@@ -78,6 +83,10 @@ __global__ void pack_stencils_kernel(const T* __restrict__ Dx, const T* __restri
         Wl[unit * per_unit + op % per_unit] = w[op];
     }
     idxl[(b * kSlots + j) * kLaneTile + tt] = p;
+    // 16-bit offset from the node's own row (past n: from row n - 1 + pid0, offset 0)
+    const int off = i < n ? p - ((int)i + pid0) : 0;
+    if (off < -32768 || off > 32767) atomicOr(wide, 1);
+    idxs[(b * kSlots + j) * kLaneTile + tt] = (short)off;
 }
 
 // One thread per node.
@@ -161,21 +170,29 @@ int pack_static_device(const CallerLayout& cl, int n, int rows, int pid0, int nn
         (e = cudaMalloc(&out.idx, (size_t)n * kSlots * sizeof(int))) ||
         (e = cudaMalloc(&out.Wl, (size_t)npad * kSlots * U * per_unit * sizeof(T))) ||
         (e = cudaMalloc(&out.idxl, (size_t)npad * kSlots * sizeof(int))) ||
+        (e = cudaMalloc(&out.idxs, (size_t)npad * kSlots * sizeof(short))) ||
         (e = cudaMalloc(&out.PT, (size_t)n * kPointStride * sizeof(T))))
         return fail(e);
     if ((e = cudaMallocAsync(reinterpret_cast<void**>(&bad), sizeof(*bad), st))) return fail(e);
     owned.push_back(bad);
     if ((e = cudaMemsetAsync(bad, 0xff, sizeof(*bad), st))) return fail(e);
+    int* wide = nullptr;
+    if ((e = cudaMallocAsync(reinterpret_cast<void**>(&wide), sizeof(int), st))) return fail(e);
+    owned.push_back(wide);
+    if ((e = cudaMemsetAsync(wide, 0, sizeof(int), st))) return fail(e);
     const long threads = npad * kSlots;
     pack_stencils_kernel<T><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
-        tDx, tDy, tDz, tL, tidx, cl, n, npad, nnbr, rows, pid0, out.W, out.idx, out.Wl, out.idxl, bad);
+        tDx, tDy, tDz, tL, tidx, cl, n, npad, nnbr, rows, pid0, out.W, out.idx, out.Wl, out.idxl, out.idxs, wide,
+        bad);
     pack_points_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(tx, ty, tz, tf, tghm, tpu, tpv, tpw, tgg, cl,
                                                                       n, out.PT);
     count_launch(2);
     unsigned long long hb = ULLONG_MAX;
+    int hw = 1;
     if ((e = cudaGetLastError()) || (e = cudaMemcpyAsync(&hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, st)) ||
-        (e = cudaStreamSynchronize(st)))
+        (e = cudaMemcpyAsync(&hw, wide, sizeof(hw), cudaMemcpyDeviceToHost, st)) || (e = cudaStreamSynchronize(st)))
         return fail(e);
+    out.idxs_ok = hw == 0;
     drop_staging();
     if (hb != ULLONG_MAX) {
         const long i = (long)(hb >> 32);

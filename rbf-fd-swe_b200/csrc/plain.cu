@@ -95,6 +95,9 @@ struct Plain {
          *Kx = nullptr, *raw = nullptr, *Wl = nullptr;
     int* idx = nullptr;
     int* idxl = nullptr;            // node-per-lane kernel: tile-transposed weights / indices
+    short* idxs = nullptr;          // the same indices as 16-bit offsets from each node's own row
+    bool idxs_fit = false;          // every offset fits 16 bits
+    bool idxs_ok = false;           // the kernel reads idxs (idxs_fit, unless 32-bit indices were asked for)
     int* halo_send = nullptr;       // patch rows this rank sends / receives (swe_cuda_halo_setup)
     int* halo_recv = nullptr;
     int n_send = 0, n_recv = 0;
@@ -134,6 +137,7 @@ struct Plain {
         n_send = n_recv = 0;
         if (idx) cudaFree(idx);
         if (idxl) cudaFree(idxl);
+        if (idxs) cudaFree(idxs);
         if (inv) cudaFree(inv);
         if (err) cudaFree(err);
         if (err_host) cudaFreeHost(err_host);
@@ -141,6 +145,8 @@ struct Plain {
         W = PT = H = Ka = Kb = D = F = Kx = raw = Wl = nullptr;
         idx = nullptr;
         idxl = nullptr;
+        idxs = nullptr;
+        idxs_fit = idxs_ok = false;
         lane_lpn = 1;
         lane_pf = 0;
         lane_minb = 4;
@@ -240,7 +246,12 @@ struct Plain {
 
     template <typename T, int LPN, int MINB>
     void launch_lane(const StageArgs<T>& a, int mode) {
-        const LaneArgs<T> la{a, reinterpret_cast<const uint4*>(Wl), idxl, lane_pf};
+        if (idxs_ok) launch_lane_i<T, LPN, MINB, true>(a, mode);
+        else launch_lane_i<T, LPN, MINB, false>(a, mode);
+    }
+    template <typename T, int LPN, int MINB, bool I16>
+    void launch_lane_i(const StageArgs<T>& a, int mode) {
+        const LaneArgs<T> la{a, reinterpret_cast<const uint4*>(Wl), idxl, idxs, lane_pf};
         const int units = ceil_div(n, kLaneTile / LPN);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(ceil_div(units, kLaneWarps));
@@ -253,11 +264,11 @@ struct Plain {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         switch (mode) {
-            case 0: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage0, LPN, MINB>, la); break;
-            case 1: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage1, LPN, MINB>, la); break;
-            case 2: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage2, LPN, MINB>, la); break;
-            case 3: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage3, LPN, MINB>, la); break;
-            default: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kEvalOnly, LPN, MINB>, la); break;
+            case 0: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage0, LPN, MINB, I16>, la); break;
+            case 1: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage1, LPN, MINB, I16>, la); break;
+            case 2: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage2, LPN, MINB, I16>, la); break;
+            case 3: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kStage3, LPN, MINB, I16>, la); break;
+            default: cudaLaunchKernelEx(&cfg, stage_lane_kernel<T, kEvalOnly, LPN, MINB, I16>, la); break;
         }
     }
 
@@ -369,6 +380,8 @@ static int upload_static(Plain& P, const void* x, const void* y, const void* z, 
     P.idx = ps.idx;
     P.Wl = ps.Wl;
     P.idxl = ps.idxl;
+    P.idxs = ps.idxs;
+    P.idxs_fit = P.idxs_ok = ps.idxs_ok;
     P.PT = ps.PT;
     P.tma_ok = true;
     {
@@ -762,6 +775,24 @@ int swe_cuda_select_kernel(int which) {
     return P.build_graph();
 }
 
+int swe_cuda_set_index_width(int bits) {
+    SWE_TRY(require_ready());
+    Plain& P = g_plain;
+    if (bits != 16 && bits != 32) {
+        set_error("swe_cuda_set_index_width: 16 or 32, got %d", bits);
+        return SWE_ERR_ARG;
+    }
+    if (bits == 16 && !P.idxs_fit) {
+        set_error("swe_cuda_set_index_width: a stencil row lies more than 32767 rows from its node");
+        return SWE_ERR_ARG;
+    }
+    SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
+    P.idxs_ok = bits == 16;
+    if (P.graph) cudaGraphExecDestroy(P.graph);
+    P.graph = nullptr;
+    return P.build_graph();
+}
+
 int swe_cuda_kernel_info(int* out) {
     SWE_TRY(require_ready());
     if (!out) { set_error("null out"); return SWE_ERR_ARG; }
@@ -773,6 +804,7 @@ int swe_cuda_kernel_info(int* out) {
     out[5] = (int)(g_plain.tune_us[2] * 1000.f);   // node-per-lane
     out[6] = g_plain.lane_pf;
     out[7] = g_plain.lane_minb;
+    out[8] = g_plain.idxs_ok ? 1 : 0;
     return SWE_OK;
 }
 

@@ -822,6 +822,9 @@ int swe_srv_add_grid(int n, int nnbr, double gh0, double dt, const int* idx, con
     G.PT = ps.PT;
     G.Wl = ps.Wl;
     G.idxl = ps.idxl;
+    // the 16-bit offsets are not read here: a second index path in the persistent
+    // kernel raises its register demand past the 128 it runs at
+    cudaFree(ps.idxs);
     std::lock_guard<std::mutex> lock(g_srv->mu);
     g_srv->grids.push_back(G);
     return (int)g_srv->grids.size() - 1;

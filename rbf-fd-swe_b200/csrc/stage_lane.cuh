@@ -36,6 +36,7 @@ struct LaneArgs {
     StageArgs<T> s;
     const uint4* Wl;   // [tile][slot][unit][32 nodes] 16-byte units (FP64: (Dx,Dy), (Dz,L); FP32: all four)
     const int* idxl;   // [tile][slot][32 nodes] gather rows
+    const short* idxs; // the same as 16-bit offsets from the node's own row (clamped to n - 1)
     int l2_prefetch;   // 1: bulk L2 prefetch of each warp's contiguous blocks at its start
 };
 
@@ -44,6 +45,11 @@ namespace lane {
 __device__ __forceinline__ int ld_stream(const int* p) {
     int v;
     asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ int ld_stream(const short* p) {
+    short v;
+    asm volatile("ld.global.nc.L1::no_allocate.b16 %0, [%1];" : "=h"(v) : "l"(p));
     return v;
 }
 __device__ __forceinline__ double2 ld_stream(const double2* p) {
@@ -70,7 +76,9 @@ __device__ __forceinline__ void weights(const uint4* u, float (&w)[4]) {
 }
 }  // namespace lane
 
-template <typename T, int MODE, int LPN, int MINB>
+// I16: read the gather rows from the 16-bit offsets (half the index bytes); every
+// patch whose stencil rows lie within 32767 rows of their node (any RCM-ordered grid)
+template <typename T, int MODE, int LPN, int MINB, bool I16>
 __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const LaneArgs<T> la) {
     static_assert(LPN == 1 || LPN == 2 || LPN == 4, "1, 2 or 4 lanes per node");
     constexpr int kNpw = 32 / LPN;          // nodes per warp
@@ -87,13 +95,14 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
     // the previous stage), then its pointwise records and own / H / D rows.  That
     // pays on small patches (latency-bound); on large ones the extra requests
     // compete with the demand loads, so the init-time timing decides.
-    constexpr uint32_t kTileW = kSlots * U * kLaneTile * 16, kTileI = kSlots * kLaneTile * 4;
+    constexpr uint32_t kTileW = kSlots * U * kLaneTile * 16, kTileI = kSlots * kLaneTile * (I16 ? 2 : 4);
     const bool pf = la.l2_prefetch != 0;
     if (pf && lane == 0 && nvalid > 0) {
         const long tb = node0 / kLaneTile;
         const int wt = (int)(node0 % kLaneTile) / kNpw;        // warp within its tile
         prefetch_l2_bulk(reinterpret_cast<const unsigned char*>(la.Wl) + tb * kTileW + wt * (kTileW / LPN), kTileW / LPN);
-        prefetch_l2_bulk(reinterpret_cast<const unsigned char*>(la.idxl) + tb * kTileI + wt * (kTileI / LPN), kTileI / LPN);
+        const void* ib = I16 ? static_cast<const void*>(la.idxs) : static_cast<const void*>(la.idxl);
+        prefetch_l2_bulk(reinterpret_cast<const unsigned char*>(ib) + tb * kTileI + wt * (kTileI / LPN), kTileI / LPN);
         prefetch_l2_bulk(a.PT + node0 * kPointStride, (uint32_t)(nvalid * kPointStride * sizeof(T)));
     }
     pdl_wait();                // neighbour states and H / D come from the previous stage
@@ -113,13 +122,15 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
     const long tile = i / kLaneTile;
     const int t = (int)(i % kLaneTile);
     const int* ip = la.idxl + (tile * kSlots + sub) * kLaneTile + t;
+    const short* sp = la.idxs + (tile * kSlots + sub) * kLaneTile + t;
+    const int own = (int)min(i, (long)a.n - 1) + a.pid0;   // the row the 16-bit offsets start from
     const uint4* wp = la.Wl + (tile * kSlots + sub) * U * kLaneTile + t;
     T acc[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) acc[q] = T(0);
 #pragma unroll
     for (int jj = 0; jj < kJpl; ++jj) {
-        const int p = lane::ld_stream(ip + jj * LPN * kLaneTile);
+        const int p = I16 ? own + lane::ld_stream(sp + jj * LPN * kLaneTile) : lane::ld_stream(ip + jj * LPN * kLaneTile);
         T w[4], kv[4];
         lane::weights(wp + jj * LPN * U * kLaneTile, w);
         Quad<T>::load_row(a.Kin + 4L * p, kv);

@@ -99,6 +99,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
     for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(r[t]);
 }
+// 16 lanes x 256 bits, 4 times along the columns (32 columns): thread i gets lanes
+// l = i / 4 and l + 8 of the 16 starting at taddr's lane, columns 8 k + 2 (i % 4) + b:
+// v[4 k + b] from lane l, v[4 k + 2 + b] from lane l + 8 (k = 0..3, b = 0, 1)
+__device__ __forceinline__ void tmem_ld16x256(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(r[t]);
+}
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // ---- mbarrier -----------------------------------------------------------------------

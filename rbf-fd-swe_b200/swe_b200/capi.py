@@ -74,6 +74,7 @@ def load() -> ctypes.CDLL:
     lib.swe_cuda_stream.restype = vp
     lib.swe_cuda_select_kernel.argtypes = [i]
     lib.swe_cuda_kernel_info.argtypes = [vp]
+    lib.swe_cuda_set_index_width.argtypes = [i]
     lib.swe_hist_open.argtypes = [ctypes.c_char_p, i]
     lib.swe_gen_stencils.argtypes = [i, i, vp, vp]
     lib.swe_selftest_wait_timeout.argtypes = [d, vp]
@@ -256,12 +257,17 @@ class Plain:
         s = li + (3 if ctas_per_sm == 5 else 0) + (6 if l2_prefetch else 0)
         return 6 + s
 
+    def set_index_width(self, bits: int) -> None:
+        """16: the node-per-lane kernel reads stencil rows as 16-bit offsets from each node's
+        own row (the default when every offset fits); 32: as the 32-bit indices."""
+        check("swe_cuda_set_index_width", self.lib.swe_cuda_set_index_width(int(bits)))
+
     def kernel_info(self) -> dict:
-        out = np.zeros(8, dtype=np.int32)
+        out = np.zeros(9, dtype=np.int32)
         check("swe_cuda_kernel_info", self.lib.swe_cuda_kernel_info(_p(out)))
         return {"in_use": ("pipelined", "register", "lane")[int(out[0])], "pipelined_available": bool(out[1]),
                 "pipelined_tile": int(out[1]), "lanes_per_node": int(out[4]), "l2_prefetch": bool(out[6]),
-                "ctas_per_sm": int(out[7]),
+                "ctas_per_sm": int(out[7]), "index_offsets_16bit": bool(out[8]),
                 "tune_us": {"pipelined": out[2] / 1e3, "register": out[3] / 1e3, "lane": out[5] / 1e3}}
 
     def invariants(self) -> np.ndarray:

@@ -28,3 +28,13 @@ def test_tensor_roofline_counts_every_chunk_product():
 
 def test_spec_fraction_uses_8_tbs():
     assert bench.SPEC_HBM_GBS == 8000.0
+
+
+def test_plain_bytes_follow_the_index_width():
+    lane16 = {"in_use": "lane", "index_offsets_16bit": True}
+    lane32 = {"in_use": "lane", "index_offsets_16bit": False}
+    assert bench.plain_alg_bytes("fp64", lane16) == 4 * 31 * 8 + 31 * 2 + 17 * 8 + 4 * 8 + 14 * 8
+    assert bench.plain_alg_bytes("fp64", lane32) == 1396
+    assert bench.plain_alg_bytes("fp32", lane16) == 760 - 62
+    # the other kernels read 32-bit indices whatever the lane kernel would read
+    assert bench.plain_alg_bytes("fp64", {"in_use": "pipelined", "index_offsets_16bit": True}) == 1396

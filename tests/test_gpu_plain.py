@@ -276,6 +276,48 @@ def test_pipelined_and_register_kernels_agree_bitwise(plain, prec):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_lane_kernel_16bit_offsets_equal_32bit_indices(plain, prec):
+    """The node-per-lane kernel reads the stencil rows as 16-bit offsets from each node's
+    own row when every offset fits (the RCM order keeps them within about 1500 rows at
+    N=40962). Both widths name the same rows, so eval_rhs and 7 RK4 steps agree bit for
+    bit with every lanes-per-node shape. In the generator's own order the offsets reach
+    38432 rows: the library falls back to 32-bit indices and refuses 16."""
+    _, d = generated_input(6)
+    m0 = swe_input.to_model(d)
+    m, _ = layout.prepare(m0, use_rcm=True, simd_length=32)
+    assert np.abs(m.idx.reshape(m.N, -1) - np.arange(m.N)[:, None]).max() <= 32767
+    plain.init_model(m, prec)
+    assert plain.kernel_info()["index_offsets_16bit"]
+    dt = np.float64 if prec == "fp64" else np.float32
+    K = _perturbed(m.H_init).astype(dt)
+    for lpn in (1, 2, 4):
+        plain.select_kernel(capi.Plain.lane_shape(lpn))
+        res = {}
+        for bits in (16, 32):
+            plain.set_index_width(bits)
+            assert plain.kernel_info()["index_offsets_16bit"] == (bits == 16)
+            F = plain.eval_rhs(K)
+            plain.set_state(m.H_init.astype(dt))
+            plain.step(7)
+            res[bits] = (F, plain.get_state())
+        assert np.array_equal(res[16][0], res[32][0]), lpn
+        assert np.array_equal(res[16][1], res[32][1]), lpn
+    plain.set_index_width(16)
+    m_raw, _ = layout.prepare(m0, use_rcm=False, simd_length=32)
+    assert np.abs(m_raw.idx.reshape(m_raw.N, -1) - np.arange(m_raw.N)[:, None]).max() > 32767
+    plain.init_model(m_raw, prec)
+    plain.select_kernel(capi.Plain.lane_shape(1))
+    assert not plain.kernel_info()["index_offsets_16bit"]
+    with pytest.raises(capi.SweError) as e:
+        plain.set_index_width(16)
+    assert capi.STATUS[e.value.status] == "SWE_ERR_ARG"
+    plain.set_index_width(32)
+    F = plain.eval_rhs(m_raw.H_init.astype(dt))
+    if prec == "fp64":
+        assert rel_err(F, oracle.Port(m_raw, "fp64").eval_rhs(m_raw.H_init)).max() <= 1e-12
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_lane_kernel_matches_oracle(plain, prec):
     """The node-per-lane kernel sums each node's slots serially per lane (1, 2 or 4
     lanes per node) instead of in the 8-lane tree, so it is held to the oracle's bars
