@@ -135,8 +135,9 @@ int swe_cuda_sync(void);
  * contiguous blocks into L2 at its start).  swe_cuda_init times every kernel
  * and shape on the patch, keeps the fastest shape of each, and uses the fastest
  * kernel.  info[9] = {kernel in use (0/1/2), pipelined tile in nodes (0 if
- * unavailable), ns per eval launch of kernel 0 (its fastest tile), of kernel 1,
- * lanes per node of kernel 2, ns per eval launch of kernel 2 (its fastest
+ * unavailable), ns per stage launch of kernel 0 (its fastest tile; stages 0-2
+ * chained as in a step), of kernel 1, lanes per node of kernel 2, ns per stage
+ * launch of kernel 2 (its fastest
  * shape), kernel 2's L2 prefetch (0/1), kernel 2's CTAs per SM (3/4/5),
  * kernel 2 reads its gather rows as 16-bit offsets from each node's own row
  * (1: every stencil row lies within 32767 rows of its node, as in any

@@ -106,7 +106,7 @@ struct Plain {
     int* err_host = nullptr;        // pinned copy of it, read back with the state
     bool tma_ok = false;            // pipelined kernel set up
     int kernel_choice = 0;          // 0 = bulk-copy pipelined, 1 = register-streaming, 2 = node-per-lane kernel
-    float tune_us[3] = {0.f, 0.f, 0.f};  // eval-mode launch time of each kernel at init (its best shape)
+    float tune_us[3] = {0.f, 0.f, 0.f};  // stage launch time of each kernel at init (its best shape)
     int lane_lpn = 1;               // node-per-lane kernel: lanes per node (1, 2, 4)
     int lane_pf = 0;                // node-per-lane kernel: bulk L2 prefetch at warp start
     int lane_minb = 4;              // node-per-lane kernel: CTAs per SM of its register bound (3, 4, 5)
@@ -544,15 +544,20 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
             if (c < 3) { P.kernel_choice = 0; P.tma_tile = cand_tile[c]; }
             else if (c == 3) P.kernel_choice = 1;
             else lane_shape(P, c - kLane0);
-            for (int w = 0; w < 2; ++w) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
+            // stages 0, 1 and 2 chained as a step chains them (none of them writes H):
+            // one sequence to warm up, then three timed
+            auto stages = [&]() {
+                for (int s = 0; s < 3; ++s) { if (fsize == 8) P.launch_t<double>(s); else P.launch_t<float>(s); }
+            };
+            stages();
             SWE_CUDA_TRY(cudaEventRecord(e0, P.stream));
-            for (int r = 0; r < 10; ++r) { if (fsize == 8) P.launch_t<double>(kEvalOnly); else P.launch_t<float>(kEvalOnly); }
+            for (int r = 0; r < 3; ++r) stages();
             SWE_CUDA_TRY(cudaEventRecord(e1, P.stream));
             SWE_CUDA_TRY(cudaEventSynchronize(e1));
             SWE_CUDA_TRY(cudaGetLastError());
             float ms = 0.f;
             SWE_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-            us_c[c] = ms * 1e3f / 10.f;
+            us_c[c] = ms * 1e3f / 9.f;
         }
         count_launch(12 * kCand);
         cudaEventDestroy(e0);
@@ -562,8 +567,16 @@ int swe_cuda_init(int fsize, int layout, int simd_length, int compute_size, int 
         int bt = 0, bl = kLane0;
         for (int c = 1; c < 3; ++c)
             if (us_c[c] < us_c[bt]) bt = c;
-        for (int c = kLane0 + 1; c < kCand; ++c)
-            if (us_c[c] < us_c[bl]) bl = c;
+        // a shape with the L2 prefetch must beat the best one without by 3 %: timed
+        // back to back the two come within a few per cent, while a step that starts
+        // from a cold L2 runs 9 % faster without (N=40962)
+        int bp = -1;
+        for (int c = kLane0; c < kCand; ++c) {
+            lane_shape(P, c - kLane0);
+            if (P.lane_pf) { if (bp < 0 || us_c[c] < us_c[bp]) bp = c; }
+            else if (us_c[c] < us_c[bl]) bl = c;
+        }
+        if (bp >= 0 && us_c[bp] < 0.97f * us_c[bl]) bl = bp;
         P.tma_tile = cand_tile[bt];
         lane_shape(P, bl - kLane0);
         P.tune_us[0] = us_c[bt];
@@ -798,7 +811,7 @@ int swe_cuda_kernel_info(int* out) {
     if (!out) { set_error("null out"); return SWE_ERR_ARG; }
     out[0] = g_plain.kernel_choice;
     out[1] = g_plain.tma_ok ? g_plain.tma_tile : 0;
-    out[2] = (int)(g_plain.tune_us[0] * 1000.f);   // nanoseconds per eval launch, pipelined
+    out[2] = (int)(g_plain.tune_us[0] * 1000.f);   // nanoseconds per stage launch, pipelined
     out[3] = (int)(g_plain.tune_us[1] * 1000.f);   // register-streaming
     out[4] = g_plain.lane_lpn;
     out[5] = (int)(g_plain.tune_us[2] * 1000.f);   // node-per-lane

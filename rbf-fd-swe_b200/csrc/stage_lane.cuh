@@ -105,6 +105,26 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
         prefetch_l2_bulk(reinterpret_cast<const unsigned char*>(ib) + tb * kTileI + wt * (kTileI / LPN), kTileI / LPN);
         prefetch_l2_bulk(a.PT + node0 * kPointStride, (uint32_t)(nvalid * kPointStride * sizeof(T)));
     }
+    // a warp's nodes lie in one tile of the packed arrays (kNpw divides 32); nodes
+    // past n in the last tile have zero weights and gather a valid row
+    const long i = node0 + tl;
+    const long tile = i / kLaneTile;
+    const int t = (int)(i % kLaneTile);
+    const int* ip = la.idxl + (tile * kSlots + sub) * kLaneTile + t;
+    const short* sp = la.idxs + (tile * kSlots + sub) * kLaneTile + t;
+    const int own = (int)min(i, (long)a.n - 1) + a.pid0;   // the row the 16-bit offsets start from
+    // the gather rows are static: with 2 or 4 lanes per node (16 or 8 rows a lane) they
+    // are read before the wait, so that the gathers issue as soon as the previous
+    // stage's states are visible (32 rows a lane would spill)
+    constexpr bool kEarlyRows = LPN > 1;
+    auto row = [&](int jj) {
+        return I16 ? own + lane::ld_stream(sp + jj * LPN * kLaneTile) : lane::ld_stream(ip + jj * LPN * kLaneTile);
+    };
+    int prow[kEarlyRows ? kJpl : 1];
+    if (kEarlyRows && nvalid > 0) {
+#pragma unroll
+        for (int jj = 0; jj < kJpl; ++jj) prow[kEarlyRows ? jj : 0] = row(jj);
+    }
     pdl_wait();                // neighbour states and H / D come from the previous stage
     pdl_trigger();
     if (nvalid <= 0) return;
@@ -116,21 +136,13 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
             prefetch_l2_bulk(a.D + 4 * node0, rows);
         }
     }
-    // a warp's nodes lie in one tile of the packed arrays (kNpw divides 32); nodes
-    // past n in the last tile have zero weights and gather a valid row
-    const long i = node0 + tl;
-    const long tile = i / kLaneTile;
-    const int t = (int)(i % kLaneTile);
-    const int* ip = la.idxl + (tile * kSlots + sub) * kLaneTile + t;
-    const short* sp = la.idxs + (tile * kSlots + sub) * kLaneTile + t;
-    const int own = (int)min(i, (long)a.n - 1) + a.pid0;   // the row the 16-bit offsets start from
     const uint4* wp = la.Wl + (tile * kSlots + sub) * U * kLaneTile + t;
     T acc[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) acc[q] = T(0);
 #pragma unroll
     for (int jj = 0; jj < kJpl; ++jj) {
-        const int p = I16 ? own + lane::ld_stream(sp + jj * LPN * kLaneTile) : lane::ld_stream(ip + jj * LPN * kLaneTile);
+        const int p = kEarlyRows ? prow[kEarlyRows ? jj : 0] : row(jj);
         T w[4], kv[4];
         lane::weights(wp + jj * LPN * U * kLaneTile, w);
         Quad<T>::load_row(a.Kin + 4L * p, kv);
