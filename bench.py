@@ -111,7 +111,7 @@ TRAFFIC_BYTES = {
     # steps (ncu --cache-control none inside the bench's own flushed loop, so
     # stage 0 of each step starts cold and stages 1-3 see what L2 kept; plain
     # kernels reading the stencil rows as 16-bit offsets)
-    "plain_fp64_n40962": 29.64e6,       # swe::stage_lane_kernel<double, *, 2, 5, true>, L2 prefetch on
+    "plain_fp64_n40962": 46.58e6,       # swe::stage_lane_kernel<double, *, 2, 5, true>, no L2 prefetch
     "plain_fp64_n163842": 186.95e6,     # swe::stage_lane_kernel<double, *, 2, 4, true>
     "plain_fp64_n655362": 905.71e6,     # swe::stage_lane_kernel<double, *, 2, 4, true>
     "plain_fp32_n655362": 461.12e6,     # swe::stage_lane_kernel<float, *, 1, 4, true>
