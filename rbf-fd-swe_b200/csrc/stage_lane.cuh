@@ -113,10 +113,11 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
     const int* ip = la.idxl + (tile * kSlots + sub) * kLaneTile + t;
     const short* sp = la.idxs + (tile * kSlots + sub) * kLaneTile + t;
     const int own = (int)min(i, (long)a.n - 1) + a.pid0;   // the row the 16-bit offsets start from
-    // the gather rows are static: with 2 or 4 lanes per node (16 or 8 rows a lane) they
-    // are read before the wait, so that the gathers issue as soon as the previous
-    // stage's states are visible (32 rows a lane would spill)
-    constexpr bool kEarlyRows = LPN > 1;
+    // the gather rows are static: with 2 or 4 lanes per node (16 or 8 rows a lane), or
+    // at 3 CTAs per SM (168 registers), they are read before the wait, so that the
+    // gathers issue as soon as the previous stage's states are visible (32 rows a
+    // lane in 96 or 128 registers would spill)
+    constexpr bool kEarlyRows = LPN > 1 || MINB <= 3;
     auto row = [&](int jj) {
         return I16 ? own + lane::ld_stream(sp + jj * LPN * kLaneTile) : lane::ld_stream(ip + jj * LPN * kLaneTile);
     };
