@@ -251,7 +251,7 @@ struct Plain {
     }
     template <typename T, int LPN, int MINB, bool I16>
     void launch_lane_i(const StageArgs<T>& a, int mode) {
-        const LaneArgs<T> la{a, reinterpret_cast<const uint4*>(Wl), idxl, idxs, lane_pf};
+        const LaneArgs<T> la{a, reinterpret_cast<const uint4*>(Wl), idxl, idxs, lane_pf, nnbr};
         const int units = ceil_div(n, kLaneTile / LPN);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(ceil_div(units, kLaneWarps));

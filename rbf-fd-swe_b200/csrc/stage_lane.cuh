@@ -38,6 +38,7 @@ struct LaneArgs {
     const int* idxl;   // [tile][slot][32 nodes] gather rows
     const short* idxs; // the same as 16-bit offsets from the node's own row (clamped to n - 1)
     int l2_prefetch;   // 1: bulk L2 prefetch of each warp's contiguous blocks at its start
+    int nnbr;          // stencil slots in use: slots nnbr.. hold zero weights (a lane's last one is not read)
 };
 
 namespace lane {
@@ -124,7 +125,8 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
     int prow[kEarlyRows ? kJpl : 1];
     if (kEarlyRows && nvalid > 0) {
 #pragma unroll
-        for (int jj = 0; jj < kJpl; ++jj) prow[kEarlyRows ? jj : 0] = row(jj);
+        for (int jj = 0; jj < kJpl; ++jj)
+            prow[kEarlyRows ? jj : 0] = jj < kJpl - 1 || jj * LPN + sub < la.nnbr ? row(jj) : own;
     }
     pdl_wait();                // neighbour states and H / D come from the previous stage
     pdl_trigger();
@@ -143,6 +145,10 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
     for (int q = 0; q < 16; ++q) acc[q] = T(0);
 #pragma unroll
     for (int jj = 0; jj < kJpl; ++jj) {
+        // a padding slot (zero weights) in a lane's last iteration moves no bytes (slot 31
+        // of 31-neighbour stencils); a test in every iteration would keep the compiler
+        // from issuing the other iterations' loads together
+        if (jj == kJpl - 1 && jj * LPN + sub >= la.nnbr) continue;
         const int p = kEarlyRows ? prow[kEarlyRows ? jj : 0] : row(jj);
         T w[4], kv[4];
         lane::weights(wp + jj * LPN * U * kLaneTile, w);
