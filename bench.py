@@ -111,10 +111,10 @@ TRAFFIC_BYTES = {
     # steps (ncu --cache-control none inside the bench's own flushed loop, so
     # stage 0 of each step starts cold and stages 1-3 see what L2 kept; plain
     # kernels reading the stencil rows as 16-bit offsets)
-    "plain_fp64_n40962": 46.58e6,       # swe::stage_lane_kernel<double, *, 2, 5, true>, no L2 prefetch
-    "plain_fp64_n163842": 186.95e6,     # swe::stage_lane_kernel<double, *, 2, 4, true>
-    "plain_fp64_n655362": 905.71e6,     # swe::stage_lane_kernel<double, *, 2, 4, true>
-    "plain_fp32_n655362": 461.12e6,     # swe::stage_lane_kernel<float, *, 1, 4, true>
+    "plain_fp64_n40962": 45.27e6,       # swe::stage_lane_kernel<double, *, 2, 5, true>
+    "plain_fp64_n163842": 181.62e6,     # swe::stage_lane_kernel<double, *, 1, 3, true>
+    "plain_fp64_n655362": 887.10e6,     # swe::stage_lane_kernel<double, *, 1, 4, true>
+    "plain_fp32_n655362": 452.35e6,     # swe::stage_lane_kernel<float, *, 1, 5, true>
     # swe::ens_stage_kernel<32, 64, stage, 3xTF32>, 12 launches (cold); 707 MB of it is
     # the streamed A-operand image (16 KB per 16-row chunk, 43128 chunks)
     "ens_tf32_n163842_b64": 1668.31e6,
