@@ -60,6 +60,7 @@ struct alignas(16) ReqDesc {   // device table entry of an admitted request
     const uint4* Wl;     // grid: tile-transposed weights (node-per-lane split)
     const int* idxl;     // grid: tile-transposed stencil indices
     int n;               // nodes
+    int nnbr;            // stencil slots in use (slot 31 of 31-neighbour stencils is padding)
     int members;
     int chunk_nodes;     // nodes per work item
     int per_stage;       // items per stage: chunks x member blocks
@@ -171,6 +172,8 @@ __device__ void serve_lanes(const ReqDesc& r, int stage, long base, long end, lo
         for (int q = 0; q < 16; ++q) acc[m][q] = 0.0;
 #pragma unroll
     for (int jj = 0; jj < kSlots / kSrvLpn; ++jj) {
+        // a padding slot (zero weights) in a lane's last iteration moves no bytes
+        if (jj == kSlots / kSrvLpn - 1 && jj * kSrvLpn + sub >= r.nnbr) continue;
         const int p = lane::ld_stream(ip + jj * kSrvLpn * kLaneTile);
         double w[4];
         lane::weights(wp + jj * kSrvLpn * 2 * kLaneTile, w);
@@ -525,6 +528,7 @@ struct Server {
         d.Wl = reinterpret_cast<const uint4*>(G.Wl);
         d.idxl = G.idxl;
         d.n = G.n;
+        d.nnbr = G.nnbr;
         d.members = r.members;
         d.chunk_nodes = chunk_nodes(G.n);
         d.nchunks = (G.n + d.chunk_nodes - 1) / d.chunk_nodes;
