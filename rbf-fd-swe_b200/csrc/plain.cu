@@ -104,6 +104,7 @@ struct Plain {
     double* inv = nullptr;
     int* err = nullptr;             // pipelined kernel: bounded-wait error word
     int* err_host = nullptr;        // pinned copy of it, read back with the state
+    bool err_pending = false;       // a pipelined launch since the error word was last read
     bool tma_ok = false;            // pipelined kernel set up
     int kernel_choice = 0;          // 0 = bulk-copy pipelined, 1 = register-streaming, 2 = node-per-lane kernel
     float tune_us[3] = {0.f, 0.f, 0.f};  // stage launch time of each kernel at init (its best shape)
@@ -142,6 +143,7 @@ struct Plain {
         if (err) cudaFree(err);
         if (err_host) cudaFreeHost(err_host);
         err_host = nullptr;
+        err_pending = false;
         W = PT = H = Ka = Kb = D = F = Kx = raw = Wl = nullptr;
         idx = nullptr;
         idxl = nullptr;
@@ -292,6 +294,7 @@ struct Plain {
             return;
         }
         if (use_tma()) {
+            err_pending = true;
             if (tma_tile == 32) launch_tma<T, 32>(a, mode);
             else if (tma_tile == 16) launch_tma<T, 16>(a, mode);
             else launch_tma<T, 64>(a, mode);
@@ -401,13 +404,16 @@ static int upload_static(Plain& P, const void* x, const void* y, const void* z, 
 // back enqueue their copy first, so one synchronisation serves both).
 static int check_tma_err() {
     Plain& P = g_plain;
-    if (!P.err || !P.err_host) {
+    // only the pipelined kernel writes the word: read it back (one more small copy before
+    // the synchronisation) only after such a launch
+    if (!P.err || !P.err_host || !P.err_pending) {
         SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
         return SWE_OK;
     }
     SWE_CUDA_TRY(cudaMemcpyAsync(P.err_host, P.err, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
     SWE_CUDA_TRY(cudaStreamSynchronize(P.stream));
     const int h = *P.err_host;
+    P.err_pending = h != 0;   // a timeout stays reported until the word is cleared
     if (h) {
         set_error("stage kernel: a bounded wait on the bulk-copy pipeline ran out (code %d)", h);
         return SWE_ERR_TIMEOUT;
@@ -666,6 +672,7 @@ int swe_cuda_step(int nsteps) {
         for (auto& e : P.step_ev) if (!e) SWE_CUDA_TRY(cudaEventCreate(&e));
         SWE_CUDA_TRY(cudaEventRecord(P.step_ev[0], P.stream));
     }
+    if (P.use_tma()) P.err_pending = true;
     for (int s = 0; s < nsteps; ++s) {
         SWE_CUDA_TRY(cudaGraphLaunch(P.graph, P.stream));
         SWE_TRY(after_step());
