@@ -93,9 +93,10 @@ __global__ void __launch_bounds__(kLaneThreads, MINB) stage_lane_kernel(const La
     // With l2_prefetch, one lane requests the warp's contiguous blocks into L2 up
     // front, so that the loads below wait on L2 rather than DRAM: this warp's share
     // of its tile's weight and index blocks (static: before the wait, overlapping
-    // the previous stage), then its pointwise records and own / H / D rows.  That
-    // pays on small patches (latency-bound); on large ones the extra requests
-    // compete with the demand loads, so the init-time timing decides.
+    // the previous stage), then its pointwise records and own / H / D rows.  On large
+    // patches the extra requests compete with the demand loads; on small ones it
+    // gains little now that the gather rows are read before the wait, so the
+    // init-time timing keeps it only where it is clearly faster.
     constexpr uint32_t kTileW = kSlots * U * kLaneTile * 16, kTileI = kSlots * kLaneTile * (I16 ? 2 : 4);
     const bool pf = la.l2_prefetch != 0;
     if (pf && lane == 0 && nvalid > 0) {
