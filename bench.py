@@ -23,9 +23,10 @@ rank steps its own state, time is the max over ranks, value is the sum.
 
 The default run also carries the targets quoted for the larger workloads, in
 `targets`: the plain FP64 form at N=163842 and N=655362 (data far beyond L2, so
-their roofline is an HBM roofline) and the 64-member 3xTF32 batched form at
-N=163842 (member-steps/s, its ratio to the plain FP64 form on the same grid, and
-the h error of all 64 members after 1000 steps against the plain FP64 GPU run).
+their roofline is an HBM roofline) and the 64-member batched form at N=163842 in
+3xTF32 and in split FP16 (member-steps/s, the ratio to the plain FP64 form on the
+same grid, and the h error of all 64 members after 1000 steps against the plain
+FP64 GPU run).
 The default workload's own data (57 MB of algorithmic bytes per stage) fits the
 126 MB L2, so its roofline is labelled L2-resident.
 
@@ -62,6 +63,8 @@ WORKLOADS = {
     "ens_tf32_n40962_b64": (6, "tf32x3", "batched ensemble, N=40962 (level 6), 64 members, 3xTF32 on tcgen05, dt=225 s"),
     "ens_bf16_n163842_b64": (7, "bf16x3", "batched ensemble, N=163842 (level 7), 64 members, split BF16 on tcgen05, "
                                           "dt=120 s"),
+    "ens_fp16_n163842_b64": (7, "fp16x3", "batched ensemble, N=163842 (level 7), 64 members, split FP16 with "
+                                          "power-of-two scales on tcgen05, dt=120 s"),
     "serve_mix": (0, "serve", "serving: Poisson arrivals over N in {2562, 10242, 40962, 163842}, 1-32 members, "
                               "10-500 steps, 80 GB budget, FP64"),
 }
@@ -121,6 +124,9 @@ TRAFFIC_BYTES = {
     # swe::ens_stage_kernel<32, 64, stage, BF16>, 12 launches (cold); 353 MB of it is the
     # streamed A-operand image (8 KB per 16-row chunk)
     "ens_bf16_n163842_b64": 1294.82e6,
+    # swe::ens_stage_kernel<32, 64, stage, FP16>, 12 launches (cold); 353 MB of it is the
+    # streamed A-operand image (8 KB per 16-row chunk)
+    "ens_fp16_n163842_b64": 1297.55e6,
 }
 
 
@@ -220,7 +226,7 @@ def ensemble_tensor_roofline(cfg: dict, members: int, precision: str, t_stage: f
     """Tensor-core side of the batched kernel: the MMA work one stage issues (every 16-row
     chunk: M = 4 x tile nodes, N = 4 x members over the member blocks, K = 16, three
     products) over the stage time, against the dense peak of the MMA kind (TF32 runs at half
-    the BF16 rate)."""
+    the BF16 rate, FP16 at the BF16 rate)."""
     flops = cfg["chunks"] * 16 * (4 * cfg["tile_nodes"]) * (4 * members) * 2 * 3
     bf16, src = measured_peak_bf16_tflops()
     peak = bf16 / 2 if precision == "tf32x3" else bf16
@@ -614,7 +620,8 @@ def run_ensemble(args, desc):
                         err_members=args.err_members, with_e2e=True)
     if rank == 0:
         line = {
-            "metric": f"member-steps/s (batched ensemble, {'3xTF32' if 'tf32' in args.workload else 'split BF16'} "
+            "metric": "member-steps/s (batched ensemble, "
+                      f"{'3xTF32' if 'tf32' in args.workload else 'split FP16' if 'fp16' in args.workload else 'split BF16'} "
                       "tcgen05) and ratio to plain FP64",
             "value": r["value"], "unit": "member-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
@@ -737,9 +744,9 @@ def main():
     level, prec, desc = WORKLOADS[args.workload]
     if args.impl == "reference":
         rlevel = level if level else 6
-        rprec = "fp64" if prec in ("tf32x3", "bf16x3", "serve") else prec
+        rprec = "fp64" if prec in ("tf32x3", "bf16x3", "fp16x3", "serve") else prec
         return run_reference(args, rlevel, rprec, args.workload, desc)
-    if prec in ("tf32x3", "bf16x3"):
+    if prec in ("tf32x3", "bf16x3", "fp16x3"):
         return run_ensemble(args, desc)
     if prec == "serve":
         return run_serving(args, desc)
@@ -865,10 +872,11 @@ def main():
         targets = {}
         for wl in ("plain_fp64_n163842", "plain_fp64_n655362", "plain_fp32_n655362"):
             targets[wl] = plain_target(wl, local, args.target_steps, args.warmup, flush, world)
-        targets["ens_tf32_n163842_b64"] = ensemble_target(
-            "ens_tf32_n163842_b64", local, args.target_steps, args.warmup, flush, world,
-            err_steps=args.err_steps, err_members=args.err_members,
-            plain_rate=targets["plain_fp64_n163842"]["member_steps_per_s"] / world)
+        for wl in ("ens_tf32_n163842_b64", "ens_fp16_n163842_b64"):
+            targets[wl] = ensemble_target(
+                wl, local, args.target_steps, args.warmup, flush, world,
+                err_steps=args.err_steps, err_members=args.err_members,
+                plain_rate=targets["plain_fp64_n163842"]["member_steps_per_s"] / world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

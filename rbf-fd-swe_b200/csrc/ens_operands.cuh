@@ -10,6 +10,13 @@
 //   Bf16x3: kind::f16 with BF16 operands, hi = bf16(x), lo = bf16(x - hi)
 //           (|x - hi - lo| <= 2^-17 |x|), one k-step of K = 16 per chunk;
 //           half the shared-memory bytes of Tf32x3 and twice the tensor rate.
+//   Fp16x3: the same with FP16 operands, which carry TF32's 11-bit significand:
+//           |x - hi - lo| <= 2^-22 |x| within FP16's range.  Power-of-two scales
+//           bring each A row (node, operator) and each state field into that range
+//           (weights: the row's largest at 2^13..2^14; state: the field's largest
+//           value at 2^11..2^12, so that centred values stay below 2^13 and the state
+//           can grow 8-fold before FP16 overflows); the epilogue divides them out
+//           exactly.
 //
 // Padding rows of a tile's neighbour list name the tile's centring node, so their
 // centred values are exactly zero (their weights are zero as well).  Every tile has
@@ -22,6 +29,9 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cstring>
 
 
 #include "tcgen05.cuh"
@@ -31,7 +41,7 @@ namespace swe {
 constexpr int kEnsTileNodes = 32;   // nodes per tile of the default shape (M = 4 operators x 32 nodes)
 constexpr int kEnsKc = 16;          // neighbour rows per pipeline chunk
 
-enum EnsPrecision { kTf32x3 = 0, kBf16x3 = 1 };
+enum EnsPrecision { kTf32x3 = 0, kBf16x3 = 1, kFp16x3 = 2 };
 
 // Row of the A operand (and TMEM lane of the accumulator) that holds operator op of
 // tile node t.  Each 32-lane quarter of tensor memory holds T/4 consecutive tile nodes,
@@ -76,6 +86,37 @@ __device__ __forceinline__ uint32_t bf16x2_split(float a, float b, uint32_t& lo)
     const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
     lo = *reinterpret_cast<const uint32_t*>(&l);
     return *reinterpret_cast<const uint32_t*>(&h);
+}
+// the same with FP16 halves
+__device__ __forceinline__ uint32_t f16x2_split(float a, float b, uint32_t& lo) {
+    const __half2 h = __floats2half2_rn(a, b);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+template <bool F16>
+__device__ __forceinline__ uint32_t half2_split(float a, float b, uint32_t& lo) {
+    return F16 ? f16x2_split(a, b, lo) : bf16x2_split(a, b, lo);
+}
+
+// Scale of state field f for the FP16 operands: 2^e with the field's largest |value|
+// (max_bits[f], an FP32 bit pattern; the velocity fields 0-2 share their largest) at
+// 2^11..2^12; 1 when that is zero.  inverse: 2^-e.
+__host__ __device__ inline float fp16_field_scale(const unsigned* max_bits, int f, bool inverse) {
+    unsigned m = max_bits[3];
+    if (f < 3) {
+        m = max_bits[0] > max_bits[1] ? max_bits[0] : max_bits[1];
+        m = m > max_bits[2] ? m : max_bits[2];
+    }
+    const int ex = (int)((m >> 23) & 0xff);      // biased exponent of the largest value
+    int e = ex == 0 ? 0 : 11 - (ex - 127);
+    e = e < -60 ? -60 : (e > 60 ? 60 : e);
+    // 2^e as an FP32 bit pattern (|e| <= 60 stays normal)
+    const unsigned bits = (unsigned)((inverse ? -e : e) + 127) << 23;
+    float r;
+    memcpy(&r, &bits, sizeof(r));
+    return r;
 }
 
 template <int T, int MPC, int PREC>
@@ -193,12 +234,12 @@ struct Operands<T, MPC, kTf32x3> {
 };
 
 // --------------------------------------------------------------------------------------
-// split BF16, tiles of 32 nodes.  B thread: columns 2p, 2p+1 (fields f, f + 1 of one
-// member, ens_b_col) of rows 8kh..8kh+7.  The A operand comes from an image split once
-// at init (a_offset), like 3xTF32's.
+// split BF16 and FP16 (F16), tiles of 32 nodes.  B thread: columns 2p, 2p+1 (fields f,
+// f + 1 of one member, ens_b_col) of rows 8kh..8kh+7.  The A operand comes from an image
+// split once at init (a_offset), like 3xTF32's.
 // --------------------------------------------------------------------------------------
-template <int MPC>
-struct Operands<32, MPC, kBf16x3> {
+template <int MPC, bool F16>
+struct HalfOperands {
     static constexpr int kStgDepth = 0, kStgBytes = 0;
     static constexpr int kN = 4 * MPC;
     static constexpr int kConvThreads = 4 * MPC;
@@ -247,22 +288,23 @@ struct Operands<32, MPC, kBf16x3> {
         for (int i = 0; i < 8; ++i) o.x[i] = ldg_f2(Kin + (long)r[i] * mf + col);
         o.cen = cen_row ? ldg_f2(cen_row + col) : prev.cen;
     }
-    // the B operand of one chunk: centred rows split into hi and lo, each member-field's
-    // 8 rows one 16-byte core row
-    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o) {
+    // the B operand of one chunk: centred rows (times the thread's two field scales sc,
+    // F16 only) split into hi and lo, each member-field's 8 rows one 16-byte core row
+    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o, float2 sc) {
         unsigned char* B_hi = slot + 2 * kAHalf;
         unsigned char* B_lo = B_hi + kBHalf;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const float c = j ? o.cen.y : o.cen.x;
+            const float m = j ? sc.y : sc.x;
             float y[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) y[i] = (j ? o.x[i].y : o.x[i].x) - c;
+            for (int i = 0; i < 8; ++i) y[i] = F16 ? ((j ? o.x[i].y : o.x[i].x) - c) * m : (j ? o.x[i].y : o.x[i].x) - c;
             uint4 hi, lo;
-            hi.x = bf16x2_split(y[0], y[1], lo.x);
-            hi.y = bf16x2_split(y[2], y[3], lo.y);
-            hi.z = bf16x2_split(y[4], y[5], lo.z);
-            hi.w = bf16x2_split(y[6], y[7], lo.w);
+            hi.x = half2_split<F16>(y[0], y[1], lo.x);
+            hi.y = half2_split<F16>(y[2], y[3], lo.y);
+            hi.z = half2_split<F16>(y[4], y[5], lo.z);
+            hi.w = half2_split<F16>(y[6], y[7], lo.w);
             const int nrow = 2 * th.p + j;
             const uint32_t off = (nrow >> 3) * kSboB + th.kh * 128 + (nrow & 7) * 16;
             *reinterpret_cast<uint4*>(B_hi + off) = hi;
@@ -270,7 +312,7 @@ struct Operands<32, MPC, kBf16x3> {
         }
     }
     __device__ static void issue(uint32_t slot, uint32_t d, bool first) {
-        constexpr uint32_t idesc = tc::idesc_bf16(128, kN);
+        constexpr uint32_t idesc = F16 ? tc::idesc_f16(128, kN) : tc::idesc_bf16(128, kN);
         const uint32_t a_hi = slot, a_lo = slot + kAHalf, b_hi = slot + 2 * kAHalf, b_lo = b_hi + kBHalf;
         const uint64_t dah = tc::smem_desc(a_hi, 128, kSboA);
         const uint64_t dal = tc::smem_desc(a_lo, 128, kSboA);
@@ -281,6 +323,11 @@ struct Operands<32, MPC, kBf16x3> {
         tc::mma_f16(d, dal, dbh, idesc, 1u);
     }
 };
+
+template <int MPC>
+struct Operands<32, MPC, kBf16x3> : HalfOperands<MPC, false> {};
+template <int MPC>
+struct Operands<32, MPC, kFp16x3> : HalfOperands<MPC, true> {};
 
 }  // namespace ens
 }  // namespace swe

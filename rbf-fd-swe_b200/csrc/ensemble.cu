@@ -142,6 +142,7 @@ struct DevTables {
     uint32_t* jmap = nullptr;
     unsigned char* aimg = nullptr;   // [chunk] 3xTF32 A operand image (hi, then lo), 512 T bytes a chunk
     unsigned char* aimg_bf16 = nullptr;   // 32-node tiles: [chunk] split-BF16 A operand image, 8 KB a chunk
+    unsigned char* aimg_f16 = nullptr;    // 32-node tiles: [chunk] FP16 A operand image (rows scaled), 8 KB a chunk
 };
 constexpr int kEnsShapes = 2;          // tiles of 32 and 16 nodes
 constexpr int kEnsShapeNodes[kEnsShapes] = {32, 16};
@@ -219,6 +220,60 @@ static_assert(ens::Operands<32, 64, kTf32x3>::kABytes == 512 * 32 && ens::Operan
               "3xTF32 A image: 512 bytes per tile node and chunk");
 static_assert(ens::Operands<32, 64, kBf16x3>::kABytes == 8192, "split-BF16 A image: 8 KB per chunk");
 
+// The FP16 A operand of every chunk (32-node tiles): as ens_build_aimg_bf16, with each
+// A row's weights times its power-of-two scale AS[node][op] (the row's largest weight at
+// 2^13..2^14) before the split, so that hi and lo stay in FP16's normal range.
+__global__ void ens_build_aimg_f16(const uint32_t* __restrict__ jmap, const int* __restrict__ chunk_tile,
+                                   const float4* __restrict__ W, const float4* __restrict__ AS, int n, int nchunks,
+                                   unsigned char* __restrict__ img) {
+    using Op = ens::Operands<32, 32, kFp16x3>;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)nchunks * 256) return;
+    const int akh = (int)(t & 1);
+    const int r = (int)((t >> 1) & 127);
+    const long gc = t >> 8;
+    const int op = ens_a_row_op<32>(r), at = ens_a_row_node<32>(r);
+    const long node = (long)chunk_tile[gc] * 32 + at;
+    const float scale = node < n ? reinterpret_cast<const float*>(AS + node)[op] : 1.f;
+    float v[8];
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t jj = jmap[(gc * 4 + 2 * akh + h) * 32 + at];
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t j = (jj >> (8 * i)) & 0xffu;
+            v[4 * h + i] =
+                (j != 0xffu && node < n) ? reinterpret_cast<const float*>(W + node * 32 + j)[op] * scale : 0.f;
+        }
+    }
+    uint4 hi, lo;
+    hi.x = ens::f16x2_split(v[0], v[1], lo.x);
+    hi.y = ens::f16x2_split(v[2], v[3], lo.y);
+    hi.z = ens::f16x2_split(v[4], v[5], lo.z);
+    hi.w = ens::f16x2_split(v[6], v[7], lo.w);
+    unsigned char* base = img + (size_t)gc * Op::kABytes + Op::a_offset(r, akh);
+    *reinterpret_cast<uint4*>(base) = hi;
+    *reinterpret_cast<uint4*>(base + Op::kAHalf) = lo;
+}
+
+// The largest |value| of each of the four state fields of an FP32 state [node][4 m + f]
+// (count values), as FP32 bit patterns (non-negative floats order as their bits): the
+// FP16 operands' field scales.  out[0..3] must start at zero.
+__global__ void ens_field_max(const float* __restrict__ X, long count, unsigned* __restrict__ out) {
+    unsigned m[4] = {0u, 0u, 0u, 0u};
+    const long q = count / 4;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < q; e += (long)gridDim.x * blockDim.x) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(X) + e);
+        m[0] = max(m[0], __float_as_uint(fabsf(v.x)));
+        m[1] = max(m[1], __float_as_uint(fabsf(v.y)));
+        m[2] = max(m[2], __float_as_uint(fabsf(v.z)));
+        m[3] = max(m[3], __float_as_uint(fabsf(v.w)));
+    }
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        const unsigned w = __reduce_max_sync(0xffffffffu, m[f]);
+        if ((threadIdx.x & 31) == 0 && w) atomicMax(out + f, w);
+    }
+}
+
 __global__ void ens_invariants_kernel(const float* __restrict__ H32, const double* __restrict__ Hh,
                                       const float4* __restrict__ PT, int n, int members, double gh0,
                                       double* __restrict__ out) {
@@ -284,6 +339,8 @@ struct Ensemble {
     // tile tables, one set per tile shape (32 and 16 nodes)
     DevTables tabs[kEnsShapes];
     float4* W = nullptr;         // raw FP32 weights [n][32], only while the A images are built
+    float4* AI = nullptr;        // [n] FP16 operands: inverse power-of-two scale of each A row
+    unsigned* bmax = nullptr;    // [8] FP16 operands: field maxima of the stepped state, then of eval_rhs's
     Variant var[kEnsVariants];   // (tile nodes, members per CTA): (32, 64), (32, 32), (16, 64), (16, 32)
     int chosen = -1;
     int prec = kTf32x3;
@@ -299,14 +356,15 @@ struct Ensemble {
     void release() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
-        void* ps[] = {perm, PT, RS, H32, D32, Ka, Kb, F, Kx, Hh, Dh, io, inv, bkH32, bkHh, err, W};
+        void* ps[] = {perm, PT, RS, AI, bmax, H32, D32, Ka, Kb, F, Kx, Hh, Dh, io, inv, bkH32, bkHh, err, W};
         for (void* p : ps) if (p) cudaFree(p);
         for (DevTables& t : tabs) {
-            void* tp[] = {t.row_off, t.rows, t.centre, t.jmap, t.aimg, t.aimg_bf16};
+            void* tp[] = {t.row_off, t.rows, t.centre, t.jmap, t.aimg, t.aimg_bf16, t.aimg_f16};
             for (void* p : tp) if (p) cudaFree(p);
             t = DevTables{};
         }
-        perm = nullptr; PT = nullptr; RS = nullptr; H32 = D32 = Ka = Kb = F = Kx = nullptr;
+        perm = nullptr; PT = nullptr; RS = nullptr; AI = nullptr; bmax = nullptr;
+        H32 = D32 = Ka = Kb = F = Kx = nullptr;
         Hh = Dh = io = inv = nullptr; bkH32 = nullptr; bkHh = nullptr; err = nullptr;
         W = nullptr;
         for (auto& v : var) v = Variant{};
@@ -327,7 +385,10 @@ struct Ensemble {
         a.units = tb.ntiles * (members / mpc);
         a.mf = mf;
         a.row_off = tb.row_off; a.rows = tb.rows;
-        a.Aimg = prec == kBf16x3 ? tb.aimg_bf16 : tb.aimg;
+        a.Aimg = prec == kBf16x3 ? tb.aimg_bf16 : prec == kFp16x3 ? tb.aimg_f16 : tb.aimg;
+        a.AI = AI;
+        // the field maxima of the state the stage reads: the stepped state, or eval_rhs's
+        a.bmax = mode >= 0 && mode <= 3 ? bmax : bmax + 4;
         a.centre = tb.centre;
         a.PT = PT;
         a.RS = RS;
@@ -364,7 +425,10 @@ struct Ensemble {
 
     void launch(int vi, int mode) {
         const Variant& v = var[vi];
-        if (prec == kBf16x3) {
+        if (prec == kFp16x3) {
+            if (v.mpc == 64) launch_v<32, 64, kFp16x3>(mode);
+            else launch_v<32, 32, kFp16x3>(mode);
+        } else if (prec == kBf16x3) {
             if (v.mpc == 64) launch_v<32, 64, kBf16x3>(mode);
             else launch_v<32, 32, kBf16x3>(mode);
         } else if (v.tile == 32) {
@@ -402,6 +466,17 @@ struct Ensemble {
             graph = nullptr;
             return SWE_ERR_CUDA;
         }
+        return SWE_OK;
+    }
+
+    // the four field maxima of FP32 state X into out[0..3] (the FP16 operands' scales)
+    int field_max(const float* X, unsigned* out) {
+        const long count = (long)n * mf;
+        SWE_CUDA_TRY(cudaMemsetAsync(out, 0, 4 * sizeof(unsigned), stream));
+        const int blocks = (int)std::min<long>(std::max<long>(1, (count / 4 + 255) / 256), 4L * nsm);
+        ens_field_max<<<blocks, 256, 0, stream>>>(X, count, out);
+        count_launch();
+        SWE_CUDA_TRY(cudaGetLastError());
         return SWE_OK;
     }
 
@@ -519,6 +594,7 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     // constants holds to FP64 accuracy (the h error of the batched form after 1000
     // steps drops several-fold).
     std::vector<float> w((size_t)n * 32 * 4, 0.f), pt((size_t)n * kPointStride, 0.f), rs((size_t)n * 4);
+    std::vector<float> as((size_t)n * 4), ai((size_t)n * 4);
     std::vector<double> X((size_t)n * 3);
     for (long i = 0; i < n; ++i) {
         const long o = E.perm_h[i];
@@ -532,6 +608,16 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
             }
         }
         for (int op = 0; op < 4; ++op) rs[i * 4 + op] = (float)sum[op];
+        // FP16 operands: each A row's scale 2^k puts its largest weight at 2^13..2^14
+        for (int op = 0; op < 4; ++op) {
+            float m = 0.f;
+            for (int j = 0; j < nnbr; ++j) m = std::max(m, std::fabs(w[((size_t)i * 32 + j) * 4 + op]));
+            int ex = 0;
+            if (m > 0.f) std::frexp(m, &ex);
+            const int k = m > 0.f ? std::min(60, std::max(-60, 14 - ex)) : 0;
+            as[i * 4 + op] = std::ldexp(1.f, k);
+            ai[i * 4 + op] = std::ldexp(1.f, -k);
+        }
         float* r = &pt[(size_t)i * kPointStride];
         r[PT_X] = (float)x[o]; r[PT_Y] = (float)y[o]; r[PT_Z] = (float)z[o]; r[PT_F] = (float)f[o];
         r[PT_GHM] = (float)ghm[o];
@@ -554,6 +640,9 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     SWE_TRY(upload(&E.perm, E.perm_h));
     SWE_TRY(upload(reinterpret_cast<float**>(&E.PT), pt));
     SWE_TRY(upload(reinterpret_cast<float**>(&E.RS), rs));
+    SWE_TRY(upload(reinterpret_cast<float**>(&E.AI), ai));
+    float4* ascale = nullptr;    // the A-row scales themselves, while the FP16 image is built
+    SWE_TRY(upload(reinterpret_cast<float**>(&ascale), as));
     for (int sh = 0; sh < kEnsShapes; ++sh) {
         DevTables& d = E.tabs[sh];
         d.ntiles = tbs[sh].ntiles;
@@ -588,6 +677,9 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
                 const long wb = (long)tb.nchunks * 256;
                 ens_build_aimg_bf16<<<(int)std::max<long>(1, (wb + 255) / 256), 256, 0, E.stream>>>(d.jmap, dct, E.W, n,
                                                                                                tb.nchunks, d.aimg_bf16);
+                SWE_CUDA_TRY(cudaMalloc(&d.aimg_f16, std::max<size_t>((size_t)tb.nchunks * 8192, 16)));
+                ens_build_aimg_f16<<<(int)std::max<long>(1, (wb + 255) / 256), 256, 0, E.stream>>>(
+                    d.jmap, dct, E.W, ascale, n, tb.nchunks, d.aimg_f16);
             } else {
                 ens_build_aimg<16><<<blocks, 256, 0, E.stream>>>(d.jmap, dct, d.row_off, E.W, E.RS, n, tb.nchunks, d.aimg);
             }
@@ -596,11 +688,12 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
             return SWE_OK;
         }();
         cudaFree(dct);
-        if (rc != SWE_OK) return rc;
+        if (rc != SWE_OK) { cudaFree(ascale); return rc; }
     }
     // the stage kernels read only the images: the raw weights are not kept
     cudaFree(E.W);
     E.W = nullptr;
+    cudaFree(ascale);
     for (float** p : {&E.H32, &E.D32, &E.Ka, &E.Kb, &E.F, &E.Kx, &E.bkH32}) SWE_CUDA_TRY(cudaMalloc(p, s32));
     for (double** p : {&E.Hh, &E.Dh, &E.bkHh}) SWE_CUDA_TRY(cudaMalloc(p, s64));
     SWE_CUDA_TRY(cudaMalloc(&E.io, (size_t)n * members * 4 * sizeof(double)));
@@ -621,6 +714,10 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     SWE_TRY((Ensemble::set_attrs<16, 64, kTf32x3>()));
     SWE_TRY((Ensemble::set_attrs<32, 32, kBf16x3>()));
     SWE_TRY((Ensemble::set_attrs<32, 64, kBf16x3>()));
+    SWE_TRY((Ensemble::set_attrs<32, 32, kFp16x3>()));
+    SWE_TRY((Ensemble::set_attrs<32, 64, kFp16x3>()));
+    SWE_CUDA_TRY(cudaMalloc(&E.bmax, 8 * sizeof(unsigned)));
+    SWE_CUDA_TRY(cudaMemset(E.bmax, 0, 8 * sizeof(unsigned)));
     E.prec = kTf32x3;
     E.ready = true;
     // default choice until tuned: 32-node tiles, all members in one CTA
@@ -636,6 +733,7 @@ int swe_ens_set_state(const double* H) {
     SWE_CUDA_TRY(cudaMemcpyAsync(E.io, H, total * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     ens_scatter_state<<<ceil_div(total, 256), 256, 0, E.stream>>>(E.io, E.perm, E.n, E.members, E.H32, E.Hh);
     count_launch();
+    SWE_TRY(E.field_max(E.H32, E.bmax));
     SWE_CUDA_TRY(cudaGetLastError());
     return SWE_OK;
 }
@@ -660,6 +758,7 @@ int swe_ens_eval_rhs(const double* K, double* Fh) {
     SWE_CUDA_TRY(cudaMemcpyAsync(E.io, K, total * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     ens_scatter_state<<<ceil_div(total, 256), 256, 0, E.stream>>>(E.io, E.perm, E.n, E.members, E.Kx, nullptr);
     count_launch();
+    SWE_TRY(E.field_max(E.Kx, E.bmax + 4));
     E.launch(E.chosen, kEvalOnly);
     ens_gather_state<<<ceil_div(total, 256), 256, 0, E.stream>>>(E.F, nullptr, E.perm, E.n, E.members, E.io);
     count_launch();
@@ -746,14 +845,14 @@ int swe_ens_config(int* out) {
 
 int swe_ens_set_precision(int precision) {
     SWE_TRY(ens_ready());
-    if (precision != kTf32x3 && precision != kBf16x3) {
-        set_error("swe_ens_set_precision: %d is neither 0 (3xTF32) nor 1 (split BF16)", precision);
+    if (precision != kTf32x3 && precision != kBf16x3 && precision != kFp16x3) {
+        set_error("swe_ens_set_precision: %d is none of 0 (3xTF32), 1 (split BF16), 2 (split FP16)", precision);
         return SWE_ERR_ARG;
     }
     SWE_CUDA_TRY(cudaStreamSynchronize(g_ens.stream));
     g_ens.prec = precision;
     for (double& t : g_ens.tune_ms) t = -1.0;
-    // split BF16 has 32-node tiles only: keep the members per CTA, move to 32-node tiles
+    // the 16-bit splits have 32-node tiles only: keep the members per CTA, move to 32-node tiles
     if (!g_ens.usable(g_ens.chosen))
         for (int vi = 0; vi < kEnsVariants; ++vi)
             if (g_ens.var[vi].tile == 32 && g_ens.var[vi].mpc == g_ens.var[g_ens.chosen].mpc) g_ens.chosen = vi;

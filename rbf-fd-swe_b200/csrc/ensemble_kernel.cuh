@@ -85,7 +85,8 @@ struct EnsCfg {
     static constexpr int kTbRs = T * kPointStride * 4;     // per-tile buffer: PT, row sums, centre
     static constexpr int kTbCen = kTbRs + T * 16;
     static constexpr int kPairs = T / 16;                  // (node, member) pairs per epilogue thread and chunk
-    static constexpr int kTileBuf = (kTbCen + kN * 4 + 127) / 128 * 128;
+    static constexpr int kTbAi = kTbCen + kN * 4;          // FP16 operands: the tile's A-row inverse scales
+    static constexpr int kTileBuf = (kTbAi + T * 16 + 127) / 128 * 128;
     static constexpr int kStgOff = kStages * kStageBytes + kEnsEpiWarps * kXchWarpFloats * 4 + 2 * kTileBuf;
     static constexpr int kSmem = kStgOff + Op::kStgDepth * Op::kStgBytes;
     static constexpr int kTmemCols = (2 * kN <= 256) ? 256 : 512;
@@ -106,6 +107,8 @@ struct EnsArgs {
     const int* centre;     // [ntiles] node whose state centres the tile
     const float4* PT;      // [n][5] pointwise record (20 floats)
     const float4* RS;      // [n] row sums of the four operators
+    const float4* AI;      // [n] FP16 operands: 2^-k of each A row's scale (Dx, Dy, Dz, L)
+    const unsigned* bmax;  // FP16 operands: the state fields' largest |value| (FP32 bits) of the state read
     const float* Kin;      // gather source [n][mf]
     float* H32;            // [n][mf]  u, v, w base state (+ FP32 mirror of h)
     double* Hh;            // [n][members] h base state, FP64
@@ -309,6 +312,12 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             const float* cen_row = p.u != u_prev ? a.Kin + (long)__ldg(a.centre + tile) * a.mf : nullptr;
             Op::fetch_ops(a.Kin, a.mf, col, cen_row, f, o, prev);
         };
+        // FP16 operands: this thread's two fields (f0, f0 + 1) and their scales
+        float2 sc = make_float2(1.f, 1.f);
+        if constexpr (PREC == kFp16x3) {
+            const int f0 = th.col() & 3;
+            sc = make_float2(ens::fp16_field_scale(a.bmax, f0, false), ens::fp16_field_scale(a.bmax, f0 + 1, false));
+        }
         int g = 0;
         auto step = [&](typename Op::Set& o, typename Op::Set& nx, int u_cur) -> bool {
             // look ahead: operands of the next step, indices of the one after
@@ -318,7 +327,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             if (nxt2.valid) Op::fetch_idx(a.rows, nxt2.gc, th, fx);
             const int s = g % C::kStages;
             if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) return false;
-            Op::build(smem + s * C::kStageBytes, th, o);
+            Op::build(smem + s * C::kStageBytes, th, o, sc);
             tc::fence_async_smem();
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&full_bar[s]);
@@ -409,6 +418,12 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
         unsigned char* tbuf = smem + C::kStages * C::kStageBytes + kEnsEpiWarps * C::kXchWarpFloats * 4;
         const int members = a.members;
         const float c32 = (float)a.c;
+        // FP16 operands: the state fields' inverse scales
+        float binv[4] = {1.f, 1.f, 1.f, 1.f};
+        if constexpr (PREC == kFp16x3) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) binv[f] = ens::fp16_field_scale(a.bmax, f, true);
+        }
         constexpr bool kHD = MODE == kStage1 || MODE == kStage2 || MODE == kStage3;
         // per-tile pointwise records (and, for split BF16, whose accumulator lacks the
         // add-back, the row sums and centre row): bulk copies into tbuf[it & 1]
@@ -416,14 +431,17 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             const int tile = u / halves;
             const int nn = min(T, a.n - tile * T);
             unsigned char* tb = tbuf + b * C::kTileBuf;
-            constexpr bool kAddBack = PREC == kBf16x3;
-            tc::mbar_arrive_expect_tx(&tile_bar[b], nn * kPointStride * 4 + (kAddBack ? nn * 16 + C::kN * 4 : 0));
+            constexpr bool kAddBack = PREC != kTf32x3;
+            constexpr bool kScaled = PREC == kFp16x3;
+            tc::mbar_arrive_expect_tx(&tile_bar[b], nn * kPointStride * 4 + (kAddBack ? nn * 16 + C::kN * 4 : 0) +
+                                                        (kScaled ? nn * 16 : 0));
             tc::bulk_g2s(tb, a.PT + (long)tile * T * 5, nn * kPointStride * 4, &tile_bar[b]);
             if constexpr (kAddBack) {
                 tc::bulk_g2s(tb + C::kTbRs, a.RS + (long)tile * T, nn * 16, &tile_bar[b]);
                 tc::bulk_g2s(tb + C::kTbCen, a.Kin + (long)__ldg(a.centre + tile) * a.mf + (u % halves) * C::kN,
                              C::kN * 4, &tile_bar[b]);
             }
+            if constexpr (kScaled) tc::bulk_g2s(tb + C::kTbAi, a.AI + (long)tile * T, nn * 16, &tile_bar[b]);
         };
         // this thread's pair pi of a chunk: tile node pair_node(pi) and chunk member
         // pair_member(pi).  32-node tiles: node qt 8 + lane / 4, members lane % 4 and
@@ -516,7 +534,16 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                         S[4 * o2] = sv.x; S[4 * o2 + 1] = sv.y; S[4 * o2 + 2] = sv.z; S[4 * o2 + 3] = sv.w;
                     }
                 }
-                if constexpr (PREC == kBf16x3) {
+                if constexpr (PREC == kFp16x3) {
+                    // divide out the A row's and the state field's power-of-two scales (exact)
+                    const float4 ai4 = *reinterpret_cast<const float4*>(tb + C::kTbAi / 4 + 4 * t);
+                    const float ai[4] = {ai4.x, ai4.y, ai4.z, ai4.w};
+#pragma unroll
+                    for (int o2 = 0; o2 < 4; ++o2)
+#pragma unroll
+                        for (int f = 0; f < 4; ++f) S[4 * o2 + f] *= ai[o2] * binv[f];
+                }
+                if constexpr (PREC != kTf32x3) {
                     // the centre term c * sum_k W (3xTF32 accumulates it in its add-back row)
                     const float4 cen = *reinterpret_cast<const float4*>(tb + C::kTbCen / 4 + (mfb - col0));
                     const float4 rs4 = *reinterpret_cast<const float4*>(tb + C::kTbRs / 4 + 4 * t);

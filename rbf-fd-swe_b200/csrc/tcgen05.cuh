@@ -1,5 +1,5 @@
 // Thin inline-PTX wrappers for the sm_100a pieces the ensemble kernel uses:
-// tensor memory (TMEM) allocation, tcgen05.mma kind::tf32 and kind::f16 (BF16)
+// tensor memory (TMEM) allocation, tcgen05.mma kind::tf32 and kind::f16 (BF16 or FP16)
 // with shared-memory operands, tcgen05.commit to an mbarrier, tcgen05.ld of the accumulator, and
 // bounded mbarrier waits.  Descriptor formats follow the PTX ISA's tcgen05
 // "shared memory descriptor" and "instruction descriptor" tables.
@@ -62,7 +62,14 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
            | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// D[tmem] (+)= A[smem] * B[smem], BF16 operands, K = 16
+// Instruction descriptor for kind::f16 with FP16 A and B, FP32 accumulator, both
+// operands K-major (A and B formats 0 = F16).
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
+    return (1u << 4)                 // D format F32
+           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[smem] * B[smem], BF16 or FP16 operands (one type for both), K = 16
 __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                         uint32_t accumulate) {
     asm volatile(

@@ -355,10 +355,11 @@ class Ensemble:
     def use_variant(self, tile_nodes: int, members_per_cta: int) -> None:
         check("swe_ens_use_variant", self.lib.swe_ens_use_variant(tile_nodes, members_per_cta))
 
-    PRECISIONS = ("tf32x3", "bf16x3")
+    PRECISIONS = ("tf32x3", "bf16x3", "fp16x3")
 
     def set_precision(self, name: str) -> None:
-        """Stencil products in 3xTF32 ("tf32x3", the default) or split BF16 ("bf16x3")."""
+        """Stencil products in 3xTF32 ("tf32x3", the default), split BF16 ("bf16x3") or split
+        FP16 with power-of-two scales ("fp16x3")."""
         if name not in self.PRECISIONS:
             raise ValueError(f"precision must be one of {self.PRECISIONS}, got {name!r}")
         check("swe_ens_set_precision", self.lib.swe_ens_set_precision(self.PRECISIONS.index(name)))

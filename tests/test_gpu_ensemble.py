@@ -42,16 +42,16 @@ def _members(m, members, seed0=100):
     return np.stack([gen.perturb_h(m.H_init, seed0 + b) for b in range(members)])
 
 
-COND_BOUND = {"tf32x3": 4e-6, "bf16x3": 5e-5}
+COND_BOUND = {"tf32x3": 4e-6, "bf16x3": 5e-5, "fp16x3": 4e-6}
 
 
-@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3"])
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3", "fp16x3"])
 @pytest.mark.parametrize("tile,mpc", VARIANTS)
 def test_eval_rhs_every_variant(ens, model_l4, tile, mpc, prec):
     m = model_l4
     ens.init(m, 64)
     ens.set_precision(prec)
-    if prec == "bf16x3" and tile == 16:
+    if prec != "tf32x3" and tile == 16:
         with pytest.raises(capi.SweError, match="32-node tiles"):
             ens.use_variant(tile, mpc)
         return
@@ -69,11 +69,12 @@ def test_eval_rhs_every_variant(ens, model_l4, tile, mpc, prec):
 
 
 # 3xTF32 is FP32-class (measured 1.3-2.9x the FP32 restatement's error after 20 steps);
-# split BF16 carries 2^-17 operand splits (measured 17-57x); the bars keep ~2x margin.
-STEP_FACTOR = {"tf32x3": 5.0, "bf16x3": 120.0}
+# split BF16 carries 2^-17 operand splits (measured 17-57x); split FP16 has TF32's
+# significands and is held to 3xTF32's bar; the bars keep ~2x margin.
+STEP_FACTOR = {"tf32x3": 5.0, "bf16x3": 120.0, "fp16x3": 5.0}
 
 
-@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3"])
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3", "fp16x3"])
 def test_steps_match_fp64_oracle(ens, model_l4, prec):
     m = model_l4
     ens.init(m, 64)
@@ -123,10 +124,11 @@ def test_tuner_times_every_variant(ens, model_l4):
     best = int(np.argmin(ms))
     cfg = ens.config()
     assert (cfg["tile_nodes"], cfg["members_per_cta"]) == VARIANTS_TUNE_ORDER[best]
-    ens.set_precision("bf16x3")
-    ms = ens.tune()
-    assert (ms[:2] > 0).all() and (ms[2:] < 0).all(), ms
-    assert ens.config()["tile_nodes"] == 32
+    for prec in ("bf16x3", "fp16x3"):
+        ens.set_precision(prec)
+        ms = ens.tune()
+        assert (ms[:2] > 0).all() and (ms[2:] < 0).all(), ms
+        assert ens.config()["tile_nodes"] == 32
 
 
 # the order of swe_ens_tune's table
@@ -136,7 +138,7 @@ VARIANTS_TUNE_ORDER = [(32, 64), (32, 32), (16, 64), (16, 32)]
 def test_rejects_bad_precision(ens, model_l4):
     ens.init(model_l4, 32)
     with pytest.raises(capi.SweError):
-        capi.check("swe_ens_set_precision", ens.lib.swe_ens_set_precision(2))
+        capi.check("swe_ens_set_precision", ens.lib.swe_ens_set_precision(3))
     with pytest.raises(ValueError):
         ens.set_precision("fp16")
 
