@@ -241,8 +241,9 @@ int swe_selftest_wait_timeout(double limit_s, double* waited_s);
  * u, v, w and the stage states K in FP32; the RK4 accumulation of h (base
  * state and D register) in FP64; invariants in FP64.
  * Device memory: besides the member states (about 40 B per node and member),
- * the static weights are kept split for the tensor cores, about 9.5 KB per
- * node for both tile shapes and precisions together (1.55 GB at N=163842). */
+ * the static weights are kept split for the tensor cores, about 11.7 KB per
+ * node for both tile shapes and all three precisions together (1.91 GB at
+ * N=163842). */
 int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int* idx,
                  const double* Dx, const double* Dy, const double* Dz, const double* L,
                  const double* x, const double* y, const double* z, const double* f,
