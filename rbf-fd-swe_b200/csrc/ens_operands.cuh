@@ -16,7 +16,7 @@
 //           (weights: the row's largest at 2^13..2^14; state: the field's largest
 //           value at 2^11..2^12, so that centred values stay below 2^13 and the state
 //           can grow 8-fold before FP16 overflows); the epilogue divides them out
-//           exactly.
+//           exactly.  The centre add-back rides in the MMA as in Tf32x3.
 //
 // Padding rows of a tile's neighbour list name the tile's centring node, so their
 // centred values are exactly zero (their weights are zero as well).  Every tile has
@@ -289,8 +289,12 @@ struct HalfOperands {
         o.cen = cen_row ? ldg_f2(cen_row + col) : prev.cen;
     }
     // the B operand of one chunk: centred rows (times the thread's two field scales sc,
-    // F16 only) split into hi and lo, each member-field's 8 rows one 16-byte core row
-    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o, float2 sc) {
+    // F16 only) split into hi and lo, each member-field's 8 rows one 16-byte core row.
+    // F16: row 15 of a unit's last chunk (last = true) is its add-back row, as in
+    // 3xTF32: it carries the centre state itself, and the image's weights there are the
+    // operators' row sums.
+    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o, float2 sc, bool last) {
+        const bool keep15 = F16 && last && th.kh == 1;
         unsigned char* B_hi = slot + 2 * kAHalf;
         unsigned char* B_lo = B_hi + kBHalf;
 #pragma unroll
@@ -300,6 +304,7 @@ struct HalfOperands {
             float y[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) y[i] = F16 ? ((j ? o.x[i].y : o.x[i].x) - c) * m : (j ? o.x[i].y : o.x[i].x) - c;
+            if (keep15) y[7] = (j ? o.x[7].y : o.x[7].x) * m;
             uint4 hi, lo;
             hi.x = half2_split<F16>(y[0], y[1], lo.x);
             hi.y = half2_split<F16>(y[2], y[3], lo.y);

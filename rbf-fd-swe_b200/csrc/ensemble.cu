@@ -222,9 +222,12 @@ static_assert(ens::Operands<32, 64, kBf16x3>::kABytes == 8192, "split-BF16 A ima
 
 // The FP16 A operand of every chunk (32-node tiles): as ens_build_aimg_bf16, with each
 // A row's weights times its power-of-two scale AS[node][op] (the row's largest weight at
-// 2^13..2^14) before the split, so that hi and lo stay in FP16's normal range.
+// 2^13..2^14) before the split, so that hi and lo stay in FP16's normal range.  Row 15
+// of a tile's last chunk is the add-back row, as in ens_build_aimg: its weights are the
+// operators' row sums (scaled the same way).
 __global__ void ens_build_aimg_f16(const uint32_t* __restrict__ jmap, const int* __restrict__ chunk_tile,
-                                   const float4* __restrict__ W, const float4* __restrict__ AS, int n, int nchunks,
+                                   const int* __restrict__ row_off, const float4* __restrict__ W,
+                                   const float4* __restrict__ RS, const float4* __restrict__ AS, int n, int nchunks,
                                    unsigned char* __restrict__ img) {
     using Op = ens::Operands<32, 32, kFp16x3>;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -244,6 +247,9 @@ __global__ void ens_build_aimg_f16(const uint32_t* __restrict__ jmap, const int*
                 (j != 0xffu && node < n) ? reinterpret_cast<const float*>(W + node * 32 + j)[op] * scale : 0.f;
         }
     }
+    const int tile = chunk_tile[gc];
+    if (akh == 1 && (gc + 1) * kEnsKc == row_off[tile + 1] && node < n)
+        v[7] = reinterpret_cast<const float*>(RS + node)[op] * scale;
     uint4 hi, lo;
     hi.x = ens::f16x2_split(v[0], v[1], lo.x);
     hi.y = ens::f16x2_split(v[2], v[3], lo.y);
@@ -679,7 +685,7 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
                                                                                                tb.nchunks, d.aimg_bf16);
                 SWE_CUDA_TRY(cudaMalloc(&d.aimg_f16, std::max<size_t>((size_t)tb.nchunks * 8192, 16)));
                 ens_build_aimg_f16<<<(int)std::max<long>(1, (wb + 255) / 256), 256, 0, E.stream>>>(
-                    d.jmap, dct, E.W, ascale, n, tb.nchunks, d.aimg_f16);
+                    d.jmap, dct, d.row_off, E.W, E.RS, ascale, n, tb.nchunks, d.aimg_f16);
             } else {
                 ens_build_aimg<16><<<blocks, 256, 0, E.stream>>>(d.jmap, dct, d.row_off, E.W, E.RS, n, tb.nchunks, d.aimg);
             }

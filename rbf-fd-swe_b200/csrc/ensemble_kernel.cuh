@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             if (nxt2.valid) Op::fetch_idx(a.rows, nxt2.gc, th, fx);
             const int s = g % C::kStages;
             if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) return false;
-            Op::build(smem + s * C::kStageBytes, th, o, sc);
+            Op::build(smem + s * C::kStageBytes, th, o, sc, cur.gc + 1 == cur.gc_end);
             tc::fence_async_smem();
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&full_bar[s]);
@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             const int tile = u / halves;
             const int nn = min(T, a.n - tile * T);
             unsigned char* tb = tbuf + b * C::kTileBuf;
-            constexpr bool kAddBack = PREC != kTf32x3;
+            constexpr bool kAddBack = PREC == kBf16x3;
             constexpr bool kScaled = PREC == kFp16x3;
             tc::mbar_arrive_expect_tx(&tile_bar[b], nn * kPointStride * 4 + (kAddBack ? nn * 16 + C::kN * 4 : 0) +
                                                         (kScaled ? nn * 16 : 0));
@@ -543,8 +543,9 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
 #pragma unroll
                         for (int f = 0; f < 4; ++f) S[4 * o2 + f] *= ai[o2] * binv[f];
                 }
-                if constexpr (PREC != kTf32x3) {
-                    // the centre term c * sum_k W (3xTF32 accumulates it in its add-back row)
+                if constexpr (PREC == kBf16x3) {
+                    // the centre term c * sum_k W (3xTF32 and split FP16 accumulate it in
+                    // their add-back row)
                     const float4 cen = *reinterpret_cast<const float4*>(tb + C::kTbCen / 4 + (mfb - col0));
                     const float4 rs4 = *reinterpret_cast<const float4*>(tb + C::kTbRs / 4 + 4 * t);
                     const float cf[4] = {cen.x, cen.y, cen.z, cen.w};
