@@ -165,6 +165,8 @@ struct Operands<T, MPC, kTf32x3> {
         float4 x[4];          // 4 gathered rows x 4 member-fields
         float4 cen;           // centre state of the same member-fields
     };
+    using Cen = float4;
+    __device__ static Cen load_cen(const float* p) { return ldg_f4(p); }
 
     __device__ static void fetch_idx(const int* rows, int gc, const Thread& th, Fetch& f) {
         f.idx = __ldg(reinterpret_cast<const int4*>(rows + gc * kEnsKc + 4 * th.kg));
@@ -189,7 +191,7 @@ struct Operands<T, MPC, kTf32x3> {
     // unit's last chunk (last = true) is its add-back row: it carries the centre state
     // itself, not centred, and its A weights are the operators' row sums, so the
     // accumulator receives c * sum_k W with the stencil sums.
-    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o, bool last) {
+    __device__ static void build(unsigned char* slot, const Thread& th, const Set& o, float2, bool last) {
         unsigned char* B_hi = slot + 2 * kAHalf;
         unsigned char* B_lo = B_hi + kBHalf;
         const bool keep15 = last && th.kg == 3;
@@ -240,7 +242,9 @@ struct Operands<T, MPC, kTf32x3> {
 // --------------------------------------------------------------------------------------
 template <int MPC, bool F16>
 struct HalfOperands {
-    static constexpr int kStgDepth = 0, kStgBytes = 0;
+    // staged gathers (cp.async, 8 bytes a row): per converter thread and chunk, 8 rows x
+    // 2 member-fields in structure-of-arrays order, three chunks in flight
+    static constexpr int kStgDepth = 3, kStgBytes = 8 * 4 * MPC * 8;
     static constexpr int kN = 4 * MPC;
     static constexpr int kConvThreads = 4 * MPC;
     static constexpr int kSboA = (kEnsKc / 8) * 128;
@@ -274,19 +278,30 @@ struct HalfOperands {
         float2 x[8];          // 8 gathered rows x 2 member-fields
         float2 cen;
     };
+    using Cen = float2;
+    __device__ static Cen load_cen(const float* p) { return ldg_f2(p); }
 
     __device__ static void fetch_idx(const int* rows, int gc, const Thread& th, Fetch& f) {
         const int4* r = reinterpret_cast<const int4*>(rows + gc * kEnsKc + 8 * th.kh);
         f.idx[0] = __ldg(r);
         f.idx[1] = __ldg(r + 1);
     }
-    __device__ static void fetch_ops(const float* Kin, int mf, long col, const float* cen_row, const Fetch& f, Set& o,
-                                     const Set& prev) {
+    // cp.async of this thread's 8 gathered rows of one chunk into staging buffer `stg`
+    __device__ static void stage_issue(unsigned char* stg, int ct, const float* Kin, int mf, long col,
+                                       const Fetch& f) {
         const int r[8] = {f.idx[0].x, f.idx[0].y, f.idx[0].z, f.idx[0].w,
                           f.idx[1].x, f.idx[1].y, f.idx[1].z, f.idx[1].w};
 #pragma unroll
-        for (int i = 0; i < 8; ++i) o.x[i] = ldg_f2(Kin + (long)r[i] * mf + col);
-        o.cen = cen_row ? ldg_f2(cen_row + col) : prev.cen;
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t dst = tc::smem_u32(stg + (i * kConvThreads + ct) * 8);
+            const float* src = Kin + (long)r[i] * mf + col;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+        }
+    }
+    __device__ static void stage_read(const unsigned char* stg, int ct, const float2& cen, Set& o) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) o.x[i] = *reinterpret_cast<const float2*>(stg + (i * kConvThreads + ct) * 8);
+        o.cen = cen;
     }
     // the B operand of one chunk: centred rows (times the thread's two field scales sc,
     // F16 only) split into hi and lo, each member-field's 8 rows one 16-byte core row.

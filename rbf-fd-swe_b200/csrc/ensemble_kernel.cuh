@@ -17,12 +17,12 @@
 //
 // Precision: both operands are split x ~ hi + lo, and D = A_hi B_hi + A_hi B_lo
 // + A_lo B_hi accumulates in FP32 in tensor memory; the split is 3xTF32
-// (|x - hi - lo| <= 2^-21 |x| as the tensor core reads it) or split BF16
-// (2^-17), see ens_operands.cuh.  The gathered states are
-// centred on the state of one node of the tile (c[mf]) before the split, and
-// c * sum_k W (row sums of the FP64 weights) is added back: with 3xTF32 by the
-// MMA itself, through one more K row whose B values are c and whose A weights
-// are the row sums; with split BF16 in the epilogue.  Derivative and
+// (|x - hi - lo| <= 2^-21 |x| as the tensor core reads it), split FP16 with
+// power-of-two scales (2^-22) or split BF16 (2^-17), see ens_operands.cuh.  The
+// gathered states are centred on the state of one node of the tile (c[mf]) before
+// the split, and c * sum_k W (row sums of the FP64 weights) is added back: with
+// 3xTF32 and split FP16 by the MMA itself, through one more K row whose B values
+// are c and whose A weights are the row sums; with split BF16 in the epilogue.  Derivative and
 // hyperviscosity weights annihilate constants, so the added-back term is small
 // and the cancellation that limits FP32 stencil sums mostly disappears.  The RK4
 // accumulation of h (base state and D register) is FP64; u, v, w and every stage
@@ -30,16 +30,16 @@
 //
 // Persistent, warp-specialised CTA (one per SM; it owns all of tensor memory):
 //   * converter warps (MPC/8): for each 16-row chunk of K they gather the rows
-//     (3xTF32: async copies into a staging buffer issued two chunks ahead, three
-//     buffers deep, so that no register waits on a gather; split BF16: 16-byte
-//     loads one chunk ahead into a ping-pong register set) and centre and split
-//     them into the B operand;
+//     as async copies into a staging buffer issued two chunks ahead, three
+//     buffers deep, so that no register waits on a gather (16 bytes a row for
+//     3xTF32, 8 for the 16-bit splits), and centre and split them into the B
+//     operand;
 //   * the A producer warp: the A chunks are static, so they are split once at
 //     init into an image of the slot's A part (per precision); one thread streams
 //     each chunk's image into its slot with one bulk copy (and prefetches the
 //     image two chunks ahead into L2);
 //   * a ring of slots (2 for 3xTF32, whose staging takes the third slot's shared
-//     memory) hands chunks to the MMA warp: one thread issues the chunk's 3
+//     memory; 5 for the 16-bit splits) hands chunks to the MMA warp: one thread issues the chunk's 3
 //     products (128 x N x 16) into one of two TMEM accumulators once the
 //     converters and the A copy have filled the slot, and commits each chunk to
 //     the slot's "empty" barrier and each tile to the accumulator's "full" barrier;
@@ -242,7 +242,12 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
 
     if (warp < C::kConvWarps) {
         // =============================== converters ===============================
-      if constexpr (PREC == kTf32x3) {
+        // FP16 operands: this thread's two fields (f0, f0 + 1) and their scales
+        float2 sc = make_float2(1.f, 1.f);
+        if constexpr (PREC == kFp16x3) {
+            const int f0 = typename Op::Thread(threadIdx.x).col() & 3;
+            sc = make_float2(ens::fp16_field_scale(a.bmax, f0, false), ens::fp16_field_scale(a.bmax, f0 + 1, false));
+        }
         // staged gathers: chunk g + 2's rows are in flight (cp.async) while chunk g is
         // built from its staging buffer
         const typename Op::Thread th(threadIdx.x);
@@ -254,15 +259,16 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
         ens::Cursor c1 = ens::next_cursor(cur, a, halves);
         ens::Cursor c2 = ens::next_cursor(c1, a, halves);
         typename Op::Fetch f2, f3;     // indices of chunks g + 2 and g + 3
-        float4 cen0 = make_float4(0.f, 0.f, 0.f, 0.f), cen1 = cen0, cen2 = cen0;   // centres of chunks g, g+1, g+2
+        using Cen = typename Op::Cen;
+        Cen cen0{}, cen1{}, cen2{};    // centres of chunks g, g+1, g+2
         // returns the centre state of chunk p's unit (a new unit loads it; else prev)
-        auto issue = [&](const ens::Cursor& p, const typename Op::Fetch& f, int slot, float4 prev) {
-            float4 c = prev;
+        auto issue = [&](const ens::Cursor& p, const typename Op::Fetch& f, int slot, Cen prev) {
+            Cen c = prev;
             if (p.valid) {
                 const int tile = p.u / halves;
                 const long col = (long)(p.u % halves) * C::kN + th.col();
                 Op::stage_issue(stg0 + slot * Op::kStgBytes, ct, a.Kin, a.mf, col, f);
-                if (p.gc == p.gc0) c = ens::ldg_f4(a.Kin + (long)__ldg(a.centre + tile) * a.mf + col);
+                if (p.gc == p.gc0) c = Op::load_cen(a.Kin + (long)__ldg(a.centre + tile) * a.mf + col);
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
             return c;
@@ -286,7 +292,7 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) break;
             typename Op::Set o;
             Op::stage_read(stg0 + (g % 3) * Op::kStgBytes, ct, cen0, o);
-            Op::build(smem + s * C::kStageBytes, th, o, cur.gc + 1 == cur.gc_end);
+            Op::build(smem + s * C::kStageBytes, th, o, sc, cur.gc + 1 == cur.gc_end);
             tc::fence_async_smem();
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&full_bar[s]);
@@ -299,58 +305,6 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             cen1 = cen2;
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
-      } else {
-        const typename Op::Thread th(threadIdx.x);
-        ens::Cursor cur = ens::first_cursor(a, halves);
-        typename Op::Fetch fx;         // indices of the step after the current one
-        typename Op::Set sa, sb;       // operands of the current / next step (ping-pong)
-        auto fetch_ops = [&](const ens::Cursor& p, const typename Op::Fetch& f, typename Op::Set& o,
-                             const typename Op::Set& prev, int u_prev) {
-            if (!p.valid) return;
-            const int tile = p.u / halves;
-            const long col = (long)(p.u % halves) * C::kN + th.col();
-            const float* cen_row = p.u != u_prev ? a.Kin + (long)__ldg(a.centre + tile) * a.mf : nullptr;
-            Op::fetch_ops(a.Kin, a.mf, col, cen_row, f, o, prev);
-        };
-        // FP16 operands: this thread's two fields (f0, f0 + 1) and their scales
-        float2 sc = make_float2(1.f, 1.f);
-        if constexpr (PREC == kFp16x3) {
-            const int f0 = th.col() & 3;
-            sc = make_float2(ens::fp16_field_scale(a.bmax, f0, false), ens::fp16_field_scale(a.bmax, f0 + 1, false));
-        }
-        int g = 0;
-        auto step = [&](typename Op::Set& o, typename Op::Set& nx, int u_cur) -> bool {
-            // look ahead: operands of the next step, indices of the one after
-            ens::Cursor nxt = ens::next_cursor(cur, a, halves);
-            fetch_ops(nxt, fx, nx, o, u_cur);
-            ens::Cursor nxt2 = ens::next_cursor(nxt, a, halves);
-            if (nxt2.valid) Op::fetch_idx(a.rows, nxt2.gc, th, fx);
-            const int s = g % C::kStages;
-            if (!ens::wait(&empty_bar[s], ((g / C::kStages) & 1) ^ 1, abort_v, a.err, 3)) return false;
-            Op::build(smem + s * C::kStageBytes, th, o, sc, cur.gc + 1 == cur.gc_end);
-            tc::fence_async_smem();
-            __syncwarp();
-            if (lane == 0) ens::mbar_arrive(&full_bar[s]);
-            ++g;
-            cur = nxt;
-            return true;
-        };
-        if (cur.valid) {
-            typename Op::Fetch f0;
-            Op::fetch_idx(a.rows, cur.gc, th, f0);
-            fetch_ops(cur, f0, sa, sa, -1);
-            const ens::Cursor n1 = ens::next_cursor(cur, a, halves);
-            if (n1.valid) Op::fetch_idx(a.rows, n1.gc, th, fx);
-        }
-        // two steps per trip so that the ping-pong sets never need copying
-        while (cur.valid) {
-            int u = cur.u;
-            if (!step(sa, sb, u)) break;
-            if (!cur.valid) break;
-            u = cur.u;
-            if (!step(sb, sa, u)) break;
-        }
-      }
     } else if (warp == C::kMmaWarp) {
         // =============================== MMA issuer ===============================
         if (lane == 0) {
