@@ -276,9 +276,9 @@ int swe_ens_use_variant(int tile_nodes, int members_per_cta);
  * FP16 (2^-22 within FP16's range), all with FP32 accumulation and the same
  * FP64 h accumulation.  Split FP16 scales each weight row by a power of two and
  * each state field by one taken from the largest |value| of that field (the
- * velocities share one) when the state is set: the state may grow 8-fold after
- * swe_ens_set_state before FP16 overflows, which swe_ens_invariants then
- * reports as SWE_ERR_NONFINITE.  Splits 1 and 2 use 32-node tiles. */
+ * velocities share one), again after every step: a field may grow 8-fold
+ * within one step before FP16 overflows, which swe_ens_invariants then reports
+ * as SWE_ERR_NONFINITE.  Splits 1 and 2 use 32-node tiles. */
 int swe_ens_set_precision(int precision);
 /* FP64 (mass, energy) per member, [members][2], definitions as swe_cuda_invariants;
  * SWE_ERR_NONFINITE (message naming the first such member) when a member's sums

@@ -14,9 +14,10 @@
 //           |x - hi - lo| <= 2^-22 |x| within FP16's range.  Power-of-two scales
 //           bring each A row (node, operator) and each state field into that range
 //           (weights: the row's largest at 2^13..2^14; state: the field's largest
-//           value at 2^11..2^12, so that centred values stay below 2^13 and the state
-//           can grow 8-fold before FP16 overflows); the epilogue divides them out
-//           exactly.  The centre add-back rides in the MMA as in Tf32x3.
+//           value at 2^11..2^12, taken again after every step, so that centred values
+//           stay below 2^13 and a field can grow 8-fold within a step before FP16
+//           overflows); the epilogue divides them out exactly.  The centre add-back
+//           rides in the MMA as in Tf32x3.
 //
 // Padding rows of a tile's neighbour list name the tile's centring node, so their
 // centred values are exactly zero (their weights are zero as well).  Every tile has

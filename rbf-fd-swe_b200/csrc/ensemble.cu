@@ -346,7 +346,8 @@ struct Ensemble {
     DevTables tabs[kEnsShapes];
     float4* W = nullptr;         // raw FP32 weights [n][32], only while the A images are built
     float4* AI = nullptr;        // [n] FP16 operands: inverse power-of-two scale of each A row
-    unsigned* bmax = nullptr;    // [8] FP16 operands: field maxima of the stepped state, then of eval_rhs's
+    unsigned* bmax = nullptr;    // [12] FP16 operands: field maxima of the stepped state, of eval_rhs's, and of
+                                 // the state stage 3 writes
     Variant var[kEnsVariants];   // (tile nodes, members per CTA): (32, 64), (32, 32), (16, 64), (16, 32)
     int chosen = -1;
     int prec = kTf32x3;
@@ -394,7 +395,11 @@ struct Ensemble {
         a.Aimg = prec == kBf16x3 ? tb.aimg_bf16 : prec == kFp16x3 ? tb.aimg_f16 : tb.aimg;
         a.AI = AI;
         // the field maxima of the state the stage reads: the stepped state, or eval_rhs's
-        a.bmax = mode >= 0 && mode <= 3 ? bmax : bmax + 4;
+        // split FP16 field maxima: [0..3] what stages 1-3 read (stage 0 copies them in),
+        // [4..7] eval_rhs's state, [8..11] the stepped state's (set_state, stage 3)
+        a.bmax = mode == 0 ? bmax + 8 : (mode >= 1 && mode <= 3 ? bmax : bmax + 4);
+        a.bmax_next = bmax + 8;
+        a.bmax_pub = bmax;
         a.centre = tb.centre;
         a.PT = PT;
         a.RS = RS;
@@ -537,6 +542,8 @@ int tune(Ensemble& E) {
         if (ms < best) { best = ms; best_i = vi; }
         SWE_CUDA_TRY(cudaMemcpyAsync(E.H32, E.bkH32, b32, cudaMemcpyDeviceToDevice, E.stream));
         SWE_CUDA_TRY(cudaMemcpyAsync(E.Hh, E.bkHh, b64, cudaMemcpyDeviceToDevice, E.stream));
+        // the restored state's field maxima, which the steps above moved on
+        SWE_TRY(E.field_max(E.H32, E.bmax + 8));
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -722,8 +729,8 @@ int swe_ens_init(int members, int n, int nnbr, double gh0, double dt, const int*
     SWE_TRY((Ensemble::set_attrs<32, 64, kBf16x3>()));
     SWE_TRY((Ensemble::set_attrs<32, 32, kFp16x3>()));
     SWE_TRY((Ensemble::set_attrs<32, 64, kFp16x3>()));
-    SWE_CUDA_TRY(cudaMalloc(&E.bmax, 8 * sizeof(unsigned)));
-    SWE_CUDA_TRY(cudaMemset(E.bmax, 0, 8 * sizeof(unsigned)));
+    SWE_CUDA_TRY(cudaMalloc(&E.bmax, 12 * sizeof(unsigned)));
+    SWE_CUDA_TRY(cudaMemset(E.bmax, 0, 12 * sizeof(unsigned)));
     E.prec = kTf32x3;
     E.ready = true;
     // default choice until tuned: 32-node tiles, all members in one CTA
@@ -739,7 +746,7 @@ int swe_ens_set_state(const double* H) {
     SWE_CUDA_TRY(cudaMemcpyAsync(E.io, H, total * sizeof(double), cudaMemcpyHostToDevice, E.stream));
     ens_scatter_state<<<ceil_div(total, 256), 256, 0, E.stream>>>(E.io, E.perm, E.n, E.members, E.H32, E.Hh);
     count_launch();
-    SWE_TRY(E.field_max(E.H32, E.bmax));
+    SWE_TRY(E.field_max(E.H32, E.bmax + 8));
     SWE_CUDA_TRY(cudaGetLastError());
     return SWE_OK;
 }

@@ -109,6 +109,9 @@ struct EnsArgs {
     const float4* RS;      // [n] row sums of the four operators
     const float4* AI;      // [n] FP16 operands: 2^-k of each A row's scale (Dx, Dy, Dz, L)
     const unsigned* bmax;  // FP16 operands: the state fields' largest |value| (FP32 bits) of the state read
+    unsigned* bmax_next;   // FP16 operands: the maxima of the state stage 3 writes (stage 2 clears them,
+                           // stage 3 raises them by atomicMax, the next stage 0 reads them)
+    unsigned* bmax_pub;    // FP16 operands, stage 0: where it copies the maxima it read for stages 1-3
     const float* Kin;      // gather source [n][mf]
     float* H32;            // [n][mf]  u, v, w base state (+ FP32 mirror of h)
     double* Hh;            // [n][members] h base state, FP64
@@ -230,6 +233,16 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
         tc::mbar_init(&fin_bar, 1);
         abort_s = 0;
         tc::fence_mbar_init();
+    }
+    // split FP16: the field maxima hand over from step to step without another launch --
+    // stage 0 copies the ones it reads (the previous stage 3's) to where stages 1-3 read
+    // them, and stage 2 clears the slot stage 3 fills.  No launch reads a slot that the
+    // same launch writes.
+    if constexpr (PREC == kFp16x3) {
+        if (blockIdx.x == 0 && threadIdx.x < 4) {
+            if constexpr (MODE == kStage0) a.bmax_pub[threadIdx.x] = a.bmax[threadIdx.x];
+            if constexpr (MODE == kStage2) a.bmax_next[threadIdx.x] = 0u;
+        }
     }
     if (warp == C::kMmaWarp) {
         tc::tmem_alloc(&tmem_s, C::kTmemCols);
@@ -424,6 +437,9 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                 }
             }
         };
+        // split FP16, stage 3: the largest |value| of each field this thread writes, for
+        // the next step's field scales
+        unsigned hmax[4] = {0u, 0u, 0u, 0u};
         // one 32-column chunk: accumulator -> exchange -> (node, member) epilogue
         auto chunk = [&](int u, int it, int ch, ens::EpiSet& o) {
             const int ab = it & 1;
@@ -546,10 +562,17 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
                     const double dh = o.dh[pi] + (double)F[3];
                     const double h = o.hh[pi] + a.dt6 * dh;
                     a.Hh[eh] = h;
-                    *reinterpret_cast<float4*>(a.H32 + e4) =
-                        make_float4(__double2float_rn((double)h4.x + a.dt6 * (double)du),
-                                    __double2float_rn((double)h4.y + a.dt6 * (double)dv),
-                                    __double2float_rn((double)h4.z + a.dt6 * (double)dw), __double2float_rn(h));
+                    const float4 hn = make_float4(__double2float_rn((double)h4.x + a.dt6 * (double)du),
+                                                  __double2float_rn((double)h4.y + a.dt6 * (double)dv),
+                                                  __double2float_rn((double)h4.z + a.dt6 * (double)dw),
+                                                  __double2float_rn(h));
+                    *reinterpret_cast<float4*>(a.H32 + e4) = hn;
+                    if constexpr (PREC == kFp16x3) {
+                        hmax[0] = max(hmax[0], __float_as_uint(fabsf(hn.x)));
+                        hmax[1] = max(hmax[1], __float_as_uint(fabsf(hn.y)));
+                        hmax[2] = max(hmax[2], __float_as_uint(fabsf(hn.z)));
+                        hmax[3] = max(hmax[3], __float_as_uint(fabsf(hn.w)));
+                    }
                 }
             }
             if constexpr (T != 32) __syncwarp();   // the exchange rows are rewritten by the next chunk
@@ -581,6 +604,13 @@ __global__ void __launch_bounds__(EnsCfg<T, MPC, PREC>::kThreads, 1) ens_stage_k
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) ens::mbar_arrive(&acce_bar[ab]);
+        }
+        if constexpr (MODE == kStage3 && PREC == kFp16x3) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                const unsigned w = __reduce_max_sync(0xffffffffu, hmax[f]);
+                if (lane == 0 && w) atomicMax(a.bmax_next + f, w);
+            }
         }
         // after an abort, a tile copy still in flight lands before the CTA ends
         if (pend >= 0) tc::mbar_wait_bounded(&tile_bar[pend & 1], (pend >> 1) & 1, kEnsWaitTries);

@@ -94,6 +94,29 @@ def test_steps_match_fp64_oracle(ens, model_l4, prec):
         assert (err <= STEP_FACTOR[prec] * fp32_err).all(), (b, err, fp32_err)
 
 
+def test_fp16_scales_follow_the_state(ens, model_l4):
+    """Split FP16 takes its field scales again after every step.  From a state at rest
+    (every velocity zero when the state is set, so the velocities' first scale is 1) the
+    flow that develops is brought into FP16's range from the next step on: 20 steps stay
+    within 3xTF32's bar against the FP64 oracle."""
+    m = model_l4
+    H0 = _members(m, 64)
+    H0[:, :, :3] = 0.0
+    ens.init(m, 64)
+    ens.set_precision("fp16x3")
+    ens.set_state(H0)
+    ens.step(20)
+    H = ens.get_state()
+    port, port32 = oracle.Port(m, "fp64"), oracle.Port(m, "fp32")
+    for b in (0, 33):
+        want = port.run(H0[b], 20)
+        assert np.abs(want[:, :3]).max() > 0
+        fp32_err = rel_err(port32.run(H0[b], 20), want)
+        err = rel_err(H[b], want)
+        print(f"20 steps from rest fp16x3 member {b}: err {err} fp32 {fp32_err}")
+        assert (err <= STEP_FACTOR["fp16x3"] * fp32_err).all(), (b, err, fp32_err)
+
+
 @pytest.mark.parametrize("tile,mpc", VARIANTS)
 def test_every_tile_shape_steps_like_the_oracle(ens, model_l4, tile, mpc):
     """Each tile shape and members-per-CTA choice, forced, over 20 RK4 steps: the same
