@@ -864,6 +864,9 @@ int swe_ens_set_precision(int precision) {
     }
     SWE_CUDA_TRY(cudaStreamSynchronize(g_ens.stream));
     g_ens.prec = precision;
+    // split FP16 reads the field maxima of the current state, which the other precisions
+    // do not keep up to date while they step
+    if (precision == kFp16x3) SWE_TRY(g_ens.field_max(g_ens.H32, g_ens.bmax + 8));
     for (double& t : g_ens.tune_ms) t = -1.0;
     // the 16-bit splits have 32-node tiles only: keep the members per CTA, move to 32-node tiles
     if (!g_ens.usable(g_ens.chosen))
