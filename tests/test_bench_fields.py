@@ -21,6 +21,8 @@ def test_tensor_roofline_counts_every_chunk_product():
     assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-3
     rb = bench.ensemble_tensor_roofline(cfg, 64, "bf16x3", 334e-6)
     assert rb["peak"] == round(bf16, 1)
+    # split FP16 runs kind::f16 at the 16-bit rate, like split BF16
+    assert bench.ensemble_tensor_roofline(cfg, 64, "fp16x3", 334e-6)["peak"] == round(bf16, 1)
     # 16-node tiles: M = 64
     r16 = bench.ensemble_tensor_roofline({"chunks": 1000, "tile_nodes": 16}, 32, "tf32x3", 1e-3)
     assert r16["mma_flops_per_launch"] == 1000 * 16 * 64 * 128 * 2 * 3
@@ -38,3 +40,9 @@ def test_plain_bytes_follow_the_index_width():
     assert bench.plain_alg_bytes("fp32", lane16) == 760 - 62
     # the other kernels read 32-bit indices whatever the lane kernel would read
     assert bench.plain_alg_bytes("fp64", {"in_use": "pipelined", "index_offsets_16bit": True}) == 1396
+
+
+def test_fp16_ensemble_workload_is_registered():
+    level, prec, desc = bench.WORKLOADS["ens_fp16_n163842_b64"]
+    assert (level, prec) == (7, "fp16x3") and "FP16" in desc
+    assert bench.TRAFFIC_BYTES["ens_fp16_n163842_b64"] > 0
